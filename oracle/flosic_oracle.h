@@ -1,0 +1,86 @@
+/*
+ * FP64 CPU oracle for the FLO-SIC per-Fermi-orbital hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library restates, routine by routine, the
+ * reference Fortran algorithm (FLOSIC/PublicRelease_2020, directory flosic/)
+ * so that the CUDA product path can be checked against it.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline legs may load it; the
+ * product library (libflosic_sic_b200.so) never links or calls it.
+ *
+ * Layout conventions (all arrays are Fortran column-major, as in the
+ * reference modules; the leading dimensions are the reference's static sizes
+ * MAX_BARE=25 and MAX_CON=15):
+ *   BFALP(MAX_BARE, ntypes)                 exponents of bare primitives
+ *   BFCON(MAX_BARE, MAX_CON, 3, ntypes)     contraction coefficients
+ *   N_CON(3, ntypes), N_BARE(ntypes)
+ *   RAT(3, natoms)      atom positions, atoms ordered by type (IFNCT, I_POS)
+ *   RMSH(3, nmsh), WMSH(nmsh)
+ *   PSI(nbasis, nwf)    KS coefficients, spin-1 orbitals first; the basis
+ *                       order inside an atom is (l, Cartesian component,
+ *                       contraction), contraction fastest (unravel2.f:160-175)
+ *   BFRM(3, ldfrm, 2)   FOD positions per spin
+ */
+#ifndef FLOSIC_ORACLE_H
+#define FLOSIC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_problem orc_problem;
+
+orc_problem* orc_create(int natoms, const int* atom_type, const double* rat,
+                        int ntypes, const int* n_bare, const double* bfalp,
+                        const int* n_con, const double* bfcon,
+                        int nmsh, const double* rmsh, const double* wmsh,
+                        int nspn, int igga_x, int idftyp_x, int igga_c, int idftyp_c);
+void orc_destroy(orc_problem* p);
+int  orc_nbasis(const orc_problem* p);
+const char* orc_last_error(void);
+
+int orc_set_orbitals(orc_problem* p, const int* nwfs, const double* psi, int ldpsi,
+                     const int* nfrm, const double* bfrm, int ldfrm);
+
+/* gorbdrv.f:18 */
+int orc_gorbdrv(orc_problem* p, int nderv, int npts, const double* pts, int ifnct,
+                double* grad, int* iupdat, int* iallctr);
+
+/* frmorb2.F:146-346 (FRMORB2(0,0)): FMAT(ld, ld, 4, 2) */
+int orc_frmorb2_fmat(orc_problem* p, double* fmat, int ld);
+/* frmiorb.f:5 (FRMIORB(1,1)): TMAT(ld, ld, 2), LOWDEN eigenvalues EVAL(ld, 2) */
+int orc_frmiorb(orc_problem* p, double* tmat, double* lowden_eval, int ld);
+/* unravel2.f (MD=0/2): FO coefficients CFO(nbasis, nfrm(spin)) */
+int orc_fo_coefficients(orc_problem* p, int spin, double* cfo);
+
+/* coupot_sic.F:9 (serial branch) for FO iorb of spin: COULOMB(nmsh), RHOG(nmsh,10) */
+int orc_coupot_sic(orc_problem* p, int spin, int iorb, int exact,
+                   double* coulomb, double* rhog, long long* stats);
+/* getvlxc.F:8 serial branch with subvlxc_libxc.F90 (NSPN forced to 2 as in apotnl_sic.F:419) */
+int orc_getvlxc_sic(orc_problem* p, const double* rhog, double* vxc, double* ergs);
+/* apotnl_sic.F:31: RESULTS(13), CFRM(3), POT(nmsh) = V_xc + V_H (the ZPOT record) */
+int orc_apotnl_sic(orc_problem* p, int spin, int iorb, double* results, double* cfrm,
+                   double* pot, double* coulomb, double* rhog);
+/* frmorb_mpi.F:2/184 SICLAGM: SIC(ld, ld) from POT(nmsh, nfrm) */
+int orc_siclagm(orc_problem* p, int spin, const double* pots, double* sic, int ld);
+/* frmorb2.F:586-717: DEBDAX(3, ld) from SIC(ld, ld) */
+int orc_frmorb2_force(orc_problem* p, int spin, const double* sic, int ld, double* debdax);
+
+/* One SIC cycle (main.F:577-759): RESULTS(13,ld,2) SIC(ld,ld,2) DEBDAX(3,ld,2) CFRM(3,ld,2) */
+int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* debdax,
+                  double* cfrm, double* esic, int nthreads, int fo_limit);
+
+/* Pair-list statistics of coupot_sic.F for one FO: stats[0]=pairs kept, [1]=batches,
+   [2]=weird pairs, [3]=near (pair,point) evaluations, [4]=far (batch,point) evaluations */
+int orc_pair_stats(orc_problem* p, int spin, int iorb, long long* stats);
+
+/* Boys values as computed by fffmtc.F/fffmt4.F/fffmt3.F (maxfmt=5/4/3): s[5] */
+void orc_boys(int maxfmt, double x, double* s);
+/* harmonics.f: real spherical harmonics up to lm for a unit vector, y[(lm+1)^2] */
+void orc_harmonics(int lm, const double* xyz, double* y);
+/* lebedev.F degree-19 mesh (146 points): ang[3*146], w[146] */
+int orc_lebedev19(double* ang, double* w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

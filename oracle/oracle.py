@@ -1,0 +1,201 @@
+"""ctypes binding of the FP64 CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/liboracle_flosic.so, a restatement of the reference Fortran
+routines (see flosic_oracle.cpp).  Only tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline legs may import this module; the product package
+never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle_flosic.so")
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_int, _ip, _dp, C.c_int, _ip, _dp, _ip, _dp, C.c_int, _dp, _dp,
+                                 C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_nbasis.argtypes = [C.c_void_p]
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_set_orbitals.argtypes = [C.c_void_p, _ip, _dp, C.c_int, _ip, _dp, C.c_int]
+        L.orc_gorbdrv.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, _ip, _ip]
+        L.orc_frmorb2_fmat.argtypes = [C.c_void_p, _dp, C.c_int]
+        L.orc_frmiorb.argtypes = [C.c_void_p, _dp, _dp, C.c_int]
+        L.orc_fo_coefficients.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.orc_coupot_sic.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, _dp, _lp]
+        L.orc_getvlxc_sic.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.orc_apotnl_sic.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.orc_siclagm.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int]
+        L.orc_frmorb2_force.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp]
+        L.orc_sic_cycle.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_int]
+        L.orc_pair_stats.argtypes = [C.c_void_p, C.c_int, C.c_int, _lp]
+        L.orc_boys.argtypes = [C.c_int, C.c_double, _dp]
+        L.orc_harmonics.argtypes = [C.c_int, _dp, _dp]
+        L.orc_lebedev19.argtypes = [_dp, _dp]
+        _lib = L
+    return _lib
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc != 0:
+        raise OracleError(f"oracle error {rc}: {lib().orc_last_error().decode()}")
+
+
+class Oracle:
+    """FP64 restatement of the reference SIC path for one System."""
+
+    def __init__(self, sysm):
+        L = lib()
+        self.sysm = sysm
+        ix, idx, ic, idc = sysm.xc
+        self.h = L.orc_create(
+            sysm.natoms, np.ascontiguousarray(sysm.atom_type, dtype=np.int32),
+            np.ascontiguousarray(sysm.rat, dtype=np.float64), sysm.ntypes,
+            np.ascontiguousarray(sysm.n_bare, dtype=np.int32), np.ascontiguousarray(sysm.bfalp),
+            np.ascontiguousarray(sysm.n_con, dtype=np.int32), np.ascontiguousarray(sysm.bfcon),
+            sysm.nmsh, np.ascontiguousarray(sysm.rmsh), np.ascontiguousarray(sysm.wmsh),
+            sysm.nspn, ix, idx, ic, idc)
+        if not self.h:
+            raise OracleError(L.orc_last_error().decode())
+        self.nbasis = L.orc_nbasis(self.h)
+        self.ld = max(max(sysm.nfrm), 1)
+        if sysm.psi is not None:
+            self.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def set_orbitals(self, psi, nwfs, fods):
+        nf = np.array([len(f) for f in fods] + [0] * (2 - len(fods)), dtype=np.int32)
+        self.ld = max(int(nf.max()), 1)
+        bfrm = np.zeros((2, self.ld, 3))
+        for s, f in enumerate(fods):
+            bfrm[s, : len(f)] = f
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        _check(lib().orc_set_orbitals(self.h, np.array(nwfs, dtype=np.int32), psi, psi.shape[1], nf,
+                                      bfrm, self.ld))
+
+    def gorbdrv(self, nderv, pts, ifnct):
+        """pts (npts<=25, 3) relative to the atom; returns GRAD(25,10,6,15,3) as C array [3][15][6][10][25]."""
+        P = np.zeros((3, 25))
+        P[:, : len(pts)] = np.asarray(pts).T
+        grad = np.zeros(25 * 10 * 6 * 15 * 3)
+        iup = np.zeros(1, dtype=np.int32)
+        iall = np.zeros(45, dtype=np.int32)
+        _check(lib().orc_gorbdrv(self.h, nderv, len(pts), np.ascontiguousarray(P), ifnct, grad, iup, iall))
+        return grad.reshape(3, 15, 6, 10, 25), bool(iup[0]), iall.reshape(3, 15)
+
+    def fmat(self):
+        out = np.zeros(2 * 4 * self.ld * self.ld)
+        _check(lib().orc_frmorb2_fmat(self.h, out, self.ld))
+        return out.reshape(2, 4, self.ld, self.ld)   # [s][K][jfm][jwf]
+
+    def frmiorb(self):
+        tm = np.zeros(2 * self.ld * self.ld)
+        ev = np.zeros(2 * self.ld)
+        _check(lib().orc_frmiorb(self.h, tm, ev, self.ld))
+        return tm.reshape(2, self.ld, self.ld), ev.reshape(2, self.ld)  # tm[s][jwf][k] = TMAT(k,jwf,s)
+
+    def fo_coefficients(self, spin):
+        nf = self.sysm.nfrm[spin - 1]
+        out = np.zeros(nf * self.nbasis)
+        _check(lib().orc_fo_coefficients(self.h, spin, out))
+        return out.reshape(nf, self.nbasis)
+
+    def coupot_sic(self, spin, iorb, exact=False):
+        n = self.sysm.nmsh
+        coul = np.zeros(n)
+        rhog = np.zeros(10 * n)
+        st = np.zeros(5, dtype=np.int64)
+        _check(lib().orc_coupot_sic(self.h, spin, iorb, int(exact), coul, rhog, st))
+        return coul, rhog.reshape(10, n), st
+
+    def getvlxc_sic(self, rhog):
+        n = self.sysm.nmsh
+        vxc = np.zeros(2 * n)
+        ergs = np.zeros(4)
+        _check(lib().orc_getvlxc_sic(self.h, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1), vxc, ergs))
+        return vxc.reshape(2, n), ergs
+
+    def apotnl_sic(self, spin, iorb):
+        n = self.sysm.nmsh
+        res = np.zeros(13)
+        cf = np.zeros(3)
+        pot = np.zeros(n)
+        coul = np.zeros(n)
+        rhog = np.zeros(10 * n)
+        _check(lib().orc_apotnl_sic(self.h, spin, iorb, res, cf, pot, coul, rhog))
+        return dict(results=res, cfrm=cf, pot=pot, coulomb=coul, rhog=rhog.reshape(10, n))
+
+    def siclagm(self, spin, pots):
+        sic = np.zeros(self.ld * self.ld)
+        _check(lib().orc_siclagm(self.h, spin, np.ascontiguousarray(pots, dtype=np.float64), sic, self.ld))
+        return sic.reshape(self.ld, self.ld)   # [l][j] = SIC(j,l)
+
+    def frmorb2_force(self, spin, sic):
+        deb = np.zeros(3 * self.ld)
+        _check(lib().orc_frmorb2_force(self.h, spin, np.ascontiguousarray(sic, dtype=np.float64).reshape(-1),
+                                       self.ld, deb))
+        return deb.reshape(self.ld, 3)
+
+    def sic_cycle(self, nthreads=1, fo_limit=0):
+        ld = self.ld
+        res = np.zeros(2 * ld * 13)
+        sic = np.zeros(2 * ld * ld)
+        deb = np.zeros(2 * ld * 3)
+        cfrm = np.zeros(2 * ld * 3)
+        esic = np.zeros(1)
+        _check(lib().orc_sic_cycle(self.h, ld, res, sic, deb, cfrm, esic, nthreads, fo_limit))
+        return dict(results=res.reshape(2, ld, 13), sic=sic.reshape(2, ld, ld), debdax=deb.reshape(2, ld, 3),
+                    cfrm=cfrm.reshape(2, ld, 3), esic=float(esic[0]))
+
+    def pair_stats(self, spin=1, iorb=1):
+        st = np.zeros(5, dtype=np.int64)
+        _check(lib().orc_pair_stats(self.h, spin, iorb, st))
+        return dict(pairs=int(st[0]), batches=int(st[1]), weird=int(st[2]), near=int(st[3]), far=int(st[4]))
+
+
+def boys(maxfmt, x):
+    s = np.zeros(5)
+    lib().orc_boys(maxfmt, float(x), s)
+    return s
+
+
+def harmonics(lm, xyz):
+    y = np.zeros((lm + 1) ** 2)
+    lib().orc_harmonics(lm, np.ascontiguousarray(xyz, dtype=np.float64), y)
+    return y
+
+
+def lebedev19():
+    a = np.zeros(146 * 3)
+    w = np.zeros(146)
+    lib().orc_lebedev19(a, w)
+    return a.reshape(146, 3), w

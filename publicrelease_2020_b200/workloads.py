@@ -1,0 +1,388 @@
+"""Seeded synthetic inputs with the shapes of the FLO-SIC benchmark systems.
+
+The reference ships no kernel-level inputs (no mesh, no converged KS
+orbitals), so every system here is generated from a seed:
+
+* ``water``      -- O at the origin, H at (+-0.757, 0, 0.587) A, an
+  even-tempered basis with the NRLMOL default shapes (O: 13 bare primitives,
+  5s4p3d; H: 6 bare primitives, 4s3p1d; 73 functions), an atom-centred
+  radial x Lebedev mesh standing in for the variational mesh (vmesh.F), 5+5
+  FODs at a 1s + tetrahedral guess perturbed by N(0, 0.05 bohr).
+* ``synthetic``  -- N atoms uniform in a cube (min separation 1.8 bohr),
+  contracted Cartesian s/p/d functions with 3 primitives each (exponents
+  log-uniform in [0.05, 1e4]), jittered uniform mesh with weights summing to
+  the box volume, N_o FODs near the atoms.
+
+KS orbitals are random coefficient vectors orthonormalised in the mesh
+overlap metric S = B^T W B.  All arrays use the reference's Fortran layouts
+(BFALP(MAX_BARE,ntypes), BFCON(MAX_BARE,MAX_CON,3,ntypes), RMSH(3,nmsh),
+PSI(nbasis,nwf), BFRM(3,ld,2)); see modules2.F90:133-331 and modules.f90:206.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+MAX_BARE = 25
+MAX_CON = 15
+BOHR_PER_ANG = 1.0 / 0.529177210903
+
+# Cartesian components in the order of gorbdrv.f (s; x y z; xx yy zz xy xz yz)
+_POWS = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (0, 2, 0), (0, 0, 2),
+         (1, 1, 0), (1, 0, 1), (0, 1, 1)]
+_NCOMP = (1, 3, 6)
+_SHIFT = (0, 1, 4)
+
+# functional codes: (IGGA_x, IDFTYP_x, IGGA_c, IDFTYP_c) as set by setdftyp.F
+FUNCTIONALS = {
+    "LDA-PW91*LDA-PW91": (0, 6, 0, 6),
+    "GGA-PBE*GGA-PBE": (1, 7, 1, 7),
+    "GGA-PW91*GGA-PW91": (1, 6, 1, 6),
+}
+
+
+@dataclasses.dataclass
+class System:
+    name: str
+    rat: np.ndarray          # (natoms, 3)   bohr, atoms grouped by type
+    atom_type: np.ndarray    # (natoms,)     0-based type index
+    n_bare: np.ndarray       # (ntypes,)
+    bfalp: np.ndarray        # (ntypes, MAX_BARE)              == BFALP(MAX_BARE, ntypes)
+    n_con: np.ndarray        # (ntypes, 3)                     == N_CON(3, ntypes)
+    bfcon: np.ndarray        # (ntypes, 3, MAX_CON, MAX_BARE)  == BFCON(MAX_BARE, MAX_CON, 3, ntypes)
+    rmsh: np.ndarray         # (nmsh, 3)
+    wmsh: np.ndarray         # (nmsh,)
+    nspn: int
+    functional: str
+    psi: np.ndarray | None = None     # (nwf, nbasis) == PSI(nbasis, nwf)
+    nwfs: tuple = (0, 0)
+    fods: list = dataclasses.field(default_factory=list)  # per spin (nfrm, 3)
+
+    @property
+    def natoms(self):
+        return int(self.rat.shape[0])
+
+    @property
+    def ntypes(self):
+        return int(self.n_bare.shape[0])
+
+    @property
+    def nmsh(self):
+        return int(self.rmsh.shape[0])
+
+    def nloc(self, t):
+        return int(sum(_NCOMP[l] * self.n_con[t, l] for l in range(3)))
+
+    @property
+    def nbasis(self):
+        return int(sum(self.nloc(t) for t in self.atom_type))
+
+    @property
+    def xc(self):
+        return FUNCTIONALS[self.functional]
+
+    @property
+    def nfrm(self):
+        return tuple(len(f) for f in self.fods) + (0,) * (2 - len(self.fods))
+
+    def bfrm(self, ld=None):
+        """FOD positions as BFRM(3, ld, 2) (C order: [2][ld][3])."""
+        ld = ld or max(self.nfrm)
+        out = np.zeros((2, ld, 3))
+        for s, f in enumerate(self.fods):
+            out[s, : len(f)] = f
+        return out
+
+
+# ---------------------------------------------------------------------------
+# basis evaluation in numpy (input preparation only: overlap metric)
+# ---------------------------------------------------------------------------
+def basis_values(sysm: System, pts: np.ndarray) -> np.ndarray:
+    """Values of all contracted functions at pts, (npts, nbasis), local order
+    (l, component, contraction) per atom as in unravel2.f."""
+    cols = []
+    for a in range(sysm.natoms):
+        t = int(sysm.atom_type[a])
+        d = pts - sysm.rat[a]
+        r2 = np.einsum("ij,ij->i", d, d)
+        nb = int(sysm.n_bare[t])
+        alp = sysm.bfalp[t, :nb]
+        g = np.exp(-np.minimum(np.outer(r2, alp), 700.0))
+        g[np.outer(r2, alp) >= 40.0] = 0.0
+        for l in range(3):
+            nc = int(sysm.n_con[t, l])
+            if nc == 0:
+                continue
+            rad = g @ sysm.bfcon[t, l, :nc, :nb].T      # (npts, nc)
+            for mu in range(_NCOMP[l]):
+                px, py, pz = _POWS[_SHIFT[l] + mu]
+                ang = d[:, 0] ** px * d[:, 1] ** py * d[:, 2] ** pz
+                cols.append(rad * ang[:, None])
+    return np.concatenate(cols, axis=1)
+
+
+def mesh_overlap(sysm: System, chunk=100000) -> np.ndarray:
+    nb = sysm.nbasis
+    S = np.zeros((nb, nb))
+    for i0 in range(0, sysm.nmsh, chunk):
+        B = basis_values(sysm, sysm.rmsh[i0:i0 + chunk])
+        S += (B * sysm.wmsh[i0:i0 + chunk, None]).T @ B
+    return S
+
+
+def orthonormal_orbitals(sysm: System, nwf: int, rng) -> np.ndarray:
+    """nwf random orbitals orthonormal in S = B^T W B; returns (nwf, nbasis)."""
+    S = mesh_overlap(sysm)
+    nb = S.shape[0]
+    C = rng.standard_normal((nb, nwf))
+    M = C.T @ S @ C
+    w, U = np.linalg.eigh(M)
+    C = C @ (U / np.sqrt(w)) @ U.T
+    return np.ascontiguousarray(C.T)
+
+
+# ---------------------------------------------------------------------------
+# basis sets
+# ---------------------------------------------------------------------------
+def _even_tempered(nprim, amin, amax):
+    return np.geomspace(amax, amin, nprim)
+
+
+def _primitive_norm(alpha, l):
+    # normalisation of x^l exp(-a r^2) (axis component)
+    return (2 * alpha / math.pi) ** 0.75 * (4 * alpha) ** (l / 2) / math.sqrt(
+        float(np.prod([2 * k - 1 for k in range(1, l + 1)]) if l > 0 else 1.0)
+    )
+
+
+def _nrlmol_like_type(nprim, ncon, amin, amax, rng):
+    """General-contraction type: ncon[l] contractions over a shared set of
+    nprim bare primitives (the NRLMOL layout, PDF pp.14-16)."""
+    alp = _even_tempered(nprim, amin, amax)
+    con = np.zeros((3, MAX_CON, MAX_BARE))
+    for l in range(3):
+        for c in range(ncon[l]):
+            if c < ncon[l] - 1:
+                # contracted: coefficients over the tighter primitives
+                w = np.exp(-0.5 * ((np.arange(nprim) - (c * nprim) / max(ncon[l], 1)) / 2.0) ** 2)
+                w[nprim - ncon[l] + c + 1:] = 0.0
+            else:
+                # most diffuse function: a single primitive with coefficient 1 (times norm)
+                w = np.zeros(nprim)
+                w[nprim - 1 - (l > 0)] = 1.0
+            for i in range(nprim):
+                con[l, c, i] = w[i] * _primitive_norm(alp[i], l)
+    return alp, con
+
+
+def _pack_types(types):
+    nt = len(types)
+    n_bare = np.array([len(t[0]) for t in types], dtype=np.int32)
+    bfalp = np.zeros((nt, MAX_BARE))
+    bfcon = np.zeros((nt, 3, MAX_CON, MAX_BARE))
+    n_con = np.zeros((nt, 3), dtype=np.int32)
+    for i, (alp, con, ncon) in enumerate(types):
+        bfalp[i, : len(alp)] = alp
+        bfcon[i] = con
+        n_con[i] = ncon
+    return n_bare, bfalp, n_con, bfcon
+
+
+# ---------------------------------------------------------------------------
+# meshes
+# ---------------------------------------------------------------------------
+def lebedev146():
+    """Degree-19 Lebedev mesh (146 points, weights summing to 4 pi): published
+    Lebedev parameters as tabulated in lebedev.F:165-190."""
+    A1, A2, A3 = 0.00753519001311713812, 0.09265184700375432421, 0.09061000833610514010
+    B = (0.09518264418191036893, 0.08487112439121475736, 0.08942676055004592969)
+    AL = (0.15746766720390817632, 0.41749612279654533594, 0.67644104001142636987)
+    AM = (0.97488864367717323548, 0.80708981835958250163, 0.29129888220952674629)
+    D1, AR, AU, AW = 0.08785259467896816188, 0.14035538117131832857, 0.44933283232695573488, 0.88227001126032263192
+    pts, w = [], []
+    for i in range(3):
+        for s in (1, -1):
+            p = [0.0, 0.0, 0.0]
+            p[i] = s
+            pts.append(p)
+            w.append(A1)
+    r2 = 1 / math.sqrt(2)
+    for i in range(3):
+        for s1 in (1, -1):
+            for s2 in (1, -1):
+                p = [0.0, 0.0, 0.0]
+                p[(i + 1) % 3] = s1 * r2
+                p[(i + 2) % 3] = s2 * r2
+                pts.append(p)
+                w.append(A2)
+    r3 = 1 / math.sqrt(3)
+    for s1 in (1, -1):
+        for s2 in (1, -1):
+            for s3 in (1, -1):
+                pts.append([s1 * r3, s2 * r3, s3 * r3])
+                w.append(A3)
+    for g in range(3):
+        for i in range(3):
+            for s0 in (1, -1):
+                for s1 in (1, -1):
+                    for s2 in (1, -1):
+                        p = [0.0, 0.0, 0.0]
+                        p[i] = s0 * AM[g]
+                        p[(i + 1) % 3] = s1 * AL[g]
+                        p[(i + 2) % 3] = s2 * AL[g]
+                        pts.append(p)
+                        w.append(B[g])
+    import itertools
+    for perm in itertools.permutations((AR, AU, AW)):
+        for s in itertools.product((1, -1), repeat=3):
+            pts.append([s[0] * perm[0], s[1] * perm[1], s[2] * perm[2]])
+            w.append(D1)
+    return np.array(pts), np.array(w)
+
+
+def atom_centred_mesh(rat, nrad=40, rscale=None, seed=0):
+    """Becke-partitioned radial x Lebedev-146 mesh around each atom (stand-in
+    for the variational mesh of vmesh.F, which needs the Fortran build)."""
+    ang, wang = lebedev146()
+    rng = np.random.default_rng(seed)
+    pts, wts = [], []
+    nat = len(rat)
+    rscale = rscale or [1.0] * nat
+    for a in range(nat):
+        # Gauss-Chebyshev (second kind) radial grid mapped to (0, inf)
+        i = np.arange(1, nrad + 1)
+        x = np.cos(i * math.pi / (nrad + 1))
+        w_x = math.pi / (nrad + 1) * np.sin(i * math.pi / (nrad + 1)) ** 2 / np.sqrt(1 - x ** 2)
+        r = rscale[a] * (1 + x) / (1 - x)
+        dr = rscale[a] * 2 / (1 - x) ** 2
+        wr = w_x * dr * r ** 2
+        # random rotation of the angular grid per atom
+        q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        angr = ang @ q
+        p = (r[:, None, None] * angr[None, :, :]).reshape(-1, 3) + rat[a]
+        w = (wr[:, None] * wang[None, :]).reshape(-1)
+        # Becke fuzzy-cell weights
+        if nat > 1:
+            dist = np.linalg.norm(p[:, None, :] - rat[None, :, :], axis=2)
+            Rab = np.linalg.norm(rat[:, None] - rat[None, :], axis=2)
+            cell = np.ones((len(p), nat))
+            for A in range(nat):
+                for B in range(nat):
+                    if A == B:
+                        continue
+                    mu = (dist[:, A] - dist[:, B]) / Rab[A, B]
+                    f = mu
+                    for _ in range(3):
+                        f = 1.5 * f - 0.5 * f ** 3
+                    cell[:, A] *= 0.5 * (1 - f)
+            w = w * cell[:, a] / cell.sum(axis=1)
+        keep = w > 1e-14
+        pts.append(p[keep])
+        wts.append(w[keep])
+    return np.concatenate(pts), np.concatenate(wts)
+
+
+# ---------------------------------------------------------------------------
+# systems
+# ---------------------------------------------------------------------------
+def water(seed=0, nrad=40):
+    """C1: water, NRLMOL-shaped basis, 5+5 FODs, LDA-PW91*LDA-PW91, NSPN=2."""
+    rng = np.random.default_rng(seed)
+    b = BOHR_PER_ANG
+    rat = np.array([[0.0, 0.0, 0.0], [0.757 * b, 0.0, 0.587 * b], [-0.757 * b, 0.0, 0.587 * b]])
+    types = []
+    alp, con = _nrlmol_like_type(13, (5, 4, 3), 0.12, 6.0e4, rng)
+    types.append((alp, con, (5, 4, 3)))
+    alp, con = _nrlmol_like_type(6, (4, 3, 1), 0.08, 80.0, rng)
+    types.append((alp, con, (4, 3, 1)))
+    n_bare, bfalp, n_con, bfcon = _pack_types(types)
+    rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[0.7, 0.5, 0.5], seed=seed + 1)
+    sysm = System("water", rat, np.array([0, 1, 1], dtype=np.int32), n_bare, bfalp, n_con, bfcon,
+                  rmsh, wmsh, 2, "LDA-PW91*LDA-PW91")
+    nocc = 5
+    C = orthonormal_orbitals(sysm, 2 * nocc, rng)
+    sysm.psi = np.ascontiguousarray(np.concatenate([C[:nocc], C[nocc:]], axis=0))
+    sysm.nwfs = (nocc, nocc)
+    # FOD guess: 1s at O, two O-H bond points, two lone pairs (tetrahedral)
+    oh1 = 0.6 * rat[1]
+    oh2 = 0.6 * rat[2]
+    lp1 = np.array([0.0, 0.55, -0.45])
+    lp2 = np.array([0.0, -0.55, -0.45])
+    base = np.array([[0.0, 0.0, 0.0], oh1, oh2, lp1, lp2])
+    sysm.fods = [base + rng.normal(0, 0.05, base.shape), base + rng.normal(0, 0.05, base.shape)]
+    return sysm
+
+
+def synthetic(natoms=40, nbasis=512, nmsh=1_000_000, nfo=128, box_ang=12.0, seed=1,
+              functional="GGA-PBE*GGA-PBE", nspn=1, min_sep=1.8):
+    """C2-shaped synthetic system (one spin channel of nfo FOs by default)."""
+    rng = np.random.default_rng(seed)
+    L = box_ang * BOHR_PER_ANG
+    rat = []
+    while len(rat) < natoms:
+        p = rng.uniform(0.1 * L, 0.9 * L, 3)
+        if all(np.linalg.norm(p - q) >= min_sep for q in rat):
+            rat.append(p)
+    rat = np.array(rat)
+    # distribute nbasis functions over atoms: each atom gets s/p/d contractions
+    # (s:1 fn, p:3 fns, d:6 fns), 3 primitives per contraction (general contraction:
+    # contraction c of every l uses primitives 3c..3c+2 of the atom)
+    ncon = np.zeros((natoms, 3), dtype=np.int32)
+    ncon[:, 0] = 1
+    total = natoms
+    order = rng.permutation(natoms)
+    k = 0
+    while total < nbasis:
+        a = order[k % natoms]
+        rem = nbasis - total
+        choice = rng.choice([0, 1, 2], p=[0.3, 0.45, 0.25])
+        size = (1, 3, 6)[choice]
+        if size > rem:
+            choice, size = 0, 1
+        if ncon[a, choice] < 4:
+            ncon[a, choice] += 1
+            total += size
+        k += 1
+    types = []
+    for a in range(natoms):
+        nc = ncon[a]
+        nprim = 3 * int(nc.max())
+        alp = np.sort(np.exp(rng.uniform(math.log(0.05), math.log(1.0e4), nprim)))[::-1]
+        con = np.zeros((3, MAX_CON, MAX_BARE))
+        for l in range(3):
+            for c in range(nc[l]):
+                for j in range(3):
+                    i = 3 * c + j
+                    con[l, c, i] = rng.uniform(0.3, 1.0) * _primitive_norm(alp[i], l)
+        types.append((alp, con, tuple(int(x) for x in nc)))
+    n_bare, bfalp, n_con, bfcon = _pack_types(types)
+    # jittered uniform mesh, weights summing to the box volume
+    n1 = int(round(nmsh ** (1 / 3)))
+    while n1 ** 3 < nmsh:
+        n1 += 1
+    h = L / n1
+    idx = np.stack(np.meshgrid(*[np.arange(n1)] * 3, indexing="ij"), -1).reshape(-1, 3)[:nmsh]
+    rmsh = (idx + 0.5 + rng.uniform(-0.35, 0.35, idx.shape)) * h
+    wmsh = rng.uniform(0.5, 1.5, nmsh)
+    wmsh *= L ** 3 / wmsh.sum()
+    sysm = System("synthetic", rat, np.arange(natoms, dtype=np.int32), n_bare, bfalp, n_con, bfcon,
+                  rmsh, wmsh, nspn, functional)
+    nb = sysm.nbasis
+    assert nb == nbasis, (nb, nbasis)
+    C = orthonormal_orbitals(sysm, nfo * nspn, rng)
+    sysm.psi = C
+    sysm.nwfs = (nfo, nfo if nspn == 2 else 0)
+    fods = []
+    for s in range(nspn):
+        at = rng.integers(0, natoms, nfo)
+        fods.append(rat[at] + rng.normal(0, 0.6, (nfo, 3)))
+    sysm.fods = fods
+    return sysm
+
+
+def small_synthetic(seed=5, natoms=3, nbasis=24, nmsh=6000, nfo=4, functional="GGA-PBE*GGA-PBE", nspn=1):
+    """Seconds-sized synthetic system for parity tests."""
+    return synthetic(natoms=natoms, nbasis=nbasis, nmsh=nmsh, nfo=nfo, box_ang=4.0, seed=seed,
+                     functional=functional, nspn=nspn, min_sep=1.8)

@@ -1,0 +1,129 @@
+/*
+ * libflosic_sic_b200 -- B200 (sm_100a) implementation of the FLO-SIC
+ * per-Fermi-orbital self-interaction-correction hot path.
+ *
+ * Drop-in boundary.  Each entry point replaces one reference Fortran routine
+ * (FLOSIC/PublicRelease_2020, directory flosic/) on the SIC path; the Fortran
+ * host keeps mesh generation, the SCF loop and the eigensolvers and calls
+ * these functions through thin iso_c_binding shims.  The reference routines
+ * read their inputs from Fortran modules; here the module arrays a routine
+ * reads are passed once (flosic_sic_set_geometry / flosic_sic_set_orbitals)
+ * and kept resident in GPU memory.
+ *
+ * Conventions
+ *   - every function returns 0 on success and a nonzero FLOSIC_ERR_* code on
+ *     failure; nothing here calls exit() or abort().  The Fortran shim maps a
+ *     nonzero status to STOPIT, as the reference does on the same conditions.
+ *   - arrays are Fortran column-major with the reference's leading dimensions;
+ *     spins and orbital indices are 1-based where the reference's are.
+ *   - one context binds one CUDA device; calls on a context are serialised on
+ *     the context's stream and return after results are in host memory.
+ */
+#ifndef FLOSIC_SIC_H
+#define FLOSIC_SIC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FLOSIC_OK = 0,
+  FLOSIC_ERR_ARG = 1,           /* invalid argument / size                       */
+  FLOSIC_ERR_CAPACITY = 2,      /* a static capacity (MAX_BARE, MAX_CON, ...)    */
+  FLOSIC_ERR_LOWDEN = 3,        /* Lowdin eigenvalue < 1e-8 (lowden_files.f:71)  */
+  FLOSIC_ERR_ZERO_DENSITY = 4,  /* zero density at an FOD                        */
+  FLOSIC_ERR_NFRM = 5,          /* MORB .NE. NFRM (frmiorb.f:418)                */
+  FLOSIC_ERR_ZERO_COULOMB = 6,  /* "COUPOT IS ZERO" (apotnl_sic.F:277-283)       */
+  FLOSIC_ERR_CUDA = 7,          /* CUDA / cuBLAS failure                         */
+  FLOSIC_ERR_STATE = 8          /* call order: geometry/orbitals not set         */
+};
+
+/* Static capacities shared with the reference (PARAMA2). */
+#define FLOSIC_MAX_BARE 25
+#define FLOSIC_MAX_CON 15
+#define FLOSIC_NSPEED 25
+
+typedef struct flosic_ctx flosic_ctx;
+
+/* Context management (no reference counterpart: replaces the MPI job farm
+   set up in cpuhog.F / senddata.F for these routines). */
+int flosic_sic_create(int device, flosic_ctx** ctx);
+int flosic_sic_destroy(flosic_ctx* ctx);
+const char* flosic_sic_last_error(void);
+
+/* Module state read by the SIC routines (modules2.F90:133-244 common2,
+   modules.f90:206-218 mesh1).  Atoms are given in the reference order
+   (function set IFNCT outer, position I_POS inner); atom_type is the 1-based
+   IFNCT of each atom.
+     RAT(3,natoms) BFALP(25,ntypes) BFCON(25,15,3,ntypes) N_BARE(ntypes)
+     N_CON(3,ntypes) RMSH(3,nmsh) WMSH(nmsh)
+   Functional: IGGA(2), IDFTYP(2) as set by SETDFTYP (setdftyp.F:61-105);
+   supported: exchange PW91/PBE/revPBE/RPBE (LDA via IGGA=0), correlation
+   PW91/PBE.  nspn = NSPN of the run (1 or 2). */
+int flosic_sic_set_geometry(flosic_ctx* ctx, int natoms, const int32_t* atom_type, const double* rat,
+                            int ntypes, const int32_t* n_bare, const double* bfalp,
+                            const int32_t* n_con, const double* bfcon, int nmsh, const double* rmsh,
+                            const double* wmsh, int nspn, const int32_t* igga, const int32_t* idftyp);
+
+/* KS orbitals and FODs (common5 PSI_COEF/PSI after UNRAVEL for C1 symmetry,
+   modules_sic.F90 FRM BFRM).  PSI(ldpsi, nwfs(1)+nwfs(2)): spin-1 orbitals
+   first, basis order per atom (l, Cartesian component, contraction) as in
+   unravel2.f:160-175.  BFRM(3, ldfrm, 2). */
+int flosic_sic_set_orbitals(flosic_ctx* ctx, const int32_t* nwfs, const double* psi, int ldpsi,
+                            const int32_t* nfrm, const double* bfrm, int ldfrm);
+
+/* GORBDRV(NDERV,IUPDAT,IALLCTR,NPTS,PTS,IFNCT,GRAD)  -- gorbdrv.f:18.
+   PTS(25,3) relative to the atom, GRAD(25,10,6,15,3), IALLCTR(15,3). */
+int flosic_sic_gorbdrv(flosic_ctx* ctx, int nderv, int32_t* iupdat, int32_t* iallctr, int npts,
+                       const double* pts, int ifnct, double* grad);
+
+/* FRMORB2(0,0) -- frmorb2.F:146-346: FMAT(ld,ld,4,2) of the FO values and
+   their FOD derivatives at the FODs. */
+int flosic_sic_frmorb2_fmat(flosic_ctx* ctx, double* fmat, int ld);
+
+/* FRMIORB(1,1) -- frmiorb.f:5: TMAT(ld,ld,2) (Lowdin-orthonormalised Fermi
+   transformation) and the Lowdin overlap eigenvalues EVAL(ld,2). */
+int flosic_sic_frmiorb(flosic_ctx* ctx, double* tmat, double* eval, int ld);
+
+/* COUPOT_SIC(MXXD=0,KXXS,KXXO) -- coupot_sic.F:9: Coulomb potential COULOMB(nmsh)
+   of the density of FO kxxo of spin kxxs, and that density RHOG(nmsh,10). */
+int flosic_sic_coupot_sic(flosic_ctx* ctx, int kxxs, int kxxo, double* coulomb, double* rhog);
+
+/* GETVLXC(NDIM,RHOG,VXC,VLO,.false.,...) SIC branch -- getvlxc.F:8 with NSPN=2
+   (apotnl_sic.F:419): VXC(2*ndim) and ERGXL,ERGXN,ERGCL,ERGCN in ergs[4]. */
+int flosic_sic_getvlxc(flosic_ctx* ctx, int ndim, const double* rhog, double* vxc, double* ergs);
+
+/* APOTNL_SIC(TOTQNUM,LSPX,IORBX) -- apotnl_sic.F:31: RESULTS(13) and CFRM(3) of
+   FO iorbx, and its SIC potential POT(nmsh) = V_xc + V_H (the ZPOT record).
+   The potential also stays in GPU memory for flosic_sic_siclagm. */
+int flosic_sic_apotnl_sic(flosic_ctx* ctx, double* totqnum, int lspx, int iorbx, double* results,
+                          double* cfrm, double* pot);
+
+/* SICLAGM(LSPN) -- frmorb_mpi.F:2: SIC(ld,ld) = -<phi_j|V_l|phi_l> from the
+   potentials of the FOs of spin lspn (kept in GPU memory instead of the
+   ZPOT#### files). */
+int flosic_sic_siclagm(flosic_ctx* ctx, int lspn, double* sic, int ld);
+
+/* FRMORB2(-LSPN,-1) -- frmorb2.F:586-717: FOD forces DEBDAX(3,ld) from SIC(ld,ld). */
+int flosic_sic_frmorb2_force(flosic_ctx* ctx, int lspn, const double* sic, int ld, double* debdax);
+
+/* One SIC block of an SCF iteration (main.F:577-759): FRMORB2(0,0), FRMIORB(1,1),
+   APOTNL_SIC for every FO of every spin, SICLAGM and FRMORB2(-s,-1), all FOs of a
+   spin batched in the same launches.  RESULTS(13,ld,2) SIC(ld,ld,2) DEBDAX(3,ld,2)
+   CFRM(3,ld,2); esic = ZSIC = sum of RESULTS(9,:,:). */
+int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, double* debdax,
+                     double* cfrm, double* esic);
+
+/* Timing/introspection (no reference counterpart): number of kernels launched by
+   the last flosic_sic_cycle, per-stage device milliseconds of the last cycle
+   (ms[0]=FO construction, [1]=orbital/density, [2]=Coulomb setup, [3]=Coulomb
+   evaluation, [4]=XC+energies, [5]=SIC matrix, [6]=forces), pair/call counts. */
+int flosic_sic_stats(flosic_ctx* ctx, int64_t* launches, double* stage_ms, int64_t* npairs,
+                     int64_t* ncalls);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLOSIC_SIC_H */

@@ -2316,6 +2316,24 @@ int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* 
   return 0;
 }
 
+int orc_xc_point(int igga_x, int idftyp_x, int igga_c, int idftyp_c, const double* r10, double w, double* v2,
+                 double* e4) {
+  Problem P;
+  P.igga[0] = igga_x;
+  P.igga[1] = igga_c;
+  P.idftyp[0] = idftyp_x;
+  P.idftyp[1] = idftyp_c;
+  double rht[2][10];
+  for (int k = 0; k < 10; ++k) {
+    rht[0][k] = r10[k];
+    rht[1][k] = 0.0;
+  }
+  v2[0] = v2[1] = 0.0;
+  for (int i = 0; i < 4; ++i) e4[i] = 0.0;
+  subvlxc_point(P, rht, w, v2, e4);
+  return 0;
+}
+
 void orc_boys(int maxfmt, double x, double* s) { boys(maxfmt, x, std::exp(-x), s); }
 void orc_harmonics(int lm, const double* xyz, double* y) { harmonics(lm, xyz[0], xyz[1], xyz[2], y); }
 int orc_lebedev19(double* ang, double* w) {

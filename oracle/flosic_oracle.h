@@ -73,6 +73,12 @@ int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* 
    [2]=weird pairs, [3]=near (pair,point) evaluations, [4]=far (batch,point) evaluations */
 int orc_pair_stats(orc_problem* p, int spin, int iorb, long long* stats);
 
+/* One mesh point of SUBVLXC (subvlxc_libxc.F90) with NSPN=2 and zero spin-down
+   density: r10 = total-density channels; v2 = spin-up/down potentials; e4 =
+   weighted EXL, EXN, ECL, ECN. */
+int orc_xc_point(int igga_x, int idftyp_x, int igga_c, int idftyp_c, const double* r10, double w,
+                 double* v2, double* e4);
+
 /* Boys values as computed by fffmtc.F/fffmt4.F/fffmt3.F (maxfmt=5/4/3): s[5] */
 void orc_boys(int maxfmt, double x, double* s);
 /* harmonics.f: real spherical harmonics up to lm for a unit vector, y[(lm+1)^2] */

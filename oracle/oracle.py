@@ -50,6 +50,7 @@ def lib():
         L.orc_frmorb2_force.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp]
         L.orc_sic_cycle.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_int]
         L.orc_pair_stats.argtypes = [C.c_void_p, C.c_int, C.c_int, _lp]
+        L.orc_xc_point.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_double, _dp, _dp]
         L.orc_boys.argtypes = [C.c_int, C.c_double, _dp]
         L.orc_harmonics.argtypes = [C.c_int, _dp, _dp]
         L.orc_lebedev19.argtypes = [_dp, _dp]
@@ -180,6 +181,14 @@ class Oracle:
         st = np.zeros(5, dtype=np.int64)
         _check(lib().orc_pair_stats(self.h, spin, iorb, st))
         return dict(pairs=int(st[0]), batches=int(st[1]), weird=int(st[2]), near=int(st[3]), far=int(st[4]))
+
+
+def xc_point(xc, r10, w=1.0):
+    """(IGGA_x, IDFTYP_x, IGGA_c, IDFTYP_c), density channels -> (v_up, v_dn), (EXL, EXN, ECL, ECN)."""
+    v = np.zeros(2)
+    e = np.zeros(4)
+    lib().orc_xc_point(xc[0], xc[1], xc[2], xc[3], np.ascontiguousarray(r10, dtype=np.float64), float(w), v, e)
+    return v, e
 
 
 def boys(maxfmt, x):

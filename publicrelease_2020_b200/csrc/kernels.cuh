@@ -1,0 +1,77 @@
+// Kernel declarations and device-side data descriptors.
+#pragma once
+
+#include "common.cuh"
+
+namespace flosic {
+
+// Basis tables in device memory (general-contraction NRLMOL layout).
+struct BasisDev {
+  int natoms, ntypes, nbasis, nprim;
+  const double* atom_pos;    // 3*natoms
+  const int* atom_type;      // natoms
+  const int* atom_boff;      // natoms: first basis function of the atom
+  const int* atom_poff;      // natoms: first global primitive of the atom
+  const int* type_nbare;     // ntypes
+  const int* type_lmax;      // ntypes
+  const int* type_ncon;      // 3*ntypes
+  const double* type_alpha;  // MAX_BARE*ntypes
+  const double* type_amin;   // ntypes: smallest exponent
+  const double* type_bfcon;  // ((t*3+l)*MAX_CON+c)*MAX_BARE+ib
+  const int* prim_atom;      // nprim: atom of each global primitive
+  const int* prim_ib;        // nprim: bare index inside the atom type
+};
+
+struct MeshDev {
+  int n, ntiles;
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* w;
+  const double* tile_lo;  // 3*ntiles
+  const double* tile_hi;  // 3*ntiles
+};
+
+// Basis values (nderv 0,1,2 -> 1,4,10 channels) of all functions at npts points
+// (px,py,pz SoA).  out[(ch*nbasis + b)*ldo + i].
+void launch_basis_values(const BasisDev& B, int nderv, int npts, const double* px, const double* py,
+                         const double* pz, double* out, int ldo, cudaStream_t st);
+
+// u[(k*nprim + gp)*10 + comp] = sum_con BFCON(ib,con,l(comp)) C(k, local(l,comp,con))
+void launch_prim_u(const BasisDev& B, int nfo, const double* cfo, int ldc, double* u, cudaStream_t st);
+
+// Per (pair, FO): 46 potential coefficients, Boys variant, centre-of-gravity partials.
+void launch_pair_coef(int npairs, const PairGeo* pairs, const CallInfo* calls, int nfo, int nprim,
+                      const double* u, int nspn, double* coef, int8_t* maxfmt, double* cgp,
+                      cudaStream_t st);
+
+// Per (call, FO): CG, RCUT, NPOT, multipole moments.
+void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, int nspn,
+                       const double* coef, const int8_t* maxfmt, const double* cgp, const MeshDev& M,
+                       const double* boys_tab, CallFO* cfo, double* mom, cudaStream_t st);
+
+// Coulomb potential of every FO at every mesh point: vh[k*ldv + p].
+void launch_coulomb_eval(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo,
+                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* mom,
+                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, cudaStream_t st);
+
+// Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as
+// in apotnl_sic.F:419) from the FO values/derivatives phi[(ch*nfo+k)*ldp+p];
+// writes the SIC potential V = Vxc + VH*nspn/2 and Y = w V phi, and per-block
+// energy partial sums part[(k*nblk + blk)*NPART + j].
+constexpr int NPART = 11;
+void launch_xc(const MeshDev& M, int nfo, int gga, int nspn, const int* xc, const double* phi, int ldp,
+               double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st);
+void launch_reduce_parts(int nfo, int nblk, const double* part, double* sums, cudaStream_t st);
+
+// FO density channels of one FO: rhog[ch*ldr + p] (10 channels for GGA).
+void launch_density(int npts, int nfo, int k, int gga, const double* phi, int ldp, double* rhog, int ldr,
+                    cudaStream_t st);
+
+// Vxc of given density channels (GETVLXC entry point): vxc[2*n], parts as above (1 FO).
+void launch_xc_rhog(const MeshDev& M, int gga, const int* xc, const double* rhog, int ldr, double* vxc,
+                    double* part, int nblk, cudaStream_t st);
+
+void upload_constants(const double* leb_ang, const double* leb_w);
+
+}  // namespace flosic

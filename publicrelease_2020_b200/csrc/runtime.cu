@@ -1,0 +1,1413 @@
+// Host runtime and C ABI of libflosic_sic_b200.
+//
+// The context keeps the module state of the reference SIC routines resident
+// on one GPU: basis tables, the mesh (sorted into spatial tiles), the
+// Gaussian-pair plan of COUPOT_SIC (coupot_sic.F:228-640, built once per
+// geometry in the reference's serial batching order), KS orbitals and FODs.
+// A spin's FO potentials are computed for all FOs in batched launches and
+// cached in GPU memory; APOTNL_SIC / SICLAGM / FRMORB2 entry points read from
+// that cache instead of the ZPOT#### files.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/flosic_sic.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace flosic;
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Fail {
+  int code;
+};
+
+[[noreturn]] void fail(int code, const std::string& msg) {
+  g_err = msg;
+  throw Fail{code};
+}
+
+#define CUDA_CHECK(x)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess) fail(FLOSIC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define BLAS_CHECK(x)                                                              \
+  do {                                                                             \
+    cublasStatus_t s_ = (x);                                                       \
+    if (s_ != CUBLAS_STATUS_SUCCESS) fail(FLOSIC_ERR_CUDA, std::string(#x) + " failed"); \
+  } while (0)
+
+const int kNcomp[3] = {1, 3, 6};
+const int kShift[3] = {0, 1, 4};
+const int kPow[10][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0},
+                         {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void ensure(size_t m) {
+    if (m <= n && p) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (m == 0) return;
+    CUDA_CHECK(cudaMalloc(&p, sizeof(T) * m));
+    n = m;
+  }
+  void upload(const T* h, size_t m, cudaStream_t st) {
+    ensure(m);
+    if (m) CUDA_CHECK(cudaMemcpyAsync(p, h, sizeof(T) * m, cudaMemcpyHostToDevice, st));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// small dense symmetric eigen-solver (cyclic Jacobi) for the Lowdin step
+// (the role of DIAGGE_FO, diagon_sic.f:45); a: n*n row-major, v columns.
+// ---------------------------------------------------------------------------
+void sym_eigen(int n, std::vector<double> a, std::vector<double>& w, std::vector<double>& v) {
+  v.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) v[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        double x = a[(size_t)i * n + j] * a[(size_t)i * n + j];
+        tot += x;
+        if (i != j) off += x;
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          const double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
+          a[(size_t)k * n + p] = c * akp - s * akq;
+          a[(size_t)k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
+          a[(size_t)p * n + k] = c * apk - s * aqk;
+          a[(size_t)q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = v[(size_t)k * n + p], vkq = v[(size_t)k * n + q];
+          v[(size_t)k * n + p] = c * vkp - s * vkq;
+          v[(size_t)k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  w.resize(n);
+  for (int i = 0; i < n; ++i) w[i] = a[(size_t)i * n + i];
+}
+
+// LOWSIC (lowden_files.f:2-172): returns S^{-1/2} (row-major), eigenvectors
+// (filo[i*n+a]) and eigenvalues lambda.
+void lowsic(int n, const std::vector<double>& over, std::vector<double>& sm12, std::vector<double>& filo,
+            std::vector<double>& lam) {
+  std::vector<double> w;
+  sym_eigen(n, over, w, filo);
+  for (int i = 0; i < n; ++i)
+    if (w[i] < 1.0e-8)
+      fail(FLOSIC_ERR_LOWDEN, "LOWSIC: LOWDEN EIGENVALUES TOO SMALL (< 1e-8): BAD POSITIONS IN FRMORB");
+  std::vector<double> e(n);
+  for (int i = 0; i < n; ++i) e[i] = 1.0 / std::sqrt(w[i]);
+  lam.resize(n);
+  for (int i = 0; i < n; ++i) lam[i] = 1.0 / (e[i] * e[i]);
+  sm12.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double s = 0.0;
+      for (int m = 0; m < n; ++m) s += filo[(size_t)j * n + m] * filo[(size_t)i * n + m] * e[m];
+      sm12[(size_t)i * n + j] = s;
+    }
+}
+
+// Boys-function table of fffmtc.F:25-97 (series for F_19, downward recursion),
+// columns F2 F3 F4 F5 F4/2 F5/2 F6/2 F5/6 F6/6 F7/6.
+std::vector<double> boys_table() {
+  std::vector<double> T((size_t)BOYS_NT * BOYS_NC);
+  for (int L = 1; L <= BOYS_NT; ++L) {
+    double F[10];
+    if (L == 1) {
+      for (int i = 0; i < 10; ++i) F[i] = 1.0 / (2 * (i + 1) - 1);
+    } else {
+      const double t = (1.0e-2) * (L - 1);
+      const double x = 2 * t;
+      double den = 39.0, term = 1.0 / den, sum = term;
+      for (int i = 2; i <= 100; ++i) {
+        den = den + 2.0;
+        term = term * x / den;
+        sum = sum + term;
+        if (term / sum - 1.0e-12 <= 0) break;
+      }
+      const double ex = std::exp(-t);
+      double G[21];
+      G[20] = ex * sum;
+      for (int i = 1; i <= 19; ++i) {
+        const int K = 21 - i, KK = K - 1;
+        G[KK] = (x * G[K] + ex) / (2 * KK - 1);
+      }
+      for (int i = 0; i < 10; ++i) F[i] = G[i + 1];
+    }
+    double* r = &T[(size_t)(L - 1) * BOYS_NC];
+    r[0] = F[2];
+    r[1] = F[3];
+    r[2] = F[4];
+    r[3] = F[5];
+    r[4] = F[4] / 2.0;
+    r[5] = F[5] / 2.0;
+    r[6] = F[6] / 2.0;
+    r[7] = F[5] / 6.0;
+    r[8] = F[6] / 6.0;
+    r[9] = F[7] / 6.0;
+  }
+  return T;
+}
+
+// Lebedev degree-19 mesh in the generation order of lebedev.F:741-905.
+void lebedev19(std::vector<double>& ang, std::vector<double>& w) {
+  const double RT2RC = 0.70710678118654752440, RT3RC = 0.57735026918962576451;
+  const double A1 = 0.00753519001311713812, A2 = 0.09265184700375432421, A3 = 0.09061000833610514010;
+  const double B[3] = {0.09518264418191036893, 0.08487112439121475736, 0.08942676055004592969};
+  const double AL[3] = {0.15746766720390817632, 0.41749612279654533594, 0.67644104001142636987};
+  const double AM[3] = {0.97488864367717323548, 0.80708981835958250163, 0.29129888220952674629};
+  const double D1 = 0.08785259467896816188, AR1 = 0.14035538117131832857, AU1 = 0.44933283232695573488,
+               AW1 = 0.88227001126032263192;
+  ang.clear();
+  w.clear();
+  auto push = [&](double x, double y, double z, double wt) {
+    ang.push_back(x);
+    ang.push_back(y);
+    ang.push_back(z);
+    w.push_back(wt);
+  };
+  double sg[3];
+  for (int i = 0; i < 3; ++i) {
+    sg[0] = 1.0;
+    for (int j = 0; j < 2; ++j) {
+      double p[3] = {0, 0, 0};
+      p[i] = sg[0];
+      push(p[0], p[1], p[2], A1);
+      sg[0] = -sg[0];
+    }
+  }
+  for (int i = 0; i < 3; ++i) {
+    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+    sg[0] = RT2RC;
+    for (int j = 0; j < 2; ++j) {
+      sg[1] = RT2RC;
+      for (int k = 0; k < 2; ++k) {
+        double p[3];
+        p[i] = 0.0;
+        p[i1] = sg[0];
+        p[i2] = sg[1];
+        push(p[0], p[1], p[2], A2);
+        sg[1] = -sg[1];
+      }
+      sg[0] = -sg[0];
+    }
+  }
+  sg[0] = RT3RC;
+  for (int i = 0; i < 2; ++i) {
+    sg[1] = RT3RC;
+    for (int j = 0; j < 2; ++j) {
+      sg[2] = RT3RC;
+      for (int k = 0; k < 2; ++k) {
+        push(sg[0], sg[1], sg[2], A3);
+        sg[2] = -sg[2];
+      }
+      sg[1] = -sg[1];
+    }
+    sg[0] = -sg[0];
+  }
+  for (int g = 0; g < 3; ++g) {
+    for (int i = 0; i < 3; ++i) {
+      const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+      sg[i] = AM[g];
+      for (int j = 0; j < 2; ++j) {
+        sg[i1] = AL[g];
+        for (int k = 0; k < 2; ++k) {
+          sg[i2] = AL[g];
+          for (int l = 0; l < 2; ++l) {
+            push(sg[0], sg[1], sg[2], B[g]);
+            sg[i2] = -sg[i2];
+          }
+          sg[i1] = -sg[i1];
+        }
+        sg[i] = -sg[i];
+      }
+    }
+  }
+  for (int i = 0; i < 3; ++i) {
+    sg[i] = AR1;
+    for (int j = 0; j < 2; ++j) {
+      int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+      for (int k = 0; k < 2; ++k) {
+        sg[i1] = AU1;
+        for (int l = 0; l < 2; ++l) {
+          sg[i2] = AW1;
+          for (int m = 0; m < 2; ++m) {
+            push(sg[0], sg[1], sg[2], D1);
+            sg[i2] = -sg[i2];
+          }
+          sg[i1] = -sg[i1];
+        }
+        std::swap(i1, i2);
+      }
+      sg[i] = -sg[i];
+    }
+  }
+}
+
+struct TypeInfo {
+  int nbare, lmax, nloc;
+  int ncon[3];
+  double alp[MAX_BARE];
+  double con[3][MAX_CON][MAX_BARE];
+};
+
+struct SpinCache {
+  bool fo_valid = false;       // FMAT/TMAT/CFO
+  bool pot_valid = false;      // potentials, RESULTS
+  int nf = 0, nw = 0;
+  std::vector<double> fmat;    // [(K*nf + jfm)*nw + jwf]
+  std::vector<double> tmat;    // [k*nw + jwf]
+  std::vector<double> lam;     // Lowdin eigenvalues
+  std::vector<double> results; // [k*13 + i]
+  std::vector<double> cfrm;    // [k*3 + d]
+  std::vector<double> sic;     // [l*nf + j] = SIC(j,l)
+  bool sic_valid = false;
+  DevBuf<double> cfo;          // nb x nf
+  DevBuf<double> phi;          // [ch][k][P]
+  DevBuf<double> vh;           // raw Coulomb [k][P]
+  DevBuf<double> vpot;         // SIC potential [k][P]
+  DevBuf<double> y;            // w V phi [k][P]
+  void release() {
+    cfo.release();
+    phi.release();
+    vh.release();
+    vpot.release();
+    y.release();
+  }
+};
+
+}  // namespace
+
+struct flosic_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cublasHandle_t blas = nullptr;
+  bool have_geom = false, have_orb = false;
+  // geometry
+  int natoms = 0, ntypes = 0, nbasis = 0, nprim = 0, nmsh = 0, nspn = 1, gga = 0;
+  int xc[4] = {0, 6, 0, 6};
+  std::vector<TypeInfo> types;
+  std::vector<int> atype, aoff, apoff;
+  std::vector<double> rat;
+  std::vector<int> perm;       // sorted index -> original index
+  int ntiles = 0;
+  int ifar_sorted = 0;         // farthest point from the origin (apotnl_sic.F:410-418)
+  double rmx = 0.0;
+  std::vector<PairGeo> pairs;
+  std::vector<CallInfo> calls;
+  // device geometry
+  DevBuf<double> d_atom_pos, d_type_alpha, d_type_amin, d_type_bfcon;
+  DevBuf<int> d_atom_type, d_atom_boff, d_atom_poff, d_type_nbare, d_type_lmax, d_type_ncon, d_prim_atom,
+      d_prim_ib;
+  DevBuf<double> d_x, d_y, d_z, d_w, d_tlo, d_thi, d_boys;
+  DevBuf<PairGeo> d_pairs;
+  DevBuf<CallInfo> d_calls;
+  // orbitals
+  int nwfs[2] = {0, 0}, nfrm[2] = {0, 0};
+  std::vector<double> psi;     // nb x nwf (column-major)
+  std::vector<double> fods[2];
+  DevBuf<double> d_psi, d_psi_thr;
+  SpinCache spin[2];
+  // scratch
+  DevBuf<double> d_basis, d_fodpts, d_psig, d_tmat, d_u, d_coef, d_cgp, d_mom, d_part, d_sums, d_sic, d_tmp;
+  DevBuf<int8_t> d_maxfmt;
+  DevBuf<CallFO> d_callfo;
+  // stats
+  long long launches = 0;
+  double stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  cudaEvent_t ev[8] = {};
+
+  BasisDev basis_dev() const {
+    BasisDev B;
+    B.natoms = natoms;
+    B.ntypes = ntypes;
+    B.nbasis = nbasis;
+    B.nprim = nprim;
+    B.atom_pos = d_atom_pos.p;
+    B.atom_type = d_atom_type.p;
+    B.atom_boff = d_atom_boff.p;
+    B.atom_poff = d_atom_poff.p;
+    B.type_nbare = d_type_nbare.p;
+    B.type_lmax = d_type_lmax.p;
+    B.type_ncon = d_type_ncon.p;
+    B.type_alpha = d_type_alpha.p;
+    B.type_amin = d_type_amin.p;
+    B.type_bfcon = d_type_bfcon.p;
+    B.prim_atom = d_prim_atom.p;
+    B.prim_ib = d_prim_ib.p;
+    return B;
+  }
+  MeshDev mesh_dev() const {
+    MeshDev M;
+    M.n = nmsh;
+    M.ntiles = ntiles;
+    M.x = d_x.p;
+    M.y = d_y.p;
+    M.z = d_z.p;
+    M.w = d_w.p;
+    M.tile_lo = d_tlo.p;
+    M.tile_hi = d_thi.p;
+    return M;
+  }
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Pair plan of COUPOT_SIC (coupot_sic.F:149-790), geometry only.
+// ---------------------------------------------------------------------------
+void build_pair_plan(flosic_ctx* c) {
+  std::vector<std::array<double, 3>> center;
+  double dmin = 1.0e30;
+  for (int a = 0; a < c->natoms; ++a) {
+    std::array<double, 3> p = {c->rat[3 * a], c->rat[3 * a + 1], c->rat[3 * a + 2]};
+    center.push_back(p);
+    const double d = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+    if (d < dmin) dmin = d;
+  }
+  int mcnt = (int)center.size();
+  if (std::sqrt(dmin) > 0.7) {
+    center.push_back({0.0, 0.0, 0.0});
+    ++mcnt;
+  }
+  const int nclass = mcnt + 1;
+  std::vector<std::vector<PairGeo>> buf((size_t)nclass * 3);
+  std::vector<PairGeo> pairs;
+  std::vector<CallInfo> calls;
+  const int nspn = c->nspn;
+  auto flush = [&](std::vector<PairGeo>& b, bool weird) {
+    auto emit = [&](const PairGeo* first, int n) {
+      CallInfo ci;
+      ci.p0 = (int)pairs.size();
+      ci.np = n;
+      ci.slots = n * nspn;
+      ci.pad = 0;
+      ci.delta_min = 1.0e30;
+      for (int i = 0; i < n; ++i) {
+        PairGeo g = first[i];
+        g.call = (int)calls.size();
+        ci.delta_min = std::min(ci.delta_min, g.delta);
+        pairs.push_back(g);
+      }
+      calls.push_back(ci);
+    };
+    if (weird)
+      for (auto& g : b) emit(&g, 1);
+    else
+      emit(b.data(), (int)b.size());
+    b.clear();
+  };
+  for (int ia = 0; ia < c->natoms; ++ia) {
+    const TypeInfo& ti = c->types[c->atype[ia]];
+    const double* AI = &c->rat[3 * ia];
+    for (int ja = ia; ja < c->natoms; ++ja) {
+      const TypeInfo& tj = c->types[c->atype[ja]];
+      const double* AJ = &c->rat[3 * ja];
+      const double times_sites = (ja > ia) ? 2.0 : 1.0;
+      const double rarg = (AI[0] - AJ[0]) * (AI[0] - AJ[0]) + (AI[1] - AJ[1]) * (AI[1] - AJ[1]) +
+                          (AI[2] - AJ[2]) * (AI[2] - AJ[2]);
+      for (int ialp = 0; ialp < ti.nbare; ++ialp) {
+        const double ai = ti.alp[ialp];
+        for (int jalp = (ia == ja) ? ialp : 0; jalp < tj.nbare; ++jalp) {
+          const double times_alpha = (ia == ja && jalp > ialp) ? 2.0 : 1.0;
+          const double aj = tj.alp[jalp];
+          const double rcalp = 1.0 / (ai + aj);
+          const double arg = ai * aj * rcalp * rarg;
+          if (arg > CUTEXP) continue;
+          double C[3];
+          for (int d = 0; d < 3; ++d) C[d] = (ai * AI[d] + aj * AJ[d]) * rcalp;
+          double dm = 1.0e30;
+          int minc = 0;
+          for (int ic = 0; ic < mcnt; ++ic) {
+            const double dist = std::sqrt((C[0] - center[ic][0]) * (C[0] - center[ic][0]) +
+                                          (C[1] - center[ic][1]) * (C[1] - center[ic][1]) +
+                                          (C[2] - center[ic][2]) * (C[2] - center[ic][2]));
+            if (dist < dm) {
+              dm = dist;
+              minc = ic;
+            }
+          }
+          if ((ai + aj) * dm * dm > 0.5) minc = mcnt;
+          if (ai + aj < 3.0) minc = mcnt;
+          int lng = 0;
+          if (ai + aj > 10.0) lng = 1;
+          if (ai + aj > 40.0) lng = 2;
+          PairGeo g;
+          std::memset(&g, 0, sizeof(g));
+          g.a = ai;
+          g.b = aj;
+          for (int d = 0; d < 3; ++d) {
+            g.A[d] = AI[d];
+            g.B[d] = AJ[d];
+          }
+          // poisson1.f:299-325
+          const double delta = ai + aj;
+          const double rcdelt = 1.0 / delta;
+          const double parg = ai * aj * rcdelt *
+                              ((AI[0] - AJ[0]) * (AI[0] - AJ[0]) + (AI[1] - AJ[1]) * (AI[1] - AJ[1]) +
+                               (AI[2] - AJ[2]) * (AI[2] - AJ[2]));
+          g.factor = 6.283185307179586 * std::exp(-parg) * rcdelt;
+          for (int d = 0; d < 3; ++d) g.C[d] = (ai * AI[d] + aj * AJ[d]) * rcdelt;
+          g.delta = delta;
+          g.times = times_sites * times_alpha;
+          g.pi = c->apoff[ia] + ialp;
+          g.pj = c->apoff[ja] + jalp;
+          auto& b = buf[(size_t)minc * 3 + lng];
+          b.push_back(g);
+          if ((int)b.size() * nspn == MXPR) flush(b, minc == mcnt);
+        }
+      }
+    }
+  }
+  for (int lng = 0; lng < 3; ++lng)
+    for (int minc = 0; minc < nclass; ++minc) {
+      auto& b = buf[(size_t)minc * 3 + lng];
+      if (!b.empty()) flush(b, minc == mcnt);
+    }
+  c->pairs.swap(pairs);
+  c->calls.swap(calls);
+}
+
+// Spatial sort of the mesh into tiles of TILE points (Morton order).
+void sort_mesh(flosic_ctx* c, const double* rmsh, const double* wmsh) {
+  const int n = c->nmsh;
+  double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], rmsh[3 * i + d]);
+      hi[d] = std::max(hi[d], rmsh[3 * i + d]);
+    }
+  auto spread = [](uint64_t v) {
+    uint64_t x = v & 0x1fffff;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+  };
+  std::vector<std::pair<uint64_t, int>> key(n);
+  for (int i = 0; i < n; ++i) {
+    uint64_t q[3];
+    for (int d = 0; d < 3; ++d) {
+      const double ext = hi[d] - lo[d];
+      double f = ext > 0 ? (rmsh[3 * i + d] - lo[d]) / ext : 0.0;
+      q[d] = (uint64_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
+    }
+    key[i] = {spread(q[0]) | (spread(q[1]) << 1) | (spread(q[2]) << 2), i};
+  }
+  std::sort(key.begin(), key.end());
+  c->perm.resize(n);
+  std::vector<double> x(n), y(n), z(n), w(n);
+  for (int i = 0; i < n; ++i) {
+    const int o = key[i].second;
+    c->perm[i] = o;
+    x[i] = rmsh[3 * o];
+    y[i] = rmsh[3 * o + 1];
+    z[i] = rmsh[3 * o + 2];
+    w[i] = wmsh[o];
+  }
+  c->ntiles = (n + TILE - 1) / TILE;
+  std::vector<double> tlo(3 * (size_t)c->ntiles), thi(3 * (size_t)c->ntiles);
+  for (int t = 0; t < c->ntiles; ++t) {
+    double l[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, h[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int i = t * TILE; i < std::min(n, (t + 1) * TILE); ++i) {
+      const double p[3] = {x[i], y[i], z[i]};
+      for (int d = 0; d < 3; ++d) {
+        l[d] = std::min(l[d], p[d]);
+        h[d] = std::max(h[d], p[d]);
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      tlo[3 * t + d] = l[d];
+      thi[3 * t + d] = h[d];
+    }
+  }
+  // farthest point from the origin, first in the original order on ties
+  double rmx = 0.0;
+  int ifar = 0;
+  for (int i = 0; i < n; ++i) {
+    const double rad = std::sqrt(rmsh[3 * i] * rmsh[3 * i] + rmsh[3 * i + 1] * rmsh[3 * i + 1] +
+                                 rmsh[3 * i + 2] * rmsh[3 * i + 2]);
+    if (rad > rmx) {
+      rmx = rad;
+      ifar = i;
+    }
+  }
+  c->rmx = rmx;
+  for (int i = 0; i < n; ++i)
+    if (c->perm[i] == ifar) c->ifar_sorted = i;
+  cudaStream_t st = c->st;
+  c->d_x.upload(x.data(), n, st);
+  c->d_y.upload(y.data(), n, st);
+  c->d_z.upload(z.data(), n, st);
+  c->d_w.upload(w.data(), n, st);
+  c->d_tlo.upload(tlo.data(), tlo.size(), st);
+  c->d_thi.upload(thi.data(), thi.size(), st);
+}
+
+void invalidate(flosic_ctx* c) {
+  for (auto& s : c->spin) {
+    s.fo_valid = s.pot_valid = s.sic_valid = false;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FO construction (FRMORB2(0,0) and FRMIORB(1,1)) for one spin
+// ---------------------------------------------------------------------------
+void fo_setup(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  if (S.fo_valid) return;
+  const int nw = c->nwfs[s], nf = c->nfrm[s], nb = c->nbasis;
+  if (nw != nf) fail(FLOSIC_ERR_NFRM, "FRMIORB: MORB .NE. NFRM");
+  if (nf <= 0) fail(FLOSIC_ERR_ARG, "no FODs for this spin");
+  S.nf = nf;
+  S.nw = nw;
+  cudaStream_t st = c->st;
+  // orbital values and gradients at the FODs (basis values -> PSIG by DGEMM with
+  // the KS coefficients whose magnitude exceeds 1e-10, frmorb2.F:270-286)
+  std::vector<double> pts(3 * (size_t)nf);
+  for (int k = 0; k < nf; ++k)
+    for (int d = 0; d < 3; ++d) pts[(size_t)d * nf + k] = c->fods[s][3 * k + d];
+  c->d_fodpts.upload(pts.data(), pts.size(), st);
+  c->d_basis.ensure((size_t)4 * nb * nf);
+  launch_basis_values(c->basis_dev(), 1, nf, c->d_fodpts.p, c->d_fodpts.p + nf, c->d_fodpts.p + 2 * nf,
+                      c->d_basis.p, nf, st);
+  c->launches++;
+  c->d_psig.ensure((size_t)4 * nf * nw);
+  const double one = 1.0, zero = 0.0;
+  const double* cthr = c->d_psi_thr.p + (size_t)s * c->nwfs[0] * nb;
+  for (int ch = 0; ch < 4; ++ch) {
+    // PSIG_ch (nf x nw) = B_ch^T (nf x nb) * C (nb x nw)
+    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nf, nw, nb, &one, c->d_basis.p + (size_t)ch * nb * nf,
+                           nf, cthr, nb, &zero, c->d_psig.p + (size_t)ch * nf * nw, nf));
+    c->launches++;
+  }
+  std::vector<double> psig((size_t)4 * nf * nw);
+  CUDA_CHECK(cudaMemcpyAsync(psig.data(), c->d_psig.p, sizeof(double) * psig.size(), cudaMemcpyDeviceToHost, st));
+  CUDA_CHECK(cudaStreamSynchronize(st));
+  auto PS = [&](int ch, int k, int j) { return psig[((size_t)ch * nw + j) * nf + k]; };
+  // FMAT (frmorb2.F:296-346)
+  S.fmat.assign((size_t)4 * nf * nw, 0.0);
+  for (int k = 0; k < nf; ++k) {
+    double rhi[4] = {0, 0, 0, 0};
+    for (int j = 0; j < nw; ++j)
+      for (int K = 0; K < 4; ++K) rhi[K] = rhi[K] + PS(0, k, j) * PS(K, k, j);
+    if (!(rhi[0] > 0.0)) fail(FLOSIC_ERR_ZERO_DENSITY, "FRMORB2: zero density at an FOD");
+    for (int K = 0; K < 4; ++K)
+      for (int j = 0; j < nw; ++j) {
+        double f = PS(K, k, j) / std::sqrt(rhi[0]);
+        if (K >= 1) f = f - S.fmat[((size_t)0 * nf + k) * nw + j] * rhi[K] / rhi[0];
+        S.fmat[((size_t)K * nf + k) * nw + j] = f;
+      }
+  }
+  // TMAT (frmiorb.f:351-480)
+  std::vector<double> T((size_t)nf * nw), over((size_t)nf * nf);
+  for (int k = 0; k < nf; ++k) {
+    double rho = 0.0;
+    for (int j = 0; j < nw; ++j) rho = rho + PS(0, k, j) * PS(0, k, j);
+    if (!(rho > 0.0)) fail(FLOSIC_ERR_ZERO_DENSITY, "FRMIORB: zero density at an FOD");
+    for (int j = 0; j < nw; ++j) T[(size_t)k * nw + j] = PS(0, k, j) / std::sqrt(rho);
+  }
+  for (int i = 0; i < nf; ++i)
+    for (int j = 0; j < nf; ++j) {
+      double v = 0.0;
+      for (int w = 0; w < nw; ++w) v = v + T[(size_t)i * nw + w] * T[(size_t)j * nw + w];
+      over[(size_t)i * nf + j] = v;
+    }
+  std::vector<double> sm12, filo;
+  lowsic(nf, over, sm12, filo, S.lam);
+  S.tmat.assign((size_t)nf * nw, 0.0);
+  for (int i = 0; i < nf; ++i)
+    for (int k = 0; k < nf; ++k) {
+      const double h = sm12[(size_t)k * nf + i];
+      for (int w = 0; w < nw; ++w) S.tmat[(size_t)i * nw + w] += h * T[(size_t)k * nw + w];
+    }
+  // FO coefficients C_FO(nb x nf) = C_KS(nb x nw) * TMAT^T (unravel2.f:200-240)
+  c->d_tmat.upload(S.tmat.data(), S.tmat.size(), st);
+  S.cfo.ensure((size_t)nb * nf);
+  const double* cks = c->d_psi.p + (size_t)s * c->nwfs[0] * nb;
+  BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nf, nw, &one, cks, nb, c->d_tmat.p, nw, &zero,
+                         S.cfo.p, nb));
+  c->launches++;
+  S.fo_valid = true;
+}
+
+// FO values (+ derivatives for GGA) on the mesh: phi[(ch*nf + k)*P + p]
+void fo_values(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  const int nf = S.nf, nb = c->nbasis, P = c->nmsh;
+  const int nch = c->gga ? 10 : 1;
+  const int nderv = c->gga ? 2 : 0;
+  S.phi.ensure((size_t)nch * nf * P);
+  const size_t budget = (size_t)3 << 30;  // bytes of basis scratch
+  int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nch * nb)));
+  chunk = std::max(TILE, chunk / TILE * TILE);
+  c->d_basis.ensure((size_t)nch * nb * chunk);
+  const double one = 1.0, zero = 0.0;
+  for (int p0 = 0; p0 < P; p0 += chunk) {
+    const int np = std::min(chunk, P - p0);
+    launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + p0, c->d_y.p + p0, c->d_z.p + p0, c->d_basis.p, np,
+                        c->st);
+    c->launches++;
+    for (int ch = 0; ch < nch; ++ch) {
+      BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, np, nf, nb, &one,
+                             c->d_basis.p + (size_t)ch * nb * np, np, S.cfo.p, nb, &zero,
+                             S.phi.p + (size_t)ch * nf * P + p0, P));
+      c->launches++;
+    }
+  }
+}
+
+void coulomb(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  const int nf = S.nf, P = c->nmsh;
+  const int npairs = (int)c->pairs.size(), ncalls = (int)c->calls.size();
+  cudaStream_t st = c->st;
+  c->d_u.ensure((size_t)nf * c->nprim * 10);
+  launch_prim_u(c->basis_dev(), nf, S.cfo.p, c->nbasis, c->d_u.p, st);
+  c->launches++;
+  c->d_coef.ensure((size_t)std::max(npairs, 1) * nf * NCOEF);
+  c->d_maxfmt.ensure((size_t)std::max(npairs, 1) * nf);
+  c->d_cgp.ensure((size_t)std::max(npairs, 1) * nf * 4);
+  c->d_callfo.ensure((size_t)std::max(ncalls, 1) * nf);
+  c->d_mom.ensure((size_t)std::max(ncalls, 1) * nf * NMOM);
+  CUDA_CHECK(cudaEventRecord(c->ev[2], st));
+  launch_pair_coef(npairs, c->d_pairs.p, c->d_calls.p, nf, c->nprim, c->d_u.p, c->nspn, c->d_coef.p,
+                   c->d_maxfmt.p, c->d_cgp.p, st);
+  c->launches++;
+  launch_call_setup(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->nspn, c->d_coef.p, c->d_maxfmt.p, c->d_cgp.p,
+                    c->mesh_dev(), c->d_boys.p, c->d_callfo.p, c->d_mom.p, st);
+  c->launches++;
+  CUDA_CHECK(cudaEventRecord(c->ev[3], st));
+  S.vh.ensure((size_t)nf * P);
+  launch_coulomb_eval(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
+                      c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Everything of APOTNL_SIC for all FOs of spin s (apotnl_sic.F:232-623).
+void spin_potentials(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  if (S.pot_valid) return;
+  cudaStream_t st = c->st;
+  CUDA_CHECK(cudaEventRecord(c->ev[0], st));
+  fo_setup(c, s);
+  CUDA_CHECK(cudaEventRecord(c->ev[1], st));
+  fo_values(c, s);
+  CUDA_CHECK(cudaEventRecord(c->ev[7], st));
+  coulomb(c, s);
+  CUDA_CHECK(cudaEventRecord(c->ev[4], st));
+  const int nf = S.nf, P = c->nmsh;
+  S.vpot.ensure((size_t)nf * P);
+  S.y.ensure((size_t)nf * P);
+  S.vh.ensure((size_t)nf * P);
+  const int nblk = std::min(1024, (P + 255) / 256);
+  c->d_part.ensure((size_t)nf * nblk * NPART);
+  c->d_sums.ensure((size_t)nf * NPART);
+  // XC reads the raw Coulomb potential; keep a scaled copy out of place
+  c->d_tmp.ensure((size_t)nf * P);
+  CUDA_CHECK(cudaMemcpyAsync(c->d_tmp.p, S.vh.p, sizeof(double) * nf * P, cudaMemcpyDeviceToDevice, st));
+  launch_xc(c->mesh_dev(), nf, c->gga, c->nspn, c->xc, S.phi.p, P, c->d_tmp.p, S.vpot.p, S.y.p, c->d_part.p, nblk,
+            st);
+  launch_reduce_parts(nf, nblk, c->d_part.p, c->d_sums.p, st);
+  c->launches += 2;
+  std::vector<double> sums((size_t)nf * NPART), far(nf);
+  CUDA_CHECK(cudaMemcpyAsync(sums.data(), c->d_sums.p, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, st));
+  CUDA_CHECK(cudaMemcpy2DAsync(far.data(), sizeof(double), c->d_tmp.p + c->ifar_sorted, sizeof(double) * P,
+                               sizeof(double), nf, cudaMemcpyDeviceToHost, st));
+  CUDA_CHECK(cudaEventRecord(c->ev[5], st));
+  CUDA_CHECK(cudaStreamSynchronize(st));
+  c->stage_ms[0] += elapsed(c->ev[0], c->ev[1]);
+  c->stage_ms[1] += elapsed(c->ev[1], c->ev[7]);
+  c->stage_ms[2] += elapsed(c->ev[7], c->ev[3]);
+  c->stage_ms[3] += elapsed(c->ev[3], c->ev[4]);
+  c->stage_ms[4] += elapsed(c->ev[4], c->ev[5]);
+  S.results.assign((size_t)nf * 13, 0.0);
+  S.cfrm.assign((size_t)nf * 3, 0.0);
+  for (int k = 0; k < nf; ++k) {
+    const double* q = &sums[(size_t)k * NPART];
+    double* r = &S.results[(size_t)k * 13];
+    const double xch1 = q[0], xcou = q[1];
+    double xexx = q[2];
+    double xdel = q[3];
+    const double ergxl = q[4], ergxn = q[5], ergcl = q[6], ergcn = q[7];
+    const double excsic = ergxl + ergxn + ergcl + ergcn;
+    xdel = xdel - xcou;
+    const double xeng = -excsic - xcou / 2.0;
+    const double pi = 4.0 * std::atan(1.0);
+    xexx = xexx * 0.75 * std::pow(6 / pi, (double)(1.0f / 3.0f));
+    r[0] = k + 1;
+    r[1] = xch1;
+    r[2] = 0.0;
+    r[3] = far[k] * c->rmx;
+    r[4] = xexx;
+    r[5] = -xcou / 2.0;
+    r[6] = xdel;
+    r[7] = xeng;
+    r[8] = xeng * (2.0 / c->nspn);
+    r[9] = ergxl;
+    r[10] = ergcl;
+    r[11] = ergxn;
+    r[12] = ergcn;
+    for (int d = 0; d < 3; ++d) S.cfrm[(size_t)k * 3 + d] = q[8 + d];
+    double addit = 0.0;
+    (void)addit;
+  }
+  S.pot_valid = true;
+}
+
+// SICLAGM (frmorb_mpi.F:456-517): SIC(j,l) = -sum_p phi_j w V_l phi_l
+void spin_sic(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  if (S.sic_valid) return;
+  spin_potentials(c, s);
+  const int nf = S.nf, P = c->nmsh;
+  cudaStream_t st = c->st;
+  CUDA_CHECK(cudaEventRecord(c->ev[0], st));
+  c->d_sic.ensure((size_t)nf * nf);
+  const double mone = -1.0, zero = 0.0;
+  BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nf, nf, P, &mone, S.phi.p, P, S.y.p, P, &zero,
+                         c->d_sic.p, nf));
+  c->launches++;
+  S.sic.resize((size_t)nf * nf);
+  CUDA_CHECK(cudaMemcpyAsync(S.sic.data(), c->d_sic.p, sizeof(double) * nf * nf, cudaMemcpyDeviceToHost, st));
+  CUDA_CHECK(cudaEventRecord(c->ev[1], st));
+  CUDA_CHECK(cudaStreamSynchronize(st));
+  c->stage_ms[5] += elapsed(c->ev[0], c->ev[1]);
+  S.sic_valid = true;
+}
+
+// FRMORB2(-s,-1) force branch (frmorb2.F:586-717), with the O(n^4) loops of
+// the second term regrouped into O(n^3) products.
+void spin_force(flosic_ctx* c, int s, const double* sic /* SIC(j,l) at [l*ld + j] */, int ld, double* deb) {
+  fo_setup(c, s);
+  SpinCache& S = c->spin[s];
+  const int nf = S.nf, nw = S.nw;
+  auto fm = [&](int kwf, int ifm, int K) { return S.fmat[((size_t)K * nf + ifm) * nw + kwf]; };
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> over((size_t)nf * nf);
+  for (int i = 0; i < nf; ++i)
+    for (int j = 0; j < nf; ++j) {
+      double v = 0.0;
+      for (int w = 0; w < nw; ++w) v = v + fm(w, i, 0) * fm(w, j, 0);
+      over[(size_t)j * nf + i] = v;
+    }
+  std::vector<double> sm12, filo, Q;
+  lowsic(nf, over, sm12, filo, Q);
+  auto FI = [&](int i, int a) { return filo[(size_t)i * nf + a]; };
+  // G = FILO^T SIC FILO  ->  HAM(b,a) = (G[a][b] - G[b][a]) / sqrt(Qa Qb)
+  std::vector<double> tmp((size_t)nf * nf, 0.0), G((size_t)nf * nf, 0.0);
+  for (int k = 0; k < nf; ++k)      // tmp[a][l] = sum_k FI(k,a) SIC(k,l)
+    for (int l = 0; l < nf; ++l) {
+      const double sv = sic[(size_t)l * ld + k];
+      if (sv == 0.0) continue;
+      for (int a = 0; a < nf; ++a) tmp[(size_t)a * nf + l] += FI(k, a) * sv;
+    }
+  for (int a = 0; a < nf; ++a)      // G[a][b] = sum_l tmp[a][l] FI(l,b)
+    for (int l = 0; l < nf; ++l) {
+      const double t = tmp[(size_t)a * nf + l];
+      for (int b = 0; b < nf; ++b) G[(size_t)a * nf + b] += t * FI(l, b);
+    }
+  std::vector<double> H((size_t)nf * nf);  // H[a*nf+b] = HAM(b,a)
+  for (int a = 0; a < nf; ++a)
+    for (int b = 0; b < nf; ++b)
+      H[(size_t)a * nf + b] = (G[(size_t)a * nf + b] - G[(size_t)b * nf + a]) / (std::sqrt(Q[b]) * std::sqrt(Q[a]));
+  // X[kx][n][m] = sum_w F(w,n,1) F(w,m,kx+1)
+  std::vector<double> X((size_t)3 * nf * nf, 0.0);
+  for (int kx = 0; kx < 3; ++kx)
+    for (int n = 0; n < nf; ++n)
+      for (int m = 0; m < nf; ++m) {
+        double v = 0.0;
+        for (int w = 0; w < nw; ++w) v += fm(w, n, 0) * fm(w, m, kx + 1);
+        X[((size_t)kx * nf + n) * nf + m] = v;
+      }
+  for (int i = 0; i < 3 * nf; ++i) deb[i] = 0.0;
+  // term 1: deb(kx,m) -= sum_a FI(m,a) sum_n SC1_a(n) X(n,m), SC1_a(n) = sum_b HAM(b,a) FI(n,b)
+  std::vector<double> sc1((size_t)nf * nf, 0.0);  // sc1[a][n]
+  for (int a = 0; a < nf; ++a)
+    for (int b = 0; b < nf; ++b) {
+      const double h = H[(size_t)a * nf + b];
+      for (int n = 0; n < nf; ++n) sc1[(size_t)a * nf + n] += h * FI(n, b);
+    }
+  for (int kx = 0; kx < 3; ++kx) {
+    std::vector<double> Z((size_t)nf * nf, 0.0);  // Z[a][m] = sum_n sc1[a][n] X(n,m)
+    for (int a = 0; a < nf; ++a)
+      for (int n = 0; n < nf; ++n) {
+        const double t = sc1[(size_t)a * nf + n];
+        const double* xr = &X[((size_t)kx * nf + n) * nf];
+        for (int m = 0; m < nf; ++m) Z[(size_t)a * nf + m] += t * xr[m];
+      }
+    for (int m = 0; m < nf; ++m) {
+      double v = 0.0;
+      for (int a = 0; a < nf; ++a) v += FI(m, a) * Z[(size_t)a * nf + m];
+      deb[3 * m + kx] -= v;
+    }
+  }
+  // term 2 with HAM'(b,a) = HAM(b,a) (sqrtQb - sqrtQa)/(sqrtQb + sqrtQa):
+  // deb(kx,m) += 0.25 sum_ab HAM'(b,a) [FI(m,a) Y_b(m) + FI(m,b) Y_a(m)] * 2,
+  // Y_b(m) = sum_i FI(i,b) 2 X(i,m)
+  std::vector<double> Hp((size_t)nf * nf);
+  for (int a = 0; a < nf; ++a)
+    for (int b = 0; b < nf; ++b) {
+      double h = H[(size_t)a * nf + b] * (std::sqrt(Q[b]) - std::sqrt(Q[a]));
+      Hp[(size_t)a * nf + b] = h / (std::sqrt(Q[b]) + std::sqrt(Q[a]));
+    }
+  for (int kx = 0; kx < 3; ++kx) {
+    std::vector<double> Yb((size_t)nf * nf, 0.0);  // Yb[b][m]
+    for (int i = 0; i < nf; ++i)
+      for (int b = 0; b < nf; ++b) {
+        const double f = FI(i, b);
+        const double* xr = &X[((size_t)kx * nf + i) * nf];
+        for (int m = 0; m < nf; ++m) Yb[(size_t)b * nf + m] += f * 2.0 * xr[m];
+      }
+    for (int m = 0; m < nf; ++m) {
+      double v = 0.0;
+      for (int a = 0; a < nf; ++a) {
+        const double fma_ = FI(m, a);
+        for (int b = 0; b < nf; ++b) {
+          const double hp = Hp[(size_t)a * nf + b];
+          v += hp * (fma_ * Yb[(size_t)b * nf + m] + FI(m, b) * Yb[(size_t)a * nf + m]);
+        }
+      }
+      deb[3 * m + kx] += 0.25 * v;
+    }
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  c->stage_ms[6] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return FLOSIC_OK;
+  } catch (const Fail& e) {
+    return e.code;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return FLOSIC_ERR_CUDA;
+  }
+}
+
+void require(flosic_ctx* c, bool orb) {
+  if (!c) fail(FLOSIC_ERR_ARG, "null context");
+  if (!c->have_geom) fail(FLOSIC_ERR_STATE, "flosic_sic_set_geometry has not been called");
+  if (orb && !c->have_orb) fail(FLOSIC_ERR_STATE, "flosic_sic_set_orbitals has not been called");
+  CUDA_CHECK(cudaSetDevice(c->device));
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* flosic_sic_last_error(void) { return g_err.c_str(); }
+
+int flosic_sic_create(int device, flosic_ctx** out) {
+  return guarded([&] {
+    if (!out) fail(FLOSIC_ERR_ARG, "null output pointer");
+    int ndev = 0;
+    CUDA_CHECK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) fail(FLOSIC_ERR_ARG, "invalid device");
+    CUDA_CHECK(cudaSetDevice(device));
+    auto* c = new flosic_ctx;
+    c->device = device;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
+      delete c;
+      fail(FLOSIC_ERR_CUDA, "cublasCreate failed");
+    }
+    cublasSetStream(c->blas, c->st);
+    cublasSetMathMode(c->blas, CUBLAS_PEDANTIC_MATH);
+    for (auto& e : c->ev) CUDA_CHECK(cudaEventCreate(&e));
+    std::vector<double> ang, w;
+    lebedev19(ang, w);
+    upload_constants(ang.data(), w.data());
+    std::vector<double> bt = boys_table();
+    c->d_boys.upload(bt.data(), bt.size(), c->st);
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    *out = c;
+  });
+}
+
+int flosic_sic_destroy(flosic_ctx* c) {
+  if (!c) return FLOSIC_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->st);
+  for (auto& s : c->spin) s.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  c->d_atom_pos.release(); c->d_type_alpha.release(); c->d_type_amin.release(); c->d_type_bfcon.release();
+  c->d_atom_type.release(); c->d_atom_boff.release(); c->d_atom_poff.release(); c->d_type_nbare.release();
+  c->d_type_lmax.release(); c->d_type_ncon.release(); c->d_prim_atom.release(); c->d_prim_ib.release();
+  c->d_x.release(); c->d_y.release(); c->d_z.release(); c->d_w.release(); c->d_tlo.release(); c->d_thi.release();
+  c->d_boys.release(); c->d_pairs.release(); c->d_calls.release(); c->d_psi.release(); c->d_psi_thr.release();
+  c->d_basis.release(); c->d_fodpts.release(); c->d_psig.release(); c->d_tmat.release(); c->d_u.release();
+  c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
+  c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release();
+  if (c->blas) cublasDestroy(c->blas);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return FLOSIC_OK;
+}
+
+int flosic_sic_set_geometry(flosic_ctx* c, int natoms, const int32_t* atom_type, const double* rat, int ntypes,
+                            const int32_t* n_bare, const double* bfalp, const int32_t* n_con, const double* bfcon,
+                            int nmsh, const double* rmsh, const double* wmsh, int nspn, const int32_t* igga,
+                            const int32_t* idftyp) {
+  return guarded([&] {
+    if (!c) fail(FLOSIC_ERR_ARG, "null context");
+    CUDA_CHECK(cudaSetDevice(c->device));
+    if (natoms <= 0 || ntypes <= 0 || nmsh <= 0) fail(FLOSIC_ERR_ARG, "natoms, ntypes and nmsh must be positive");
+    if (nspn != 1 && nspn != 2) fail(FLOSIC_ERR_ARG, "nspn must be 1 or 2");
+    if (!atom_type || !rat || !n_bare || !bfalp || !n_con || !bfcon || !rmsh || !wmsh || !igga || !idftyp)
+      fail(FLOSIC_ERR_ARG, "null array argument");
+    for (int i = 0; i < 2; ++i)
+      if (igga[i] < 0 || igga[i] > 1) fail(FLOSIC_ERR_ARG, "IGGA must be 0 (LDA) or 1 (GGA)");
+    if (idftyp[0] < 6 || idftyp[0] > 9) fail(FLOSIC_ERR_ARG, "exchange IDFTYP must be PW91, PBE, REVPBE or RPBE");
+    if (idftyp[1] != 6 && idftyp[1] != 7) fail(FLOSIC_ERR_ARG, "correlation IDFTYP must be PW91 or PBE");
+    invalidate(c);
+    c->have_geom = c->have_orb = false;
+    c->natoms = natoms;
+    c->ntypes = ntypes;
+    c->nmsh = nmsh;
+    c->nspn = nspn;
+    c->xc[0] = igga[0];
+    c->xc[1] = idftyp[0];
+    c->xc[2] = igga[1];
+    c->xc[3] = idftyp[1];
+    c->gga = (igga[0] > 0 || igga[1] > 0) ? 1 : 0;
+    c->types.assign(ntypes, TypeInfo());
+    for (int t = 0; t < ntypes; ++t) {
+      TypeInfo& T = c->types[t];
+      T.nbare = n_bare[t];
+      if (T.nbare < 1 || T.nbare > MAX_BARE) fail(FLOSIC_ERR_CAPACITY, "N_BARE exceeds MAX_BARE=25");
+      T.lmax = 0;
+      T.nloc = 0;
+      for (int l = 0; l < 3; ++l) {
+        T.ncon[l] = n_con[t * 3 + l];
+        if (T.ncon[l] < 0 || T.ncon[l] > MAX_CON) fail(FLOSIC_ERR_CAPACITY, "N_CON exceeds MAX_CON=15");
+        if (T.ncon[l] > 0) T.lmax = l;
+        T.nloc += kNcomp[l] * T.ncon[l];
+      }
+      for (int ib = 0; ib < MAX_BARE; ++ib) T.alp[ib] = bfalp[(size_t)t * MAX_BARE + ib];
+      for (int ib = 0; ib < T.nbare; ++ib)
+        if (!(T.alp[ib] > 0.0)) fail(FLOSIC_ERR_ARG, "BFALP must be positive");
+      for (int l = 0; l < 3; ++l)
+        for (int cc = 0; cc < MAX_CON; ++cc)
+          for (int ib = 0; ib < MAX_BARE; ++ib)
+            T.con[l][cc][ib] = bfcon[(((size_t)t * 3 + l) * MAX_CON + cc) * MAX_BARE + ib];
+    }
+    c->atype.resize(natoms);
+    c->aoff.resize(natoms);
+    c->apoff.resize(natoms);
+    c->rat.assign(rat, rat + 3 * (size_t)natoms);
+    int off = 0, poff = 0;
+    std::vector<int> prim_atom, prim_ib;
+    for (int a = 0; a < natoms; ++a) {
+      const int t = atom_type[a] - 1;
+      if (t < 0 || t >= ntypes) fail(FLOSIC_ERR_ARG, "atom_type out of range (1-based IFNCT)");
+      if (a > 0 && t < c->atype[a - 1])
+        fail(FLOSIC_ERR_ARG, "atoms must be ordered by function set (IFNCT outer, I_POS inner)");
+      c->atype[a] = t;
+      c->aoff[a] = off;
+      c->apoff[a] = poff;
+      off += c->types[t].nloc;
+      for (int ib = 0; ib < c->types[t].nbare; ++ib) {
+        prim_atom.push_back(a);
+        prim_ib.push_back(ib);
+      }
+      poff += c->types[t].nbare;
+    }
+    c->nbasis = off;
+    c->nprim = poff;
+    for (int i = 0; i < nmsh; ++i)
+      if (!(wmsh[i] > 0.0) && wmsh[i] != 0.0) fail(FLOSIC_ERR_ARG, "WMSH must be finite");
+    cudaStream_t st = c->st;
+    // device basis tables
+    std::vector<double> alpha((size_t)ntypes * MAX_BARE), amin(ntypes), con((size_t)ntypes * 3 * MAX_CON * MAX_BARE);
+    std::vector<int> nbarev(ntypes), lmaxv(ntypes), nconv(3 * (size_t)ntypes);
+    for (int t = 0; t < ntypes; ++t) {
+      const TypeInfo& T = c->types[t];
+      nbarev[t] = T.nbare;
+      lmaxv[t] = T.lmax;
+      double am = DBL_MAX;
+      for (int ib = 0; ib < MAX_BARE; ++ib) {
+        alpha[(size_t)t * MAX_BARE + ib] = T.alp[ib];
+        if (ib < T.nbare) am = std::min(am, T.alp[ib]);
+      }
+      amin[t] = am;
+      for (int l = 0; l < 3; ++l) {
+        nconv[3 * t + l] = T.ncon[l];
+        for (int cc = 0; cc < MAX_CON; ++cc)
+          for (int ib = 0; ib < MAX_BARE; ++ib)
+            con[(((size_t)t * 3 + l) * MAX_CON + cc) * MAX_BARE + ib] = T.con[l][cc][ib];
+      }
+    }
+    c->d_atom_pos.upload(c->rat.data(), c->rat.size(), st);
+    c->d_atom_type.upload(c->atype.data(), natoms, st);
+    c->d_atom_boff.upload(c->aoff.data(), natoms, st);
+    c->d_atom_poff.upload(c->apoff.data(), natoms, st);
+    c->d_type_nbare.upload(nbarev.data(), ntypes, st);
+    c->d_type_lmax.upload(lmaxv.data(), ntypes, st);
+    c->d_type_ncon.upload(nconv.data(), nconv.size(), st);
+    c->d_type_alpha.upload(alpha.data(), alpha.size(), st);
+    c->d_type_amin.upload(amin.data(), ntypes, st);
+    c->d_type_bfcon.upload(con.data(), con.size(), st);
+    c->d_prim_atom.upload(prim_atom.data(), prim_atom.size(), st);
+    c->d_prim_ib.upload(prim_ib.data(), prim_ib.size(), st);
+    sort_mesh(c, rmsh, wmsh);
+    build_pair_plan(c);
+    c->d_pairs.upload(c->pairs.data(), c->pairs.size(), st);
+    c->d_calls.upload(c->calls.data(), c->calls.size(), st);
+    CUDA_CHECK(cudaStreamSynchronize(st));
+    c->have_geom = true;
+  });
+}
+
+int flosic_sic_set_orbitals(flosic_ctx* c, const int32_t* nwfs, const double* psi, int ldpsi, const int32_t* nfrm,
+                            const double* bfrm, int ldfrm) {
+  return guarded([&] {
+    require(c, false);
+    if (!nwfs || !psi || !nfrm || !bfrm) fail(FLOSIC_ERR_ARG, "null array argument");
+    if (ldpsi < c->nbasis) fail(FLOSIC_ERR_ARG, "ldpsi smaller than the number of basis functions");
+    const int ns = c->nspn;
+    for (int s = 0; s < ns; ++s) {
+      if (nwfs[s] < 0 || nfrm[s] < 0 || nfrm[s] > ldfrm) fail(FLOSIC_ERR_ARG, "bad NWFS/NFRM");
+      if (nwfs[s] != nfrm[s]) fail(FLOSIC_ERR_NFRM, "MORB .NE. NFRM (frmiorb.f:418)");
+    }
+    invalidate(c);
+    c->nwfs[0] = nwfs[0];
+    c->nwfs[1] = (ns == 2) ? nwfs[1] : 0;
+    c->nfrm[0] = nfrm[0];
+    c->nfrm[1] = (ns == 2) ? nfrm[1] : 0;
+    const int nwf = c->nwfs[0] + c->nwfs[1];
+    const int nb = c->nbasis;
+    c->psi.assign((size_t)nb * nwf, 0.0);
+    std::vector<double> thr((size_t)nb * nwf, 0.0);
+    for (int j = 0; j < nwf; ++j)
+      for (int i = 0; i < nb; ++i) {
+        const double v = psi[(size_t)j * ldpsi + i];
+        c->psi[(size_t)j * nb + i] = v;
+        thr[(size_t)j * nb + i] = (std::fabs(v) > 1.0e-10) ? v : 0.0;
+      }
+    for (int s = 0; s < ns; ++s) {
+      c->fods[s].resize(3 * (size_t)c->nfrm[s]);
+      for (int k = 0; k < c->nfrm[s]; ++k)
+        for (int d = 0; d < 3; ++d) c->fods[s][3 * k + d] = bfrm[((size_t)s * ldfrm + k) * 3 + d];
+    }
+    c->d_psi.upload(c->psi.data(), c->psi.size(), c->st);
+    c->d_psi_thr.upload(thr.data(), thr.size(), c->st);
+    c->have_orb = true;
+  });
+}
+
+int flosic_sic_gorbdrv(flosic_ctx* c, int nderv, int32_t* iupdat, int32_t* iallctr, int npts, const double* pts,
+                       int ifnct, double* grad) {
+  return guarded([&] {
+    require(c, false);
+    if (nderv < 0 || nderv > 2) fail(FLOSIC_ERR_ARG, "GORBDRV: INVALID VALUE FOR NDERV");
+    if (npts < 0 || npts > NSPEED) fail(FLOSIC_ERR_CAPACITY, "GORBDRV: NSPEED MUST BE AT LEAST NPTS");
+    if (ifnct < 1 || ifnct > c->ntypes) fail(FLOSIC_ERR_ARG, "GORBDRV: bad IFNCT");
+    if (!iupdat || !iallctr || !pts || !grad) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int t = ifnct - 1;
+    const TypeInfo& T = c->types[t];
+    const int nch = nderv == 0 ? 1 : (nderv == 1 ? 4 : 10);
+    // one-atom basis at the origin; points are relative to the atom already
+    int tz = t, boff = 0, poff = 0;
+    double origin[3] = {0, 0, 0};
+    DevBuf<double> pos, ptsd, out;
+    DevBuf<int> ty, bo, po;
+    pos.upload(origin, 3, c->st);
+    ty.upload(&tz, 1, c->st);
+    bo.upload(&boff, 1, c->st);
+    po.upload(&poff, 1, c->st);
+    std::vector<double> p(3 * (size_t)std::max(npts, 1));
+    for (int i = 0; i < npts; ++i)
+      for (int d = 0; d < 3; ++d) p[(size_t)d * npts + i] = pts[(size_t)d * NSPEED + i];
+    ptsd.upload(p.data(), p.size(), c->st);
+    BasisDev B = c->basis_dev();
+    B.natoms = 1;
+    B.nbasis = T.nloc;
+    B.atom_pos = pos.p;
+    B.atom_type = ty.p;
+    B.atom_boff = bo.p;
+    B.atom_poff = po.p;
+    out.ensure((size_t)nch * T.nloc * std::max(npts, 1));
+    launch_basis_values(B, nderv, npts, ptsd.p, ptsd.p + npts, ptsd.p + 2 * npts, out.p, npts, c->st);
+    std::vector<double> h((size_t)nch * T.nloc * std::max(npts, 1));
+    CUDA_CHECK(cudaMemcpyAsync(h.data(), out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    pos.release(); ptsd.release(); out.release(); ty.release(); bo.release(); po.release();
+    // GRAD(NSPEED,10,6,MAX_CON,3)
+    auto gi = [](int ipt, int igr, int ia, int nb, int l) {
+      return (((size_t)l * MAX_CON + nb) * 6 + ia) * 10 * NSPEED + (size_t)igr * NSPEED + ipt;
+    };
+    std::memset(grad, 0, sizeof(double) * (size_t)NSPEED * 10 * 6 * MAX_CON * 3);
+    int base = 0;
+    for (int l = 0; l <= T.lmax; ++l) {
+      for (int mu = 0; mu < kNcomp[l]; ++mu)
+        for (int cc = 0; cc < T.ncon[l]; ++cc)
+          for (int ch = 0; ch < nch; ++ch)
+            for (int i = 0; i < npts; ++i)
+              grad[gi(i, ch, mu, cc, l)] = h[((size_t)ch * T.nloc + base + mu * T.ncon[l] + cc) * npts + i];
+      base += kNcomp[l] * T.ncon[l];
+    }
+    // IUPDAT / IALLCTR screening flags (gorbdrv.f:183-220)
+    const double geps = std::exp(-CUTEXP);
+    bool up = false;
+    for (int l = 0; l < 3; ++l)
+      for (int cc = 0; cc < MAX_CON; ++cc) iallctr[l * MAX_CON + cc] = 0;
+    for (int ib = 0; ib < T.nbare; ++ib) {
+      bool icount = false;
+      std::vector<double> gaus(npts);
+      for (int i = 0; i < npts; ++i) {
+        const double r2 = pts[i] * pts[i] + pts[NSPEED + i] * pts[NSPEED + i] + pts[2 * NSPEED + i] * pts[2 * NSPEED + i];
+        const double rex = T.alp[ib] * r2;
+        gaus[i] = rex < CUTEXP ? std::exp(-rex) : 0.0;
+        if (rex < CUTEXP) icount = true;
+      }
+      if (!icount) continue;
+      up = true;
+      for (int l = 0; l <= T.lmax; ++l)
+        for (int cc = 0; cc < T.ncon[l]; ++cc)
+          for (int i = 0; i < npts; ++i)
+            if (std::fabs(T.con[l][cc][ib]) * gaus[i] > geps) iallctr[l * MAX_CON + cc] = 1;
+    }
+    *iupdat = up ? 1 : 0;
+  });
+}
+
+int flosic_sic_frmorb2_fmat(flosic_ctx* c, double* fmat, int ld) {
+  return guarded([&] {
+    require(c, true);
+    if (!fmat) fail(FLOSIC_ERR_ARG, "null array argument");
+    for (int s = 0; s < c->nspn; ++s) {
+      if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+      fo_setup(c, s);
+      const SpinCache& S = c->spin[s];
+      for (int K = 0; K < 4; ++K)
+        for (int j = 0; j < S.nf; ++j)
+          for (int w = 0; w < S.nw; ++w)
+            fmat[(((size_t)s * 4 + K) * ld + j) * ld + w] = S.fmat[((size_t)K * S.nf + j) * S.nw + w];
+    }
+  });
+}
+
+int flosic_sic_frmiorb(flosic_ctx* c, double* tmat, double* eval, int ld) {
+  return guarded([&] {
+    require(c, true);
+    if (!tmat || !eval) fail(FLOSIC_ERR_ARG, "null array argument");
+    for (int s = 0; s < c->nspn; ++s) {
+      if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+      fo_setup(c, s);
+      const SpinCache& S = c->spin[s];
+      for (int k = 0; k < S.nf; ++k) {
+        for (int w = 0; w < S.nw; ++w) tmat[((size_t)s * ld + w) * ld + k] = S.tmat[(size_t)k * S.nw + w];
+        eval[(size_t)s * ld + k] = S.lam[k];
+      }
+    }
+  });
+}
+
+int flosic_sic_coupot_sic(flosic_ctx* c, int kxxs, int kxxo, double* coulomb, double* rhog) {
+  return guarded([&] {
+    require(c, true);
+    if (kxxs < 1 || kxxs > c->nspn) fail(FLOSIC_ERR_ARG, "KXXS out of range");
+    const int s = kxxs - 1;
+    if (kxxo < 1 || kxxo > c->nfrm[s]) fail(FLOSIC_ERR_ARG, "KXXO out of range");
+    spin_potentials(c, s);
+    SpinCache& S = c->spin[s];
+    const int P = c->nmsh, k = kxxo - 1;
+    std::vector<double> v(P), r((size_t)10 * P, 0.0);
+    CUDA_CHECK(cudaMemcpyAsync(v.data(), S.vh.p + (size_t)k * P, sizeof(double) * P, cudaMemcpyDeviceToHost, c->st));
+    c->d_tmp.ensure((size_t)10 * P);
+    launch_density(P, S.nf, k, c->gga, S.phi.p, P, c->d_tmp.p, P, c->st);
+    const int nch = c->gga ? 10 : 1;
+    CUDA_CHECK(cudaMemcpyAsync(r.data(), c->d_tmp.p, sizeof(double) * nch * P, cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    S.pot_valid = false;  // the scratch buffer was reused
+    for (int i = 0; i < P; ++i) {
+      const int o = c->perm[i];
+      if (coulomb) coulomb[o] = v[i];
+      if (rhog)
+        for (int ch = 0; ch < 10; ++ch) rhog[(size_t)ch * P + o] = r[(size_t)ch * P + i];
+    }
+  });
+}
+
+int flosic_sic_getvlxc(flosic_ctx* c, int ndim, const double* rhog, double* vxc, double* ergs) {
+  return guarded([&] {
+    require(c, false);
+    if (ndim != c->nmsh) fail(FLOSIC_ERR_ARG, "NDIM must equal the mesh size");
+    if (!rhog || !vxc || !ergs) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int P = c->nmsh;
+    std::vector<double> r((size_t)10 * P);
+    for (int i = 0; i < P; ++i)
+      for (int ch = 0; ch < 10; ++ch) r[(size_t)ch * P + i] = rhog[(size_t)ch * ndim + c->perm[i]];
+    DevBuf<double> dr, dv;
+    dr.upload(r.data(), r.size(), c->st);
+    dv.ensure(2 * (size_t)P);
+    const int nblk = std::min(1024, (P + 255) / 256);
+    c->d_part.ensure((size_t)nblk * NPART);
+    c->d_sums.ensure(NPART);
+    launch_xc_rhog(c->mesh_dev(), c->gga, c->xc, dr.p, P, dv.p, c->d_part.p, nblk, c->st);
+    launch_reduce_parts(1, nblk, c->d_part.p, c->d_sums.p, c->st);
+    std::vector<double> v(2 * (size_t)P), sums(NPART);
+    CUDA_CHECK(cudaMemcpyAsync(v.data(), dv.p, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaMemcpyAsync(sums.data(), c->d_sums.p, sizeof(double) * NPART, cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    dr.release();
+    dv.release();
+    for (int i = 0; i < P; ++i) {
+      vxc[c->perm[i]] = v[i];
+      vxc[ndim + c->perm[i]] = v[P + i];
+    }
+    for (int j = 0; j < 4; ++j) ergs[j] = sums[4 + j];
+  });
+}
+
+int flosic_sic_apotnl_sic(flosic_ctx* c, double* totqnum, int lspx, int iorbx, double* results, double* cfrm,
+                          double* pot) {
+  return guarded([&] {
+    require(c, true);
+    if (lspx < 1 || lspx > c->nspn) fail(FLOSIC_ERR_ARG, "LSPX out of range");
+    const int s = lspx - 1;
+    if (iorbx == 0) fail(FLOSIC_ERR_ARG, "APOTNL_SIC is trying to run DFT calculation");
+    const int k = std::abs(iorbx) - 1;
+    if (k >= c->nfrm[s]) fail(FLOSIC_ERR_ARG, "IORBX out of range");
+    spin_potentials(c, s);
+    SpinCache& S = c->spin[s];
+    if (results)
+      for (int i = 0; i < 13; ++i) results[i] = S.results[(size_t)k * 13 + i];
+    if (cfrm)
+      for (int d = 0; d < 3; ++d) cfrm[d] = S.cfrm[(size_t)k * 3 + d];
+    if (totqnum) *totqnum = S.results[(size_t)k * 13 + 1];
+    if (pot) {
+      const int P = c->nmsh;
+      std::vector<double> v(P);
+      CUDA_CHECK(cudaMemcpyAsync(v.data(), S.vpot.p + (size_t)k * P, sizeof(double) * P, cudaMemcpyDeviceToHost, c->st));
+      CUDA_CHECK(cudaStreamSynchronize(c->st));
+      for (int i = 0; i < P; ++i) pot[c->perm[i]] = v[i];
+    }
+  });
+}
+
+int flosic_sic_siclagm(flosic_ctx* c, int lspn, double* sic, int ld) {
+  return guarded([&] {
+    require(c, true);
+    if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
+    const int s = lspn - 1;
+    if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+    if (!sic) fail(FLOSIC_ERR_ARG, "null array argument");
+    spin_sic(c, s);
+    const SpinCache& S = c->spin[s];
+    for (int l = 0; l < S.nf; ++l)
+      for (int j = 0; j < S.nf; ++j) sic[(size_t)l * ld + j] = S.sic[(size_t)l * S.nf + j];
+  });
+}
+
+int flosic_sic_frmorb2_force(flosic_ctx* c, int lspn, const double* sic, int ld, double* debdax) {
+  return guarded([&] {
+    require(c, true);
+    if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
+    const int s = lspn - 1;
+    if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+    if (!sic || !debdax) fail(FLOSIC_ERR_ARG, "null array argument");
+    std::vector<double> deb(3 * (size_t)c->nfrm[s]);
+    spin_force(c, s, sic, ld, deb.data());
+    for (int k = 0; k < c->nfrm[s]; ++k)
+      for (int d = 0; d < 3; ++d) debdax[3 * (size_t)k + d] = deb[3 * (size_t)k + d];
+  });
+}
+
+int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double* debdax, double* cfrm,
+                     double* esic) {
+  return guarded([&] {
+    require(c, true);
+    if (!results || !sic || !debdax || !cfrm || !esic) fail(FLOSIC_ERR_ARG, "null array argument");
+    for (int s = 0; s < c->nspn; ++s)
+      if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+    c->launches = 0;
+    for (double& m : c->stage_ms) m = 0.0;
+    invalidate(c);
+    double zsic = 0.0;
+    for (int s = 0; s < c->nspn; ++s) {
+      const int nf = c->nfrm[s];
+      if (nf == 0) continue;
+      spin_sic(c, s);
+      const SpinCache& S = c->spin[s];
+      for (int k = 0; k < nf; ++k) {
+        for (int i = 0; i < 13; ++i) results[((size_t)s * ld + k) * 13 + i] = S.results[(size_t)k * 13 + i];
+        for (int d = 0; d < 3; ++d) cfrm[((size_t)s * ld + k) * 3 + d] = S.cfrm[(size_t)k * 3 + d];
+        zsic += S.results[(size_t)k * 13 + 8];
+      }
+      double* ps = sic + (size_t)s * ld * ld;
+      for (int l = 0; l < nf; ++l)
+        for (int j = 0; j < nf; ++j) ps[(size_t)l * ld + j] = S.sic[(size_t)l * nf + j];
+      spin_force(c, s, ps, ld, debdax + (size_t)s * ld * 3);
+    }
+    *esic = zsic;
+  });
+}
+
+int flosic_sic_stats(flosic_ctx* c, int64_t* launches, double* stage_ms, int64_t* npairs, int64_t* ncalls) {
+  if (!c) return FLOSIC_ERR_ARG;
+  if (launches) *launches = c->launches;
+  if (stage_ms)
+    for (int i = 0; i < 7; ++i) stage_ms[i] = c->stage_ms[i];
+  if (npairs) *npairs = (int64_t)c->pairs.size();
+  if (ncalls) *ncalls = (int64_t)c->calls.size();
+  return FLOSIC_OK;
+}
+
+}  // extern "C"

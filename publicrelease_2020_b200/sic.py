@@ -1,0 +1,208 @@
+"""Python binding of libflosic_sic_b200 (ctypes over the C ABI in
+include/flosic_sic.h).
+
+The methods keep the names and argument meaning of the reference routines
+they replace (APOTNL_SIC, COUPOT_SIC, GETVLXC, SICLAGM, FRMORB2, FRMIORB,
+GORBDRV in FLOSIC/PublicRelease_2020 flosic/), with numpy arrays in place of
+the Fortran module state.  Errors from the library are raised as
+``FlosicError`` carrying the library's status code, mirroring the reference's
+STOPIT on the same conditions.  There is no CPU implementation behind this
+class: without the CUDA library or a GPU it raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libflosic_sic_b200.so")
+
+ERRORS = {
+    1: "FLOSIC_ERR_ARG", 2: "FLOSIC_ERR_CAPACITY", 3: "FLOSIC_ERR_LOWDEN", 4: "FLOSIC_ERR_ZERO_DENSITY",
+    5: "FLOSIC_ERR_NFRM", 6: "FLOSIC_ERR_ZERO_COULOMB", 7: "FLOSIC_ERR_CUDA", 8: "FLOSIC_ERR_STATE",
+}
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64 = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+EXPORTS = [
+    "flosic_sic_create", "flosic_sic_destroy", "flosic_sic_last_error", "flosic_sic_set_geometry",
+    "flosic_sic_set_orbitals", "flosic_sic_gorbdrv", "flosic_sic_frmorb2_fmat", "flosic_sic_frmiorb",
+    "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
+    "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats",
+]
+
+_lib = None
+
+
+class FlosicError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load_library(path=LIB_PATH):
+    """Load the CUDA library and declare the C ABI (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run __graft_entry__.build() (no CPU fallback exists)")
+    L = C.CDLL(path)
+    L.flosic_sic_create.argtypes = [C.c_int, C.POINTER(_vp)]
+    L.flosic_sic_destroy.argtypes = [_vp]
+    L.flosic_sic_last_error.restype = C.c_char_p
+    L.flosic_sic_set_geometry.argtypes = [_vp, C.c_int, _ip, _dp, C.c_int, _ip, _dp, _ip, _dp, C.c_int, _dp, _dp,
+                                          C.c_int, _ip, _ip]
+    L.flosic_sic_set_orbitals.argtypes = [_vp, _ip, _dp, C.c_int, _ip, _dp, C.c_int]
+    L.flosic_sic_gorbdrv.argtypes = [_vp, C.c_int, _ip, _ip, C.c_int, _dp, C.c_int, _dp]
+    L.flosic_sic_frmorb2_fmat.argtypes = [_vp, _dp, C.c_int]
+    L.flosic_sic_frmiorb.argtypes = [_vp, _dp, _dp, C.c_int]
+    L.flosic_sic_coupot_sic.argtypes = [_vp, C.c_int, C.c_int, _dp, _dp]
+    L.flosic_sic_getvlxc.argtypes = [_vp, C.c_int, _dp, _dp, _dp]
+    L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
+    L.flosic_sic_siclagm.argtypes = [_vp, C.c_int, _dp, C.c_int]
+    L.flosic_sic_frmorb2_force.argtypes = [_vp, C.c_int, _dp, C.c_int, _dp]
+    L.flosic_sic_cycle.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
+    L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64]
+    _lib = L
+    return L
+
+
+class FlosicSIC:
+    """One GPU context holding the SIC-path module state."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        h = _vp()
+        self._check(self.L.flosic_sic_create(int(device), C.byref(h)))
+        self.h = h
+        self.sysm = None
+        self.ld = 1
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.flosic_sic_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise FlosicError(rc, self.L.flosic_sic_last_error().decode())
+
+    # -- module state ------------------------------------------------------
+    def set_geometry(self, sysm):
+        ix, idx, ic, idc = sysm.xc
+        self.sysm = sysm
+        self._check(self.L.flosic_sic_set_geometry(
+            self.h, sysm.natoms, np.ascontiguousarray(sysm.atom_type + 1, dtype=np.int32),
+            np.ascontiguousarray(sysm.rat, dtype=np.float64), sysm.ntypes,
+            np.ascontiguousarray(sysm.n_bare, dtype=np.int32), np.ascontiguousarray(sysm.bfalp),
+            np.ascontiguousarray(sysm.n_con, dtype=np.int32), np.ascontiguousarray(sysm.bfcon), sysm.nmsh,
+            np.ascontiguousarray(sysm.rmsh), np.ascontiguousarray(sysm.wmsh), sysm.nspn,
+            np.array([ix, ic], dtype=np.int32), np.array([idx, idc], dtype=np.int32)))
+
+    def set_orbitals(self, psi, nwfs, fods):
+        nf = np.array([len(f) for f in fods] + [0] * (2 - len(fods)), dtype=np.int32)
+        self.ld = max(int(nf.max()), 1)
+        bfrm = np.zeros((2, self.ld, 3))
+        for s, f in enumerate(fods):
+            bfrm[s, : len(f)] = f
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        self._check(self.L.flosic_sic_set_orbitals(self.h, np.array(list(nwfs) + [0] * (2 - len(nwfs)), dtype=np.int32),
+                                                   psi, psi.shape[1], nf, bfrm, self.ld))
+        self.nfrm = tuple(int(x) for x in nf)
+
+    # -- reference routines ------------------------------------------------
+    def gorbdrv(self, nderv, pts, ifnct):
+        """GORBDRV: pts (npts<=25, 3) relative to the atom of function set ifnct (1-based);
+        returns GRAD(25,10,6,15,3) as a C array [3][15][6][10][25], IUPDAT, IALLCTR(15,3)."""
+        P = np.zeros((3, 25))
+        P[:, : len(pts)] = np.asarray(pts).T
+        grad = np.zeros(25 * 10 * 6 * 15 * 3)
+        iup = np.zeros(1, dtype=np.int32)
+        iall = np.zeros(45, dtype=np.int32)
+        self._check(self.L.flosic_sic_gorbdrv(self.h, nderv, iup, iall, len(pts), np.ascontiguousarray(P), ifnct, grad))
+        return grad.reshape(3, 15, 6, 10, 25), bool(iup[0]), iall.reshape(3, 15)
+
+    def frmorb2_fmat(self):
+        out = np.zeros(2 * 4 * self.ld * self.ld)
+        self._check(self.L.flosic_sic_frmorb2_fmat(self.h, out, self.ld))
+        return out.reshape(2, 4, self.ld, self.ld)
+
+    def frmiorb(self):
+        tm = np.zeros(2 * self.ld * self.ld)
+        ev = np.zeros(2 * self.ld)
+        self._check(self.L.flosic_sic_frmiorb(self.h, tm, ev, self.ld))
+        return tm.reshape(2, self.ld, self.ld), ev.reshape(2, self.ld)
+
+    def coupot_sic(self, kxxs, kxxo):
+        n = self.sysm.nmsh
+        coul = np.zeros(n)
+        rhog = np.zeros(10 * n)
+        self._check(self.L.flosic_sic_coupot_sic(self.h, kxxs, kxxo, coul, rhog))
+        return coul, rhog.reshape(10, n)
+
+    def getvlxc(self, rhog):
+        n = self.sysm.nmsh
+        vxc = np.zeros(2 * n)
+        ergs = np.zeros(4)
+        self._check(self.L.flosic_sic_getvlxc(self.h, n, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
+                                              vxc, ergs))
+        return vxc.reshape(2, n), ergs
+
+    def apotnl_sic(self, lspx, iorbx):
+        n = self.sysm.nmsh
+        totq = np.zeros(1)
+        res = np.zeros(13)
+        cf = np.zeros(3)
+        pot = np.zeros(n)
+        self._check(self.L.flosic_sic_apotnl_sic(self.h, totq, lspx, iorbx, res, cf, pot))
+        return dict(totqnum=float(totq[0]), results=res, cfrm=cf, pot=pot)
+
+    def siclagm(self, lspn):
+        sic = np.zeros(self.ld * self.ld)
+        self._check(self.L.flosic_sic_siclagm(self.h, lspn, sic, self.ld))
+        return sic.reshape(self.ld, self.ld)
+
+    def frmorb2_force(self, lspn, sic):
+        deb = np.zeros(3 * self.ld)
+        self._check(self.L.flosic_sic_frmorb2_force(self.h, lspn, np.ascontiguousarray(sic, dtype=np.float64).reshape(-1),
+                                                    self.ld, deb))
+        return deb.reshape(self.ld, 3)
+
+    def cycle(self, out=None):
+        ld = self.ld
+        if out is None:
+            out = dict(results=np.zeros(2 * ld * 13), sic=np.zeros(2 * ld * ld), debdax=np.zeros(2 * ld * 3),
+                       cfrm=np.zeros(2 * ld * 3), esic=np.zeros(1))
+        self._check(self.L.flosic_sic_cycle(self.h, ld, out["results"], out["sic"], out["debdax"], out["cfrm"],
+                                            out["esic"]))
+        return dict(results=out["results"].reshape(2, ld, 13), sic=out["sic"].reshape(2, ld, ld),
+                    debdax=out["debdax"].reshape(2, ld, 3), cfrm=out["cfrm"].reshape(2, ld, 3),
+                    esic=float(out["esic"][0]))
+
+    def stats(self):
+        la = np.zeros(1, dtype=np.int64)
+        ms = np.zeros(7)
+        npairs = np.zeros(1, dtype=np.int64)
+        ncalls = np.zeros(1, dtype=np.int64)
+        self._check(self.L.flosic_sic_stats(self.h, la, ms, npairs, ncalls))
+        return dict(launches=int(la[0]), stage_ms=ms, npairs=int(npairs[0]), ncalls=int(ncalls[0]))
+
+
+def open_system(sysm, device=0):
+    """Context with geometry and orbitals of a workloads.System loaded."""
+    ctx = FlosicSIC(device)
+    ctx.set_geometry(sysm)
+    ctx.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
+    return ctx

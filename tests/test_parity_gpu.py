@@ -1,0 +1,139 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle on
+the same seeded inputs.
+
+Tolerances (FP64 path): the GPU forms the FO density as phi^2 from the
+orbital values, the reference (and the oracle) from the Gaussian-pair
+polynomials at near points only; both are exact to ~1e-13 relative.  Summation
+orders differ (spatially tiled mesh, tree reductions).  Per-point potentials
+are compared at 1e-9 relative to the potential scale, energies at 1e-10 Ha
+absolute, SIC-matrix entries at 1e-9 relative to the matrix scale, forces at
+1e-8 Ha/bohr."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from publicrelease_2020_b200 import sic as S
+from publicrelease_2020_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-10      # Ha, energies and RESULTS entries
+POT_RTOL = 1e-9    # potentials, relative to max |V|
+SIC_RTOL = 1e-9    # SIC matrix, relative to max |lambda|
+F_TOL = 1e-8       # Ha/bohr, FOD forces
+
+
+def systems():
+    return {
+        "water_lda_nspn2": W.water(seed=0, nrad=18),
+        "synthetic_pbe_nspn1": W.small_synthetic(seed=5, natoms=3, nbasis=24, nmsh=5000, nfo=4),
+        "synthetic_pw91gga_nspn2": W.small_synthetic(seed=7, natoms=3, nbasis=30, nmsh=4000, nfo=3,
+                                                     functional="GGA-PW91*GGA-PW91", nspn=2),
+    }
+
+
+@pytest.fixture(scope="module", params=list(systems().keys()))
+def pair(request):
+    sysm = systems()[request.param]
+    ctx = S.open_system(sysm)
+    orc = O.Oracle(sysm)
+    yield request.param, sysm, ctx, orc
+    ctx.close()
+
+
+def test_cycle_matches_oracle(pair):
+    name, sysm, ctx, orc = pair
+    g = ctx.cycle()
+    r = orc.sic_cycle(nthreads=8)
+    for s in range(sysm.nspn):
+        n = sysm.nfrm[s]
+        gr, orr = g["results"][s][:n], r["results"][s][:n]
+        assert np.allclose(gr[:, 0], orr[:, 0])
+        assert np.max(np.abs(gr[:, 1:] - orr[:, 1:])) < E_TOL * max(1.0, np.abs(orr[:, 1:]).max()), name
+        lam_g, lam_o = g["sic"][s][:n, :n], r["sic"][s][:n, :n]
+        assert np.max(np.abs(lam_g - lam_o)) < SIC_RTOL * np.abs(lam_o).max(), name
+        assert np.max(np.abs(g["debdax"][s][:n] - r["debdax"][s][:n])) < F_TOL * max(1.0, np.abs(r["debdax"][s]).max())
+        assert np.max(np.abs(g["cfrm"][s][:n] - r["cfrm"][s][:n])) < 1e-9
+    assert abs(g["esic"] - r["esic"]) < E_TOL * max(1.0, sysm.nspn * max(sysm.nfrm))
+
+
+def test_coupot_and_potential_match_oracle(pair):
+    name, sysm, ctx, orc = pair
+    for k in range(1, sysm.nfrm[0] + 1):
+        cg, rg = ctx.coupot_sic(1, k)
+        co, ro, _ = orc.coupot_sic(1, k)
+        assert np.max(np.abs(cg - co)) < POT_RTOL * np.abs(co).max(), (name, k)
+        nch = 10 if sysm.xc[0] or sysm.xc[2] else 1
+        assert np.max(np.abs(rg[:nch] - ro[:nch])) < 1e-10 * np.abs(ro[0]).max() + 1e-13, (name, k)
+        a = ctx.apotnl_sic(1, k)
+        b = orc.apotnl_sic(1, k)
+        assert np.max(np.abs(a["pot"] - b["pot"])) < POT_RTOL * np.abs(b["pot"]).max(), (name, k)
+        assert np.max(np.abs(a["results"][1:] - b["results"][1:])) < E_TOL * max(1.0, np.abs(b["results"]).max())
+
+
+def test_fo_construction_matches_oracle(pair):
+    name, sysm, ctx, orc = pair
+    fg = ctx.frmorb2_fmat()
+    fo = orc.fmat()
+    tg, eg = ctx.frmiorb()
+    to, eo = orc.frmiorb()
+    for s in range(sysm.nspn):
+        n = sysm.nfrm[s]
+        assert np.allclose(fg[s, :, :n, :n], fo[s, :, :n, :n], rtol=1e-11, atol=1e-11)
+        assert np.allclose(tg[s, :n, :n], to[s, :n, :n], rtol=1e-10, atol=1e-10)
+        assert np.allclose(np.sort(eg[s, :n]), np.sort(eo[s, :n]), rtol=1e-11)
+
+
+def test_getvlxc_matches_oracle(pair):
+    name, sysm, ctx, orc = pair
+    _, rho, _ = orc.coupot_sic(1, 1)
+    vg, eg = ctx.getvlxc(rho)
+    vo, eo = orc.getvlxc_sic(rho)
+    assert np.max(np.abs(vg[0] - vo[0])) < 1e-10 * np.abs(vo[0]).max()
+    assert np.max(np.abs(eg - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+
+
+def test_gorbdrv_matches_oracle(pair):
+    name, sysm, ctx, orc = pair
+    rng = np.random.default_rng(3)
+    pts = rng.normal(0, 0.8, (25, 3))
+    for nderv in (0, 1, 2):
+        for ifnct in range(1, min(sysm.ntypes, 3) + 1):
+            gg, ug, ag = ctx.gorbdrv(nderv, pts, ifnct)
+            go, uo, ao = orc.gorbdrv(nderv, pts, ifnct)
+            nch = (1, 4, 10)[nderv]
+            assert ug == uo
+            assert np.array_equal(ag, ao)
+            a, b = gg[:, :, :, :nch, :], go[:, :, :, :nch, :]
+            assert np.max(np.abs(a - b)) < 1e-12 * max(1.0, np.abs(b).max())
+
+
+def test_siclagm_and_force_entry_points(pair):
+    name, sysm, ctx, orc = pair
+    for s in range(1, sysm.nspn + 1):
+        lam = ctx.siclagm(s)
+        n = sysm.nfrm[s - 1]
+        pots = np.stack([orc.apotnl_sic(s, k)["pot"] for k in range(1, n + 1)])
+        lo = orc.siclagm(s, pots)
+        assert np.max(np.abs(lam[:n, :n] - lo[:n, :n])) < SIC_RTOL * np.abs(lo[:n, :n]).max()
+        fg = ctx.frmorb2_force(s, lo)
+        fo = orc.frmorb2_force(s, lo)
+        assert np.max(np.abs(fg[:n] - fo[:n])) < 1e-9 * max(1.0, np.abs(fo[:n]).max())
+
+
+def test_error_codes():
+    sysm = W.water(seed=0, nrad=12)
+    ctx = S.open_system(sysm)
+    f = [x.copy() for x in sysm.fods]
+    f[0][1] = f[0][0]
+    ctx.set_orbitals(sysm.psi, sysm.nwfs, f)
+    with pytest.raises(S.FlosicError) as e:
+        ctx.frmiorb()
+    assert e.value.code == 3  # FLOSIC_ERR_LOWDEN
+    with pytest.raises(S.FlosicError) as e:
+        ctx.set_orbitals(sysm.psi, (5, 4), sysm.fods)
+    assert e.value.code == 5  # FLOSIC_ERR_NFRM
+    with pytest.raises(S.FlosicError) as e:
+        ctx.apotnl_sic(1, 99)
+    assert e.value.code in (1, 8)
+    ctx.close()

@@ -1,0 +1,307 @@
+#!/usr/bin/env python
+"""Benchmark: seconds per FLO-SIC SCF cycle (all FOs + FOD forces) on B200.
+
+A step is one SIC block of an SCF iteration (main.F:577-759): FO construction,
+APOTNL_SIC for every FO (basis values, Gaussian-pair Coulomb potential, XC),
+the SIC matrix and the FOD forces, through the C ABI (flosic_sic_cycle).
+
+Workload (N=1): the synthetic kernel shape -- 40 atoms in a 12 A cube, 512
+contracted s/p/d functions (3 primitives each, exponents log-uniform in
+[0.05, 1e4]), 1,000,000 mesh points, 128 FOs, PBE -- generated from a seed
+(there is no dataset); the FP64 path.  Multi-GPU (torchrun): every rank runs
+its own SCF cycle on its own GPU (replicas, no data-path collective);
+value = max-over-ranks time / N.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s per FLO-SIC SCF cycle (all FOs + FOD forces)"
+COULOMB_FLOPS_NEAR = 200.0   # per near (pair, point, FO): work model of the Gaussian-pair Poisson solver
+COULOMB_FLOPS_FAR = 98.0     # per far (call, point, FO): 2*49 multipole terms
+
+
+def workload(name):
+    from publicrelease_2020_b200 import workloads as W
+    if name == "c2":
+        return W.synthetic(natoms=40, nbasis=512, nmsh=1_000_000, nfo=128, seed=1), \
+            dict(workload="synthetic C2: 40 atoms, 512 s/p/d functions (3 prims), 1e6 mesh points, 128 FOs, PBE",
+                 atoms=40, nbasis=512, nmsh=1_000_000, nfo=128, functional="GGA-PBE*GGA-PBE", nspn=1)
+    if name == "c2half":
+        return W.synthetic(natoms=40, nbasis=512, nmsh=250_000, nfo=128, seed=1), \
+            dict(workload="synthetic C2 shape on a 2.5e5-point mesh", atoms=40, nbasis=512, nmsh=250_000, nfo=128,
+                 functional="GGA-PBE*GGA-PBE", nspn=1)
+    if name == "c2tiny":
+        return W.synthetic(natoms=40, nbasis=512, nmsh=20_000, nfo=128, seed=1), \
+            dict(workload="synthetic C2 shape on a 2e4-point mesh (profiling case)", atoms=40, nbasis=512,
+                 nmsh=20_000, nfo=128, functional="GGA-PBE*GGA-PBE", nspn=1)
+    if name == "water":
+        s = W.water(seed=0, nrad=40)
+        return s, dict(workload="water LDA-PW91, 5+5 FODs", atoms=3, nbasis=s.nbasis, nmsh=s.nmsh, nfo=5,
+                       functional="LDA-PW91*LDA-PW91", nspn=2)
+    if name == "small":
+        s = W.small_synthetic(seed=5, natoms=6, nbasis=60, nmsh=40000, nfo=12)
+        return s, dict(workload="small synthetic", atoms=6, nbasis=60, nmsh=40000, nfo=12,
+                       functional="GGA-PBE*GGA-PBE", nspn=1)
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for n, v in zip(names, r[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 throughput of cuBLAS DGEMM on this GPU (roofline denominator
+    for the FP64 Coulomb kernel; MEASURED_PEAKS.json carries no FP64 figure)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(5):
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(sysm, threads, budget_s=20.0):
+    """The oracle (the reference algorithm restated in C++) timed on the host
+    cores on a bounded sample: the same system on every m-th mesh point, a
+    subset of the FOs; seconds scaled to one full SCF cycle."""
+    from oracle import oracle as O
+    import copy
+    sub = copy.copy(sysm)
+    stride = max(1, sysm.nmsh // 20000)
+    sub.rmsh = np.ascontiguousarray(sysm.rmsh[::stride])
+    sub.wmsh = np.ascontiguousarray(sysm.wmsh[::stride] * stride)
+    nf = max(sysm.nfrm)
+    nrun = min(nf, max(1, threads))
+    orc = O.Oracle(sub)
+    t0 = time.perf_counter()
+    orc.sic_cycle(nthreads=threads, fo_limit=nrun if nrun < nf else 0)
+    dt = time.perf_counter() - t0
+    nfo_total = sum(sysm.nfrm)
+    scale = (sysm.nmsh / sub.nmsh) * (nfo_total / (nrun * sysm.nspn if nrun < nf else nfo_total))
+    return dt * scale, dict(points=sub.nmsh, fos=nrun if nrun < nf else nfo_total, seconds=dt)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sysm, cfg = workload(args.workload)
+    threads = os.cpu_count() or 1
+    vals = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        v, sample = cpu_baseline(sysm, threads)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    cfg["parallelism"] = "host threads"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": f"oracle (reference algorithm restated in C++) on {sample['points']} of "
+                                   f"{sysm.nmsh} mesh points and {sample['fos']} FOs, scaled to one cycle"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from publicrelease_2020_b200 import sic as S
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    sysm, cfg = workload(args.workload)
+    ctx = S.FlosicSIC(local_rank)
+    ctx.set_geometry(sysm)
+    ctx.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
+    ld = ctx.ld
+    out = dict(results=np.zeros(2 * ld * 13), sic=np.zeros(2 * ld * ld), debdax=np.zeros(2 * ld * 3),
+               cfrm=np.zeros(2 * ld * 3), esic=np.zeros(1))
+    for _ in range(args.warmup):
+        ctx.cycle(out)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # timed region: inputs resident in GPU memory
+    st_acc = dict(coul_ms=0.0, near=0, far=0, launches=0, stage=np.zeros(7))
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            r = ctx.cycle(out)
+            st = ctx.stats()
+            st_acc["coul_ms"] += st["stage_ms"][3]
+            st_acc["near"] += st["near_evals"]
+            st_acc["far"] += st["far_evals"]
+            st_acc["launches"] += st["launches"]
+            st_acc["stage"] += st["stage_ms"]
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+    t_ms = e0.elapsed_time(e1)
+    # e2e: host buffers through the C ABI (KS orbitals + FODs in, results out)
+    psi = np.ascontiguousarray(sysm.psi)
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        ctx.set_orbitals(psi, sysm.nwfs, sysm.fods)
+        ctx.cycle(out)
+    f1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+    h2d = psi.nbytes + 8 * 3 * ld * 2
+    d2h = sum(v.nbytes for v in out.values())
+    if dist is not None:
+        t = torch.tensor([t_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, e2e_ms = float(t[0]), float(t[1])
+    ctx_stats = ctx.stats()
+    esic = r["esic"]
+    ctx.close()
+    if rank != 0:
+        return
+    per_step_s = t_ms / 1e3 / args.steps
+    value = per_step_s / world
+    coul_s = st_acc["coul_ms"] / 1e3 / args.steps
+    flops = (st_acc["near"] * COULOMB_FLOPS_NEAR + st_acc["far"] * COULOMB_FLOPS_FAR) / args.steps
+    peak = fp64_peak_tflops(torch)
+    achieved = flops / coul_s / 1e12 if coul_s > 0 else 0.0
+    cfg.update(parallelism=f"replicas x{world}" if world > 1 else "single GPU", l2="working set >> L2 (126 MB)",
+               npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision="fp64")
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": cfg,
+        "e2e": {"value": e2e_ms / 1e3 / args.steps / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(st_acc["launches"]),
+        "roofline": {"bound": "tensor", "kernel": "k_coulomb_eval", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                     "peak_kind": "FP64 cuBLAS DGEMM measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                     "work": f"{st_acc['near'] / args.steps:.4g} near (pair,point,FO) x {COULOMB_FLOPS_NEAR:.0f} + "
+                             f"{st_acc['far'] / args.steps:.4g} far (call,point,FO) x {COULOMB_FLOPS_FAR:.0f} flops"},
+        "stage_ms": {k: round(float(v) / args.steps, 3) for k, v in
+                     zip(["fo", "orbitals", "coul_setup", "coul_eval", "xc", "sicmat", "forces"], st_acc["stage"])},
+        "esic": esic,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        cb, sample = cpu_baseline(sysm, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": cb, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"oracle on {sample['points']} of {sysm.nmsh} mesh points, {sample['fos']} "
+                                          f"FOs ({sample['seconds']:.1f} s), scaled to one cycle"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "water", "small"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

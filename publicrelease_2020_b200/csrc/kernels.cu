@@ -715,6 +715,26 @@ void launch_coulomb_eval(int ncalls, const CallInfo* calls, const PairGeo* pairs
                                              ldv);
 }
 
+// Algorithmic work of the Coulomb evaluation: near (pair, point, FO) and far
+// (call, point, FO) evaluations; cnt[0] += near, cnt[1] += far.
+__global__ void k_work_counts(int ncalls, const CallInfo* __restrict__ calls, int nfo, int npts,
+                              const CallFO* __restrict__ cfo, unsigned long long* __restrict__ cnt) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)ncalls * nfo) return;
+  const int c = (int)(i / nfo);
+  const CallFO f = cfo[i];
+  const unsigned long long nearp = (unsigned long long)(npts - f.nfar);
+  atomicAdd(&cnt[0], nearp * (unsigned long long)calls[c].np);
+  atomicAdd(&cnt[1], (unsigned long long)f.nfar);
+}
+
+void launch_work_counts(int ncalls, const CallInfo* calls, int nfo, int npts, const CallFO* cfo,
+                        unsigned long long* cnt, cudaStream_t st) {
+  const size_t n = (size_t)ncalls * nfo;
+  if (n == 0) return;
+  k_work_counts<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ncalls, calls, nfo, npts, cfo, cnt);
+}
+
 // ---------------------------------------------------------------------------
 // XC, SIC potential and energy partial sums
 // ---------------------------------------------------------------------------

@@ -55,6 +55,9 @@ void launch_coulomb_eval(int ncalls, const CallInfo* calls, const PairGeo* pairs
                          const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* mom,
                          const MeshDev& M, const double* boys_tab, double* vh, int ldv, cudaStream_t st);
 
+void launch_work_counts(int ncalls, const CallInfo* calls, int nfo, int npts, const CallFO* cfo,
+                        unsigned long long* cnt, cudaStream_t st);
+
 // Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as
 // in apotnl_sic.F:419) from the FO values/derivatives phi[(ch*nfo+k)*ldp+p];
 // writes the SIC potential V = Vxc + VH*nspn/2 and Y = w V phi, and per-block

@@ -350,6 +350,8 @@ struct flosic_ctx {
   // scratch
   DevBuf<double> d_basis, d_fodpts, d_psig, d_tmat, d_u, d_coef, d_cgp, d_mom, d_part, d_sums, d_sic, d_tmp;
   DevBuf<int8_t> d_maxfmt;
+  DevBuf<unsigned long long> d_cnt;
+  unsigned long long work_near = 0, work_far = 0;
   DevBuf<CallFO> d_callfo;
   // stats
   long long launches = 0;
@@ -723,6 +725,15 @@ void coulomb(flosic_ctx* c, int s) {
   launch_coulomb_eval(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
                       c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
   c->launches++;
+  c->d_cnt.ensure(2);
+  CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 2 * sizeof(unsigned long long), st));
+  launch_work_counts(ncalls, c->d_calls.p, nf, P, c->d_callfo.p, c->d_cnt.p, st);
+  c->launches++;
+  unsigned long long cnt[2];
+  CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  CUDA_CHECK(cudaStreamSynchronize(st));
+  c->work_near += cnt[0];
+  c->work_far += cnt[1];
   CUDA_CHECK(cudaGetLastError());
 }
 
@@ -993,7 +1004,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_boys.release(); c->d_pairs.release(); c->d_calls.release(); c->d_psi.release(); c->d_psi_thr.release();
   c->d_basis.release(); c->d_fodpts.release(); c->d_psig.release(); c->d_tmat.release(); c->d_u.release();
   c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
-  c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release();
+  c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release();
   if (c->blas) cublasDestroy(c->blas);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -1275,7 +1286,6 @@ int flosic_sic_coupot_sic(flosic_ctx* c, int kxxs, int kxxo, double* coulomb, do
     const int nch = c->gga ? 10 : 1;
     CUDA_CHECK(cudaMemcpyAsync(r.data(), c->d_tmp.p, sizeof(double) * nch * P, cudaMemcpyDeviceToHost, c->st));
     CUDA_CHECK(cudaStreamSynchronize(c->st));
-    S.pot_valid = false;  // the scratch buffer was reused
     for (int i = 0; i < P; ++i) {
       const int o = c->perm[i];
       if (coulomb) coulomb[o] = v[i];
@@ -1378,6 +1388,7 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
     for (int s = 0; s < c->nspn; ++s)
       if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
     c->launches = 0;
+    c->work_near = c->work_far = 0;
     for (double& m : c->stage_ms) m = 0.0;
     invalidate(c);
     double zsic = 0.0;
@@ -1400,8 +1411,13 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
   });
 }
 
-int flosic_sic_stats(flosic_ctx* c, int64_t* launches, double* stage_ms, int64_t* npairs, int64_t* ncalls) {
+int flosic_sic_stats(flosic_ctx* c, int64_t* launches, double* stage_ms, int64_t* npairs, int64_t* ncalls,
+                     int64_t* work) {
   if (!c) return FLOSIC_ERR_ARG;
+  if (work) {
+    work[0] = (int64_t)c->work_near;
+    work[1] = (int64_t)c->work_far;
+  }
   if (launches) *launches = c->launches;
   if (stage_ms)
     for (int i = 0; i < 7; ++i) stage_ms[i] = c->stage_ms[i];

@@ -68,7 +68,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_siclagm.argtypes = [_vp, C.c_int, _dp, C.c_int]
     L.flosic_sic_frmorb2_force.argtypes = [_vp, C.c_int, _dp, C.c_int, _dp]
     L.flosic_sic_cycle.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
-    L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64]
+    L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64, _i64]
     _lib = L
     return L
 
@@ -196,8 +196,10 @@ class FlosicSIC:
         ms = np.zeros(7)
         npairs = np.zeros(1, dtype=np.int64)
         ncalls = np.zeros(1, dtype=np.int64)
-        self._check(self.L.flosic_sic_stats(self.h, la, ms, npairs, ncalls))
-        return dict(launches=int(la[0]), stage_ms=ms, npairs=int(npairs[0]), ncalls=int(ncalls[0]))
+        work = np.zeros(2, dtype=np.int64)
+        self._check(self.L.flosic_sic_stats(self.h, la, ms, npairs, ncalls, work))
+        return dict(launches=int(la[0]), stage_ms=ms, npairs=int(npairs[0]), ncalls=int(ncalls[0]),
+                    near_evals=int(work[0]), far_evals=int(work[1]))
 
 
 def open_system(sysm, device=0):

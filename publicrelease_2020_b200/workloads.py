@@ -374,12 +374,35 @@ def synthetic(natoms=40, nbasis=512, nmsh=1_000_000, nfo=128, box_ang=12.0, seed
     C = orthonormal_orbitals(sysm, nfo * nspn, rng)
     sysm.psi = C
     sysm.nwfs = (nfo, nfo if nspn == 2 else 0)
-    fods = []
-    for s in range(nspn):
-        at = rng.integers(0, natoms, nfo)
-        fods.append(rat[at] + rng.normal(0, 0.6, (nfo, 3)))
-    sysm.fods = fods
+    sysm.fods = [place_fods(sysm, C[s * nfo:(s + 1) * nfo], rng) for s in range(nspn)]
     return sysm
+
+
+def place_fods(sysm, C, rng, min_eig=1e-3, tries=200):
+    """FODs near the atoms, redrawn one at a time until the Fermi-orbital
+    overlap T T^T (frmiorb.f:426-438) is safely non-singular."""
+    nfo = C.shape[0]
+    at = rng.integers(0, sysm.natoms, nfo)
+    fods = sysm.rat[at] + rng.normal(0, 0.6, (nfo, 3))
+
+    def lowden_min(f):
+        psi = basis_values(sysm, f) @ C.T            # (nfod, nwf)
+        rho = np.einsum("ij,ij->i", psi, psi)
+        T = psi / np.sqrt(rho)[:, None]
+        return np.linalg.eigvalsh(T @ T.T)
+
+    for _ in range(tries):
+        ev = lowden_min(fods)
+        if ev.min() > min_eig:
+            break
+        # move the FOD with the largest weight in the softest eigenvector
+        psi = basis_values(sysm, fods) @ C.T
+        rho = np.einsum("ij,ij->i", psi, psi)
+        T = psi / np.sqrt(rho)[:, None]
+        w, V = np.linalg.eigh(T @ T.T)
+        k = int(np.argmax(np.abs(V[:, 0])))
+        fods[k] = sysm.rat[rng.integers(0, sysm.natoms)] + rng.normal(0, 0.6, 3)
+    return fods
 
 
 def small_synthetic(seed=5, natoms=3, nbasis=24, nmsh=6000, nfo=4, functional="GGA-PBE*GGA-PBE", nspn=1):

@@ -542,16 +542,16 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
   }
 }
 
+void init_call_setup() {
+  cudaFuncSetAttribute(k_call_setup, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(double) * (NANG * NMOM + NANG)));
+}
+
 void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, int nspn,
                        const double* coef, const int8_t* maxfmt, const double* cgp, const MeshDev& M,
                        const double* boys_tab, CallFO* cfo, double* mom, cudaStream_t st) {
   if (ncalls <= 0) return;
   const size_t smem = sizeof(double) * (NANG * NMOM + NANG);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_call_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
   dim3 grid(ncalls, nfo);
   k_call_setup<<<grid, SETUP_THREADS, smem, st>>>(calls, pairs, nfo, nspn, coef, maxfmt, cgp, M, boys_tab,
                                                    cfo, mom);

@@ -55,6 +55,14 @@ void launch_coulomb_eval(int ncalls, const CallInfo* calls, const PairGeo* pairs
                          const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* mom,
                          const MeshDev& M, const double* boys_tab, double* vh, int ldv, cudaStream_t st);
 
+// FP64 tensor-core form of the Coulomb evaluation (csrc/coulomb_mma.cu).
+void init_coulomb_mma();
+void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
+                        const double* coef, const int8_t* maxfmt, int8_t* pair_fmt, const CallFO* cfo,
+                        const double* mom, const MeshDev& M, const double* boys_tab, double* vh, int ldv,
+                        cudaStream_t st);
+void init_call_setup();
+
 void launch_work_counts(int ncalls, const CallInfo* calls, int nfo, int npts, const CallFO* cfo,
                         unsigned long long* cnt, cudaStream_t st);
 

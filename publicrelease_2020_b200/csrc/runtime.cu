@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -349,7 +350,8 @@ struct flosic_ctx {
   SpinCache spin[2];
   // scratch
   DevBuf<double> d_basis, d_fodpts, d_psig, d_tmat, d_u, d_coef, d_cgp, d_mom, d_part, d_sums, d_sic, d_tmp;
-  DevBuf<int8_t> d_maxfmt;
+  DevBuf<int8_t> d_maxfmt, d_pairfmt;
+  bool scalar_coulomb = false;   // FLOSIC_COULOMB=scalar selects the per-thread kernel (A/B checks)
   DevBuf<unsigned long long> d_cnt;
   unsigned long long work_near = 0, work_far = 0;
   DevBuf<CallFO> d_callfo;
@@ -722,8 +724,15 @@ void coulomb(flosic_ctx* c, int s) {
   c->launches++;
   CUDA_CHECK(cudaEventRecord(c->ev[3], st));
   S.vh.ensure((size_t)nf * P);
-  launch_coulomb_eval(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                      c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
+  if (c->scalar_coulomb) {
+    launch_coulomb_eval(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
+                        c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
+  } else {
+    c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
+    launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_pairfmt.p,
+                       c->d_callfo.p, c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
+    c->launches++;
+  }
   c->launches++;
   c->d_cnt.ensure(2);
   CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 2 * sizeof(unsigned long long), st));
@@ -972,6 +981,7 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     CUDA_CHECK(cudaSetDevice(device));
     auto* c = new flosic_ctx;
     c->device = device;
+    if (const char* e = std::getenv("FLOSIC_COULOMB")) c->scalar_coulomb = (std::string(e) == "scalar");
     CUDA_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
       delete c;
@@ -983,6 +993,8 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     std::vector<double> ang, w;
     lebedev19(ang, w);
     upload_constants(ang.data(), w.data());
+    init_call_setup();
+    init_coulomb_mma();
     std::vector<double> bt = boys_table();
     c->d_boys.upload(bt.data(), bt.size(), c->st);
     CUDA_CHECK(cudaStreamSynchronize(c->st));
@@ -1004,7 +1016,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_boys.release(); c->d_pairs.release(); c->d_calls.release(); c->d_psi.release(); c->d_psi_thr.release();
   c->d_basis.release(); c->d_fodpts.release(); c->d_psig.release(); c->d_tmat.release(); c->d_u.release();
   c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
-  c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release();
+  c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
   if (c->blas) cublasDestroy(c->blas);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;

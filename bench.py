@@ -47,6 +47,11 @@ def workload(name):
         return W.synthetic(natoms=40, nbasis=512, nmsh=20_000, nfo=128, seed=1), \
             dict(workload="synthetic C2 shape on a 2e4-point mesh (profiling case)", atoms=40, nbasis=512,
                  nmsh=20_000, nfo=128, functional="GGA-PBE*GGA-PBE", nspn=1)
+    if name == "c2prof":
+        return W.synthetic(natoms=10, nbasis=128, nmsh=250_000, nfo=64, box_ang=7.56, seed=1), \
+            dict(workload="C2 density of atoms and points in a 7.56 A box: 10 atoms, 128 functions, 2.5e5 points, "
+                          "64 FOs (profiling case)", atoms=10, nbasis=128, nmsh=250_000, nfo=64,
+                 functional="GGA-PBE*GGA-PBE", nspn=1)
     if name == "water":
         s = W.water(seed=0, nrad=40)
         return s, dict(workload="water LDA-PW91, 5+5 FODs", atoms=3, nbasis=s.nbasis, nmsh=s.nmsh, nfo=5,
@@ -280,7 +285,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "water", "small"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "water", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

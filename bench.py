@@ -29,8 +29,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "s per FLO-SIC SCF cycle (all FOs + FOD forces)"
-COULOMB_FLOPS_NEAR = 200.0   # per near (pair, point, FO): work model of the Gaussian-pair Poisson solver
-COULOMB_FLOPS_FAR = 98.0     # per far (call, point, FO): 2*49 multipole terms
+COULOMB_FLOPS_NEAR = 92.0    # per near (pair, point, FO): 46 polynomial coefficients x Boys-monomial terms
+COULOMB_FLOPS_FAR = 98.0     # per far (call, point, FO): 49 multipole moments x harmonics
+# (the Boys values, monomials and harmonics depend on geometry only and are
+# formed once per (pair or call, point); the per-FO work is the contraction)
 
 
 def workload(name):
@@ -44,9 +46,10 @@ def workload(name):
             dict(workload="synthetic C2 shape on a 2.5e5-point mesh", atoms=40, nbasis=512, nmsh=250_000, nfo=128,
                  functional="GGA-PBE*GGA-PBE", nspn=1)
     if name == "c2tiny":
-        return W.synthetic(natoms=40, nbasis=512, nmsh=20_000, nfo=128, seed=1), \
-            dict(workload="synthetic C2 shape on a 2e4-point mesh (profiling case)", atoms=40, nbasis=512,
-                 nmsh=20_000, nfo=128, functional="GGA-PBE*GGA-PBE", nspn=1)
+        return W.synthetic(natoms=40, nbasis=512, nmsh=37_888, nfo=128, seed=1), \
+            dict(workload="synthetic C2 shape on a 37888-point mesh: 296 tiles, two waves of 148 CTAs "
+                          "(profiling case)", atoms=40, nbasis=512, nmsh=37_888, nfo=128,
+                 functional="GGA-PBE*GGA-PBE", nspn=1)
     if name == "c2prof":
         return W.synthetic(natoms=10, nbasis=128, nmsh=250_000, nfo=64, box_ang=7.56, seed=1), \
             dict(workload="C2 density of atoms and points in a 7.56 A box: 10 atoms, 128 functions, 2.5e5 points, "
@@ -261,7 +264,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_ms / 1e3 / args.steps / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(st_acc["launches"]),
-        "roofline": {"bound": "tensor", "kernel": "k_coulomb_eval", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "tensor", "kernel": "k_coulomb_shared + k_coulomb_mma", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
                      "peak_kind": "FP64 cuBLAS DGEMM measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                      "work": f"{st_acc['near'] / args.steps:.4g} near (pair,point,FO) x {COULOMB_FLOPS_NEAR:.0f} + "

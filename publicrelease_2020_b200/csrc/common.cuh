@@ -15,6 +15,8 @@ constexpr int LM = 6;             // multipole order of poisson1.f:75
 constexpr int NMOM = 49;          // (LM+1)^2
 constexpr int NANG = 146;         // Lebedev degree-19 mesh used by ANGMSH(LMAX=18)
 constexpr int NCOEF = 46;         // potential polynomial coefficients per pair
+constexpr int COEF_LD = 52;       // coefficient row stride (zero padded; 52 = 4 mod 16 doubles)
+constexpr int MOM_LD = 52;        // normalised-moment row stride (zero padded)
 constexpr int TILE = 128;         // mesh points per spatial tile
 constexpr int BOYS_NT = 1601;     // Boys table rows (T = 0..16 step 0.01)
 constexpr int BOYS_NC = 10;       // columns: F2 F3 F4 F5 F4/2 F5/2 F6/2 F5/6 F6/6 F7/6
@@ -47,6 +49,21 @@ struct CallFO {
   double rcut2;       // RCUT^2, or +inf when every point is evaluated exactly (NPOT=1)
   int32_t npot;       // 1 or 2
   int32_t nfar;       // number of far points
+  uint64_t keep;      // multipole terms kept by the skip rule of poisson1.f:1252-1270
+  int32_t lmax;       // highest kept degree
+  int32_t pad;
+};
+
+// Near/far geometry of one call when it is the same for every FO (bitwise equal
+// CG, RCUT^2 and NPOT), as for a single-pair call with NSPN=1 (poisson1.f:503-520
+// then gives CG = the pair centre).
+struct CallShare {
+  double cg[3];
+  double rcut2;
+  int32_t npot;
+  int32_t kf;         // moment columns of the far segment: (lmax over FOs + 1)^2 rounded up to 4; 0 = none
+  int32_t shared;     // 1 when the geometry is FO independent
+  int32_t pad;
 };
 
 #define FLOSIC_HD __host__ __device__ __forceinline__

@@ -1,17 +1,33 @@
 // Coulomb potential of all FOs at all mesh points, FP64 tensor-core form.
 //
 // For one POISSON1 call (a batch of Gaussian pairs, poisson1.f:611-1098) the
-// near-field potential of FO k at point p is
-//     T[k][p] = sum_{pair q} sum_{t<46} COEF[q][k][t] * G[q][t][p],
+// potential of FO k at mesh point p is, at points inside RCUT of the call's
+// centre CG (near points),
+//     sum_{pair q} sum_{t<46} COEF[q][k][t] * G[q][t][p],
 //     G[q][t][p] = F_{m(t)}(delta_q |p-C_q|^2) * mono_t(p - C_q),
-// where COEF are the pair's potential-polynomial coefficients of FO k and G is
-// FO independent (Boys values times monomials).  A CTA owns 128 spatially
-// sorted mesh points and 64 FOs; for each call it builds G for two pairs at a
-// time in shared memory and contracts it with the coefficient tile on the FP64
-// tensor cores (mma.sync m8n8k4 .f64), then merges per (FO, point): near points
-// take T, far points (beyond RCUT of that FO's call, NPOT=2) take the L<=6
-// multipole expansion (poisson1.f:1224-1600).  Calls are walked in order, so
-// per-point sums are deterministic.
+// and at the other points (far points, NPOT=2) the L<=6 multipole expansion
+//     sum_{lm} MV[c][k][lm] * H[c][lm][p],  H = Y_lm(u) / r^(l+1),  u = (p-CG)/r
+// (poisson1.f:1224-1600), MV being the normalised moments.  COEF and MV depend
+// on the FO, G and H only on geometry.  Two kernels evaluate it:
+//
+//   k_coulomb_shared  calls whose CG, RCUT and NPOT are the same for every FO
+//                     (every single-pair call with NSPN=1: CG is the pair
+//                     centre).  Near/far is then a property of the point alone,
+//                     so G (near points) and H (far points) are built once per
+//                     (call, point) with the other points' columns zeroed, and
+//                     both are segments of ONE GEMM  V[k][p] += A[k][:] B[:][p]
+//                     over all such calls, on the FP64 tensor cores
+//                     (mma.sync m8n8k4 .f64).  A CTA owns 128 points and up to
+//                     128 FOs; segments are double buffered (A by cp.async, B by
+//                     the first four warps while the others multiply).
+//   k_coulomb_mma     the remaining calls, whose CG (charge weighted,
+//                     poisson1.f:503-520) differs per FO: near field as a GEMM
+//                     into a per-call accumulator merged per (FO, point), far
+//                     field per (FO, point).
+//
+// Both walk their calls in order, so every per-point sum is deterministic.
+// Both count the evaluations they perform: near (pair, point, FO) and far
+// (call, point, FO), the units of the reference's POISSON1 work.
 #include <cfloat>
 
 #include "device_math.cuh"
@@ -19,47 +35,10 @@
 
 namespace flosic {
 
-constexpr int MMA_PTS = TILE;               // 128 points per CTA
-constexpr int MMA_FOS = 64;                 // FOs per CTA
-constexpr int MMA_THREADS = 256;            // 8 warps: 2 (FO) x 4 (points), 32x32 warp tiles
-constexpr int KPP = 48;                     // coefficients per pair, padded to a multiple of 4
-constexpr int PAIRS_PER_STEP = 2;
-constexpr int KSTEP = KPP * PAIRS_PER_STEP; // 96
-constexpr int A_LD = KSTEP + 4;             // 100: conflict-free A fragment loads
-constexpr int G_LD = MMA_PTS + 4;           // 132 (= 4 mod 16 doubles): conflict-free B fragment loads
-
-__constant__ double c_vfac[NMOM];           // harmonics.f prefactors sqrt(NRUN (2l+1)/4pi (l-m)!/(l+m)!)
-__constant__ int8_t c_slot_m[NCOEF];        // u^2 power of coefficient slot t (Boys index)
-__constant__ int8_t c_slot_mono[NCOEF];     // monomial of slot t (POLY order)
-
-void upload_mma_constants() {
-  double vfac[NMOM];
-  const double onofpi = 1.0 / (16 * atan(1.0));
-  for (int l = 0; l <= LM; ++l) {
-    double facfc = (2 * l + 1) * onofpi;
-    int now = l * l;
-    for (int m = 0; m <= l; ++m) {
-      const int nrun = (m == 0) ? 1 : 2;
-      const double v = sqrt(nrun * facfc);
-      for (int r = 0; r < nrun; ++r) vfac[now++] = v;
-      facfc = facfc / ((l - m > 1 ? l - m : 1) * (l + m + 1));
-    }
-  }
-  int8_t sm[NCOEF], sn[NCOEF];
-  // COEFICIENT order of poisson1.f:402-482
-  sm[0] = 0; sn[0] = 0;
-  sm[1] = 1; sn[1] = 0;
-  sm[2] = 2; sn[2] = 0;
-  for (int i = 0; i < 3; ++i) { sm[3 + i] = 1; sn[3 + i] = (int8_t)(1 + i); }
-  for (int i = 0; i < 3; ++i) { sm[6 + i] = 2; sn[6 + i] = (int8_t)(1 + i); }
-  for (int i = 0; i < 6; ++i) { sm[9 + i] = 2; sn[9 + i] = (int8_t)(4 + i); }
-  for (int i = 0; i < 6; ++i) { sm[15 + i] = 3; sn[15 + i] = (int8_t)(4 + i); }
-  for (int i = 0; i < 10; ++i) { sm[21 + i] = 3; sn[21 + i] = (int8_t)(10 + i); }
-  for (int i = 0; i < 15; ++i) { sm[31 + i] = 4; sn[31 + i] = (int8_t)(20 + i); }
-  cudaMemcpyToSymbol(c_vfac, vfac, sizeof(vfac));
-  cudaMemcpyToSymbol(c_slot_m, sm, sizeof(sm));
-  cudaMemcpyToSymbol(c_slot_mono, sn, sizeof(sn));
-}
+constexpr int MMA_THREADS = 256;            // 8 warps
+constexpr int G_LD = TILE + 4;              // 132 (= 4 mod 16 doubles): conflict-free B fragment loads
+constexpr int KSEG = 52;                    // rows of one B segment (46 coefficients or 49 moments, padded)
+static_assert(COEF_LD == KSEG && MOM_LD == KSEG, "segment rows and global row strides must agree");
 
 __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -67,63 +46,151 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                : "d"(a), "d"(b));
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 __device__ __forceinline__ double sqdist_rn2(double x, double y, double z, double cx, double cy, double cz) {
   const double dx = __dadd_rn(x, -cx), dy = __dadd_rn(y, -cy), dz = __dadd_rn(z, -cz);
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-// L<=6 multipole potential at unit direction (ux,uy,uz), 1/r = hn, with the
-// unnormalised recursion of harmonics.f evaluated level by level.
-__device__ __forceinline__ double multipole(const double* __restrict__ mo, int lmx, unsigned long long keep,
-                                            double ux, double uy, double uz, double hn) {
-  double p2[13], p1[13], cu[13];
-  double pot = 0.0, rec = hn;
-  // l = 0
-  if (keep & 1ull) pot += mo[0] * (c_vfac[0] * 1.0) * rec;
-  if (lmx == 0) return pot;
-  rec *= hn;
-  p2[0] = 1.0;
-  p1[0] = uz;
-  p1[1] = ux;
-  p1[2] = uy;
-  for (int j = 0; j < 3; ++j)
-    if (keep & (1ull << (1 + j))) pot += mo[1 + j] * (c_vfac[1 + j] * p1[j]) * rec;
+// Tile classification against a sphere: 0 every point inside, 1 every point
+// outside, 2 decided per point.  The 1e-9 margins leave boundary cases to the
+// exact per-point test.
+__device__ __forceinline__ int tile_class(const double lo[3], const double hi[3], double cx, double cy, double cz,
+                                          double rc2) {
+  const double cgv[3] = {cx, cy, cz};
+  double dmin2 = 0.0, dmax2 = 0.0;
 #pragma unroll
-  for (int l = 2; l <= LM; ++l) {
-    if (l > lmx) break;
-    rec *= hn;
-    const int n = 2 * l + 1;
-    const double ifc = (double)(2 * l - 1);
+  for (int d = 0; d < 3; ++d) {
+    const double a = lo[d] - cgv[d], b = cgv[d] - hi[d];
+    const double m = fmax(fmax(a, b), 0.0);
+    dmin2 += m * m;
+    const double e = fmax(fabs(cgv[d] - lo[d]), fabs(hi[d] - cgv[d]));
+    dmax2 += e * e;
+  }
+  if (dmin2 > rc2 * (1.0 + 1e-9)) return 1;
+  if (dmax2 < rc2 * (1.0 - 1e-9)) return 0;
+  return 2;
+}
+
+// Unnormalised harmonics of harmonics.f times 1/r^(l+1), in the row order of
+// the moments (l*l + j; j = 0 for m = 0, 2m-1 and 2m for the two m > 0
+// partners), for l <= lmx.  The recursion of harmonics.f runs level by level;
+// here it runs m-major so that only a few values are live, but every value is
+// formed by the same operations on the same operands:
+//   m = l (sectoral):  C_l = (2l-1)(C_{l-1} ux - S_{l-1} uy),  S_l = (2l-1)(S_{l-1} ux + C_{l-1} uy)
+//   m < l:             P_l = ((2l-1)/(l-m)) P_{l-1} uz - ((l+m-1)/(l-m)) P_{l-2}
+// op(row, value) receives each term.
+template <typename Op>
+__device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz, double hn, int lmx, Op op) {
+  double rec[LM + 1];
+  rec[0] = hn;
 #pragma unroll
-    for (int j = 0; j < 2 * l - 1; ++j) {
-      const int m = (j + 1) / 2;
+  for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
+  // m = 0
+  {
+    op(0, 1.0 * rec[0]);
+    if (lmx >= 1) op(1, uz * rec[1]);
+    double p2 = 1.0, p1 = uz;
+#pragma unroll
+    for (int l = 2; l <= LM; ++l) {
+      if (l > lmx) break;
+      const double facrc = 1.0 / l;
+      const double aa = facrc * (2 * l - 1), bb = facrc * (l - 1);
+      const double cu = aa * p1 * uz - bb * p2;
+      op(l * l, cu * rec[l]);
+      p2 = p1;
+      p1 = cu;
+    }
+  }
+  double sc = ux, ss = uy;  // sectoral pair at l = m
+#pragma unroll
+  for (int m = 1; m <= LM; ++m) {
+    if (m > lmx) break;
+    if (m > 1) {
+      const double ifc = (double)(2 * m - 1);
+      const double nc = ifc * (sc * ux - ss * uy);
+      const double ns = ifc * (ss * ux + sc * uy);
+      sc = nc;
+      ss = ns;
+    }
+    op(m * m + 2 * m - 1, sc * rec[m]);
+    op(m * m + 2 * m, ss * rec[m]);
+    double c2 = 0.0, s2 = 0.0, c1 = sc, s1 = ss;
+#pragma unroll
+    for (int l = m + 1; l <= LM; ++l) {
+      if (l > lmx) break;
       const double facrc = 1.0 / (l - m);
       const double aa = facrc * (2 * l - 1);
       const double bb = (m == l - 1) ? 0.0 : facrc * (l + m - 1);
-      const double prev2 = (j < 2 * l - 3) ? p2[j] : 0.0;
-      cu[j] = aa * p1[j] * uz - bb * prev2;
-    }
-    cu[2 * l - 1] = ifc * (p1[2 * l - 3] * ux - p1[2 * l - 2] * uy);
-    cu[2 * l] = ifc * (p1[2 * l - 2] * ux + p1[2 * l - 3] * uy);
-    const int base = l * l;
-#pragma unroll
-    for (int j = 0; j < n; ++j)
-      if (keep & (1ull << (base + j))) pot += mo[base + j] * (c_vfac[base + j] * cu[j]) * rec;
-#pragma unroll
-    for (int j = 0; j < 13; ++j) {
-      p2[j] = p1[j];
-      p1[j] = (j < n) ? cu[j] : 0.0;
+      const double cc = aa * c1 * uz - bb * c2;
+      const double cs = aa * s1 * uz - bb * s2;
+      op(l * l + 2 * m - 1, cc * rec[l]);
+      op(l * l + 2 * m, cs * rec[l]);
+      c2 = c1;
+      s2 = s1;
+      c1 = cc;
+      s1 = cs;
     }
   }
-  return pot;
 }
 
-// G column of one (pair, point) in the COEFICIENT slot order (poisson1.f:402-482):
-// slot t holds F_{m(t)} * POLY(mono(t)); monomials are formed in the order of
-// poisson1.f:925-959 and stored as soon as they are complete.
-__device__ __forceinline__ void write_g(double* g, double x, double y, double z, double F0, double F1, double F2,
-                                        double F3, double F4) {
+// Boys values F_0..F_{fmt-1} of the FFFMTC3/4/5 variant (same arithmetic as
+// boys_all); absent orders are zero.
+__device__ __forceinline__ void boys_fmt(const double* __restrict__ tab, double x, double chgd, int fmt,
+                                         double F[5]) {
+  if (x > 16.0) {
+    const double ROOTPI = 1.77245385090551602728;
+    const double pol1 = -chgd;
+    const double rt = __dmul_rn(sqrt(x), ROOTPI);
+    const double rect1 = 0.5 / x;
+    F[0] = rect1 * (rt + pol1);
+    F[1] = rect1 * (F[0] + pol1);
+    F[2] = rect1 * (3 * F[1] + pol1);
+    F[3] = (fmt >= 4) ? rect1 * (5 * F[2] + pol1) : 0.0;
+    F[4] = (fmt >= 5) ? rect1 * (7 * F[3] + pol1) : 0.0;
+    return;
+  }
+  const int it = (int)(100 * x + 1.5);
+  const double pol1 = chgd;
+  const double rect1 = 2 * x;
+  const double dt = (1.0e-2) * (it - 1) - x;
+  const double* f = tab + (size_t)(it - 1) * BOYS_NC;
+  const double o7 = 1.0 / 7.0, o5 = 1.0 / 5.0, o3 = 1.0 / 3.0;
+  if (fmt == 5) {
+    F[4] = f[2] + dt * (f[3] + dt * (f[6] + dt * f[9]));
+    F[3] = (F[4] * rect1 + pol1) * o7;
+    F[2] = (F[3] * rect1 + pol1) * o5;
+  } else if (fmt == 4) {
+    F[4] = 0.0;
+    F[3] = f[1] + dt * (f[2] + dt * (f[5] + dt * f[8]));
+    F[2] = (F[3] * rect1 + pol1) * o5;
+  } else {
+    F[4] = 0.0;
+    F[3] = 0.0;
+    F[2] = f[0] + dt * (f[1] + dt * (f[4] + dt * f[7]));
+  }
+  F[1] = (F[2] * rect1 + pol1) * o3;
+  F[0] = (F[1] * rect1 + pol1);
+}
+
+// Rows of the near segment used by a pair whose largest Boys variant is fmt:
+// slots 15.. carry F_3 and slots 31.. carry F_4 (COEFICIENT order,
+// poisson1.f:402-482).
+__device__ __forceinline__ int near_rows(int fmt) { return fmt >= 5 ? 48 : (fmt == 4 ? 32 : 16); }
+
+// G column of one (pair, point) in the COEFICIENT slot order: slot t holds
+// F_{m(t)} * POLY(mono(t)), monomials in the order of poisson1.f:925-959.
+// Rows >= kn (16, 32 or 48) are not written.
+__device__ __forceinline__ void write_g(double* g, int kn, double x, double y, double z, const double F[5]) {
 #define GW(t, v) g[(size_t)(t) * G_LD] = (v)
+  const double F0 = F[0], F1 = F[1], F2 = F[2], F3 = F[3], F4 = F[4];
+  const double zz = z * z, yz = y * z, yy = y * y, xz = x * z, xy = x * y, xx = x * x;
   GW(0, F0);
   GW(1, F1);
   GW(2, F2);
@@ -133,7 +200,6 @@ __device__ __forceinline__ void write_g(double* g, double x, double y, double z,
   GW(6, F2 * z);
   GW(7, F2 * y);
   GW(8, F2 * x);
-  const double zz = z * z, yz = y * z, yy = y * y, xz = x * z, xy = x * y, xx = x * x;
   GW(9, F2 * zz);
   GW(10, F2 * yz);
   GW(11, F2 * yy);
@@ -141,6 +207,7 @@ __device__ __forceinline__ void write_g(double* g, double x, double y, double z,
   GW(13, F2 * xy);
   GW(14, F2 * xx);
   GW(15, F3 * zz);
+  if (kn <= 16) return;
   GW(16, F3 * yz);
   GW(17, F3 * yy);
   GW(18, F3 * xz);
@@ -157,6 +224,7 @@ __device__ __forceinline__ void write_g(double* g, double x, double y, double z,
   GW(29, F3 * (y * xx));
   GW(30, F3 * (x * xx));
   GW(31, F4 * (zz * zz));
+  if (kn <= 32) return;
   GW(32, F4 * (zz * yz));
   GW(33, F4 * (yy * zz));
   GW(34, F4 * (yy * yz));
@@ -176,25 +244,284 @@ __device__ __forceinline__ void write_g(double* g, double x, double y, double z,
 #undef GW
 }
 
+__device__ __forceinline__ void zero_rows(double* g, int k) {
+  for (int t = 0; t < k; ++t) g[(size_t)t * G_LD] = 0.0;
+}
+
+__device__ __forceinline__ void count_add(unsigned long long* cnt, unsigned long long near, unsigned long long far) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    near += __shfl_down_sync(0xffffffffu, near, o);
+    far += __shfl_down_sync(0xffffffffu, far, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (near) atomicAdd(&cnt[0], near);
+    if (far) atomicAdd(&cnt[1], far);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-geometry calls
+// ---------------------------------------------------------------------------
+template <int WM>
+struct SharedSmem {
+  double A[2][32 * WM * KSEG];  // FO rows of the segment's coefficients / moments
+  double B[2][KSEG * G_LD];     // G or H columns
+  double px[TILE], py[TILE], pz[TILE];
+};
+
+// One segment of the shared GEMM: the near part of one pair or the far part of
+// one call, restricted to this tile.
+struct Segment {
+  int far;       // 0 near (pair q), 1 far (call c)
+  int idx;       // q or c
+  int rows;      // contraction length, a multiple of 4
+  int cls;       // tile class against the call's sphere
+  double cx, cy, cz, rc2;
+};
+
+// Walks the shared calls of the list in order and yields their segments for a
+// tile: near segments for each pair unless the tile is entirely far, then the
+// far segment unless the tile is entirely near or NPOT=1.  Every thread runs
+// it identically.
+struct SegmentWalker {
+  const int* list;
+  int n;
+  const CallShare* share;
+  const CallInfo* calls;
+  const int8_t* pair_fmt;
+  double lo[3], hi[3];
+  int li, sub;
+  int c, p0, np, cls, kf, npot;
+  double cx, cy, cz, rc2;
+  unsigned long long direct_far;  // far points of all-far tiles of calls without kept moments
+
+  __device__ bool next(Segment& s, int npts) {
+    while (li < n) {
+      if (sub < 0) {
+        c = list[li];
+        const CallShare sh = share[c];
+        const CallInfo ci = calls[c];
+        cx = sh.cg[0];
+        cy = sh.cg[1];
+        cz = sh.cg[2];
+        rc2 = sh.rcut2;
+        kf = sh.kf;
+        npot = sh.npot;
+        p0 = ci.p0;
+        np = ci.np;
+        cls = (npot == 1) ? 0 : tile_class(lo, hi, cx, cy, cz, rc2);
+        sub = (cls == 1) ? np : 0;
+      }
+      if (sub < np) {
+        const int q = p0 + sub;
+        ++sub;
+        s = Segment{0, q, near_rows(pair_fmt[q]), cls, cx, cy, cz, rc2};
+        return true;
+      }
+      const bool want_far = npot == 2 && cls != 0;
+      sub = -1;
+      ++li;
+      if (want_far) {
+        if (kf > 0 || cls == 2) {
+          s = Segment{1, c, kf, cls, cx, cy, cz, rc2};
+          return true;
+        }
+        direct_far += (unsigned long long)npts;
+      }
+    }
+    return false;
+  }
+};
+
+template <int WM>
+__global__ void __launch_bounds__(MMA_THREADS, 1)
+k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __restrict__ share,
+                 const CallInfo* __restrict__ calls, int nfo, const double* __restrict__ coef,
+                 const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
+                 const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
+                 double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
+  constexpr int FOB = 32 * WM, WN = 8 / WM, WPTS = TILE / WN, NT = WPTS / 8;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  SharedSmem<WM>& S = *reinterpret_cast<SharedSmem<WM>*>(smraw);
+  const int tile = blockIdx.x;
+  const int k0 = blockIdx.y * FOB;
+  const int nk = min(FOB, nfo - k0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp % WM, wn = warp / WM;
+  const int p0 = tile * TILE;
+  const int np = min(TILE, M.n - p0);
+  for (int i = tid; i < TILE; i += MMA_THREADS) {
+    const bool a = i < np;
+    S.px[i] = a ? M.x[p0 + i] : 0.0;
+    S.py[i] = a ? M.y[p0 + i] : 0.0;
+    S.pz[i] = a ? M.z[p0 + i] : 0.0;
+  }
+  SegmentWalker W;
+  W.list = lists;
+  W.n = lists[2 * ncalls];
+  W.share = share;
+  W.calls = calls;
+  W.pair_fmt = pair_fmt;
+  for (int d = 0; d < 3; ++d) {
+    W.lo[d] = M.tile_lo[3 * tile + d];
+    W.hi[d] = M.tile_hi[3 * tile + d];
+  }
+  W.li = 0;
+  W.sub = -1;
+  W.c = W.p0 = W.np = W.cls = W.kf = 0;
+  W.npot = 1;
+  W.cx = W.cy = W.cz = W.rc2 = 0.0;
+  W.direct_far = 0ull;
+  __syncthreads();
+
+  double V[4][NT][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < NT; ++b) V[a][b][0] = V[a][b][1] = 0.0;
+  unsigned long long my_near = 0, my_far = 0;
+
+  // Stage segment s into buffer b: A rows by cp.async (all threads), B columns
+  // by threads 0..127 (one point each).
+  auto stage = [&](const Segment& s, int b) {
+    if (s.rows > 0) {
+      const double* src = s.far ? momv + ((size_t)s.idx * nfo + k0) * MOM_LD
+                                : coef + ((size_t)s.idx * nfo + k0) * COEF_LD;
+      const int nchunk = nk * (KSEG / 2);
+      double* dst = S.A[b];
+      for (int i = tid; i < nchunk; i += MMA_THREADS) cp_async16(dst + 2 * i, src + 2 * i);
+    }
+    cp_async_commit();
+    if (tid < TILE) {
+      const int p = tid;
+      double* g = &S.B[b][p];
+      const double x = S.px[p], y = S.py[p], z = S.pz[p];
+      if (!s.far) {
+        bool nr = p < np;
+        if (nr && s.cls == 2) nr = !(sqdist_rn2(x, y, z, s.cx, s.cy, s.cz) > s.rc2);
+        if (nr) {
+          ++my_near;
+          const PairGeo& pg = pairs[s.idx];
+          const double rx = x - pg.C[0], ry = y - pg.C[1], rz = z - pg.C[2];
+          const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
+          double F[5];
+          boys_fmt(boys_tab, xx, exp(-xx), s.rows >= 48 ? 5 : (s.rows == 32 ? 4 : 3), F);
+          write_g(g, s.rows, rx, ry, rz, F);
+        } else {
+          zero_rows(g, s.rows);
+        }
+      } else {
+        double r2 = 0.0;
+        bool fr = p < np;
+        if (fr) {
+          r2 = sqdist_rn2(x, y, z, s.cx, s.cy, s.cz);
+          if (s.cls == 2) fr = r2 > s.rc2;
+        }
+        if (fr) {
+          ++my_far;
+          if (s.rows > 0) {
+            const double hn = 1.0 / sqrt(r2);
+            const int kr = s.rows;
+            harmonics_mmajor(hn * (x - s.cx), hn * (y - s.cy), hn * (z - s.cz), hn, LM, [&](int row, double v) {
+              if (row < kr) g[(size_t)row * G_LD] = v;
+            });
+            for (int t = NMOM; t < kr; ++t) g[(size_t)t * G_LD] = 0.0;
+          }
+        } else {
+          zero_rows(g, s.rows);
+        }
+      }
+    }
+  };
+
+  Segment cur, nxt;
+  bool have = W.next(cur, np);
+  if (have) stage(cur, 0);
+  cp_async_wait_all();
+  __syncthreads();
+  int buf = 0;
+  while (have) {
+    const bool more = W.next(nxt, np);
+    if (more) stage(nxt, buf ^ 1);
+    if (wm * 32 < nk && cur.rows > 0) {
+      const double* As = &S.A[buf][(wm * 32 + (lane >> 2)) * KSEG + (lane & 3)];
+      const double* Bs = &S.B[buf][(lane & 3) * G_LD + wn * WPTS + (lane >> 2)];
+      for (int kk = 0; kk < cur.rows; kk += 4) {
+        double af[4], bf[NT];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) af[mt] = As[mt * 8 * KSEG + kk];
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(size_t)kk * G_LD + nt * 8];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) dmma884(V[mt][nt][0], V[mt][nt][1], af[mt], bf[nt]);
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    have = more;
+    cur = nxt;
+    buf ^= 1;
+  }
+
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int k = wm * 32 + mt * 8 + (lane >> 2);
+    if (k >= nk) continue;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int p = wn * WPTS + nt * 8 + 2 * (lane & 3) + i;
+        if (p < np) vh[(size_t)(k0 + k) * ldv + p0 + p] = V[mt][nt][i];
+      }
+  }
+  if (tid == 0) my_far += W.direct_far;
+  count_add(cnt, my_near * (unsigned long long)nk, my_far * (unsigned long long)nk);
+}
+
+// ---------------------------------------------------------------------------
+// Per-FO-geometry calls
+// ---------------------------------------------------------------------------
+constexpr int MMA_PTS = TILE;               // 128 points per CTA
+constexpr int MMA_FOS = 64;                 // FOs per CTA
+constexpr int KPP = 48;                     // coefficients per pair, padded to a multiple of 4
+constexpr int PAIRS_PER_STEP = 2;
+constexpr int KSTEP = KPP * PAIRS_PER_STEP; // 96
+constexpr int A_LD = KSTEP + 4;             // 100: conflict-free A fragment loads
+
 struct MmaSmem {
   double A[MMA_FOS * A_LD];
   double G[KSTEP * G_LD];
   double px[MMA_PTS], py[MMA_PTS], pz[MMA_PTS];
   double cg[MMA_FOS][3];
   double rc2[MMA_FOS];
-  unsigned long long keep[MMA_FOS];
   int stat[MMA_FOS];
   int npot[MMA_FOS];
   int lmax[MMA_FOS];
   int anynear, anyfar;
 };
 
+// Far-field potential of one FO at one point: sum_lm MV[lm] H_lm.
+__device__ __forceinline__ double multipole(const double* __restrict__ mv, int lmx, double ux, double uy, double uz,
+                                            double hn) {
+  double pot = 0.0;
+  harmonics_mmajor(ux, uy, uz, hn, lmx, [&](int row, double v) { pot += mv[row] * v; });
+  return pot;
+}
+
 __global__ void __launch_bounds__(MMA_THREADS, 1)
-k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __restrict__ pairs, int nfo,
-              const double* __restrict__ coef, const int8_t* __restrict__ pair_fmt,
-              const CallFO* __restrict__ cfo, const double* __restrict__ mom, MeshDev M,
-              const double* __restrict__ boys_tab, double* __restrict__ vh, int ldv) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+k_coulomb_mma(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
+              const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
+              const int8_t* __restrict__ pair_fmt, const CallFO* __restrict__ cfo, const double* __restrict__ momv,
+              MeshDev M, const double* __restrict__ boys_tab, double* __restrict__ vh, int ldv,
+              unsigned long long* __restrict__ cnt) {
+  const int* list = lists + ncalls;
+  const int nl = lists[2 * ncalls + 1];
+  if (accumulate && nl == 0) return;
+  extern __shared__ __align__(128) unsigned char smraw[];
   MmaSmem& S = *reinterpret_cast<MmaSmem*>(smraw);
   const int tile = blockIdx.x;
   const int k0 = blockIdx.y * MMA_FOS;
@@ -217,8 +544,10 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) V[a][b][0] = V[a][b][1] = 0.0;
+  unsigned long long my_near = 0, my_far = 0;
 
-  for (int c = 0; c < ncalls; ++c) {
+  for (int li = 0; li < nl; ++li) {
+    const int c = list[li];
     __syncthreads();
     if (tid == 0) {
       S.anynear = 0;
@@ -227,7 +556,6 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
     __syncthreads();
     if (tid < MMA_FOS) {
       int st = 1, npot = 2, lmx = 0;
-      unsigned long long keep = 0ull;
       double cgx = 0, cgy = 0, cgz = 0, rc2 = 0;
       if (tid < nk) {
         const CallFO f = cfo[(size_t)c * nfo + k0 + tid];
@@ -236,37 +564,11 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
         cgz = f.cg[2];
         rc2 = f.rcut2;
         npot = f.npot;
-        double dmin2 = 0.0, dmax2 = 0.0;
-        const double cgv[3] = {cgx, cgy, cgz};
-        for (int d = 0; d < 3; ++d) {
-          const double a = lo[d] - cgv[d], b = cgv[d] - hi[d];
-          const double m = fmax(fmax(a, b), 0.0);
-          dmin2 += m * m;
-          const double e = fmax(fabs(cgv[d] - lo[d]), fabs(hi[d] - cgv[d]));
-          dmax2 += e * e;
-        }
-        if (npot == 1) st = 0;
-        else if (dmin2 > rc2 * (1.0 + 1e-9)) st = 1;
-        else if (dmax2 < rc2 * (1.0 - 1e-9)) st = 0;
-        else st = 2;
+        st = (npot == 1) ? 0 : tile_class(lo, hi, cgx, cgy, cgz, rc2);
         if (st != 1) atomicOr(&S.anynear, 1);
-        if (st != 0) {
+        if (st != 0 && npot == 2) {
           atomicOr(&S.anyfar, 1);
-          // skip rule of poisson1.f:1252-1270; RI1 bounded by the tile box and RCUT
-          const double* mo = mom + ((size_t)c * nfo + k0 + tid) * NMOM;
-          const double ri1 = 1.0 / fmax(sqrt(dmin2), f.rcut);
-          double rt = ri1;
-          int m = 0;
-          for (int l = 0; l <= LM; ++l) {
-            for (int j = -l; j <= l; ++j, ++m) {
-              const double tst = fabs((2 * l + 1) * mo[m] * rt);
-              if (!(tst < 1.0e-12)) {
-                keep |= (1ull << m);
-                lmx = l;
-              }
-            }
-            rt *= ri1;
-          }
+          lmx = f.lmax;
         }
       }
       S.stat[tid] = st;
@@ -275,7 +577,6 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
       S.cg[tid][1] = cgy;
       S.cg[tid][2] = cgz;
       S.rc2[tid] = rc2;
-      S.keep[tid] = keep;
       S.lmax[tid] = lmx;
     }
     __syncthreads();
@@ -297,22 +598,11 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
             const PairGeo& pg = pairs[q];
             const double rx = S.px[p] - pg.C[0], ry = S.py[p] - pg.C[1], rz = S.pz[p] - pg.C[2];
             const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
-            const double chgd = exp(-xx);
-            double s3[3], s4[4], s5[5];
-            boys_all(boys_tab, xx, chgd, s3, s4, s5);
-            const int fmt = pair_fmt[q];
-            double F0, F1, F2, F3, F4;
-            if (fmt == 5) {
-              F0 = s5[0]; F1 = s5[1]; F2 = s5[2]; F3 = s5[3]; F4 = s5[4];
-            } else if (fmt == 4) {
-              F0 = s4[0]; F1 = s4[1]; F2 = s4[2]; F3 = s4[3]; F4 = 0.0;
-            } else {
-              F0 = s3[0]; F1 = s3[1]; F2 = s3[2]; F3 = 0.0; F4 = 0.0;
-            }
-            write_g(g, rx, ry, rz, F0, F1, F2, F3, F4);
+            double F[5];
+            boys_fmt(boys_tab, xx, exp(-xx), pair_fmt[q], F);
+            write_g(g, KPP, rx, ry, rz, F);
           } else {
-#pragma unroll
-            for (int t = 0; t < KPP; ++t) g[(size_t)t * G_LD] = 0.0;
+            zero_rows(g, KPP);
           }
         }
         // coefficient tile A[k][ql*48 + t]
@@ -320,7 +610,7 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
           const int k = e / KSTEP, col = e - k * KSTEP;
           const int ql = col / KPP, t = col - ql * KPP;
           double v = 0.0;
-          if (k < nk && ql < npc && t < NCOEF) v = coef[((size_t)(ci.p0 + q0 + ql) * nfo + k0 + k) * NCOEF + t];
+          if (k < nk && ql < npc) v = coef[((size_t)(ci.p0 + q0 + ql) * nfo + k0 + k) * COEF_LD + t];
           S.A[k * A_LD + col] = v;
         }
         __syncthreads();
@@ -353,7 +643,10 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
             bool nr = (st == 0);
             if (st == 2)
               nr = !(sqdist_rn2(S.px[p], S.py[p], S.pz[p], S.cg[k][0], S.cg[k][1], S.cg[k][2]) > S.rc2[k]);
-            if (nr) V[mt][nt][i] += T[mt][nt][i];
+            if (nr) {
+              V[mt][nt][i] += T[mt][nt][i];
+              if (p < np) my_near += (unsigned long long)ci.np;
+            }
           }
       }
     }
@@ -366,8 +659,7 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
         if (st == 0 || S.npot[k] == 1) continue;
         const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
         const int lmx = S.lmax[k];
-        const unsigned long long keep = S.keep[k];
-        const double* mo = mom + ((size_t)c * nfo + k0 + k) * NMOM;
+        const double* mv = momv + ((size_t)c * nfo + k0 + k) * MOM_LD;
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
@@ -376,9 +668,9 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
             if (p >= np) continue;
             const double r2 = sqdist_rn2(S.px[p], S.py[p], S.pz[p], cx, cy, cz);
             if (!(r2 > rc2)) continue;
+            ++my_far;
             const double hn = 1.0 / sqrt(r2);
-            V[mt][nt][i] += multipole(mo, lmx, keep, hn * (S.px[p] - cx), hn * (S.py[p] - cy), hn * (S.pz[p] - cz),
-                                      hn);
+            V[mt][nt][i] += multipole(mv, lmx, hn * (S.px[p] - cx), hn * (S.py[p] - cy), hn * (S.pz[p] - cz), hn);
           }
       }
     }
@@ -392,11 +684,17 @@ k_coulomb_mma(int ncalls, const CallInfo* __restrict__ calls, const PairGeo* __r
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int p = wn * 32 + nt * 8 + 2 * (lane & 3) + i;
-        if (p < np) vh[(size_t)(k0 + k) * ldv + p0 + p] = V[mt][nt][i];
+        if (p >= np) continue;
+        double* o = &vh[(size_t)(k0 + k) * ldv + p0 + p];
+        *o = accumulate ? *o + V[mt][nt][i] : V[mt][nt][i];
       }
   }
+  count_add(cnt, my_near, my_far);
 }
 
+// ---------------------------------------------------------------------------
+// Call classification
+// ---------------------------------------------------------------------------
 // Largest Boys variant over the FOs of each pair (the G tile is shared by all FOs).
 __global__ void k_pair_fmt(int npairs, int nfo, const int8_t* __restrict__ maxfmt, int8_t* __restrict__ out) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -406,21 +704,124 @@ __global__ void k_pair_fmt(int npairs, int nfo, const int8_t* __restrict__ maxfm
   out[q] = (int8_t)m;
 }
 
-// Per-device set-up: constant tables and the dynamic shared-memory opt-in.
+// One warp per call: is (CG, RCUT^2, NPOT) bitwise the same for every FO, and
+// how many moment rows do the FOs keep.
+__global__ void k_call_share(int ncalls, int nfo, const CallFO* __restrict__ cfo, CallShare* __restrict__ out) {
+  const int c = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= ncalls) return;
+  const CallFO f0 = cfo[(size_t)c * nfo];
+  bool same = true;
+  int lmx = -1;
+  for (int k = lane; k < nfo; k += 32) {
+    const CallFO f = cfo[(size_t)c * nfo + k];
+    same = same && f.cg[0] == f0.cg[0] && f.cg[1] == f0.cg[1] && f.cg[2] == f0.cg[2] && f.rcut2 == f0.rcut2 &&
+           f.npot == f0.npot;
+    if (f.npot == 2 && f.keep != 0ull) lmx = max(lmx, f.lmax);
+  }
+  same = __all_sync(0xffffffffu, same);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lmx = max(lmx, __shfl_xor_sync(0xffffffffu, lmx, o));
+  if (lane == 0) {
+    CallShare s;
+    s.cg[0] = f0.cg[0];
+    s.cg[1] = f0.cg[1];
+    s.cg[2] = f0.cg[2];
+    s.rcut2 = f0.rcut2;
+    s.npot = f0.npot;
+    s.kf = (lmx < 0) ? 0 : (((lmx + 1) * (lmx + 1) + 3) / 4) * 4;
+    s.shared = same ? 1 : 0;
+    s.pad = 0;
+    out[c] = s;
+  }
+}
+
+// Stable partition of the calls into lists[0..ns) (shared geometry) and
+// lists[ncalls..ncalls+nf) (per-FO geometry); lists[2 ncalls] = ns,
+// lists[2 ncalls + 1] = nf.  One block.
+constexpr int LIST_THREADS = 1024;
+__global__ void __launch_bounds__(LIST_THREADS) k_call_lists(int ncalls, int per_fo_only,
+                                                             const CallShare* __restrict__ share,
+                                                             int* __restrict__ lists) {
+  __shared__ int wsum[LIST_THREADS / 32];
+  __shared__ int base;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < ncalls; c0 += LIST_THREADS) {
+    const int c = c0 + tid;
+    const bool valid = c < ncalls;
+    const bool sh = valid && !per_fo_only && share[c].shared;
+    const unsigned bal = __ballot_sync(0xffffffffu, sh);
+    if (lane == 0) wsum[wid] = __popc(bal);
+    __syncthreads();
+    int before = base;
+    for (int w = 0; w < wid; ++w) before += wsum[w];
+    const int rank_s = before + __popc(bal & ((1u << lane) - 1u));
+    if (valid) {
+      if (sh) lists[rank_s] = c;
+      else lists[ncalls + (c - rank_s)] = c;  // c minus the shared calls before it
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < LIST_THREADS / 32; ++w) t += wsum[w];
+      base += t;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    lists[2 * ncalls] = base;
+    lists[2 * ncalls + 1] = ncalls - base;
+  }
+}
+
+template <int WM>
+static void set_shared_attr() {
+  cudaFuncSetAttribute(k_coulomb_shared<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(SharedSmem<WM>));
+}
+
+// Per-device set-up: the dynamic shared-memory opt-ins.
 void init_coulomb_mma() {
-  upload_mma_constants();
   cudaFuncSetAttribute(k_coulomb_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MmaSmem));
+  set_shared_attr<1>();
+  set_shared_attr<2>();
+  set_shared_attr<4>();
+}
+
+template <int WM>
+static void launch_shared(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
+                          const double* coef, const int8_t* pair_fmt, const PairGeo* pairs, const double* momv,
+                          const MeshDev& M, const double* boys_tab, double* vh, int ldv, unsigned long long* cnt,
+                          cudaStream_t st) {
+  dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
+  k_coulomb_shared<WM><<<grid, MMA_THREADS, sizeof(SharedSmem<WM>), st>>>(
+      ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M, boys_tab, vh, ldv, cnt);
 }
 
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
-                        const double* coef, const int8_t* maxfmt, int8_t* pair_fmt, const CallFO* cfo,
-                        const double* mom, const MeshDev& M, const double* boys_tab, double* vh, int ldv,
-                        cudaStream_t st) {
-  const size_t smem = sizeof(MmaSmem);
-  if (npairs > 0) k_pair_fmt<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, nfo, maxfmt, pair_fmt);
+                        const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
+                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,
+                        const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st) {
+  if (npairs > 0) k_pair_fmt<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, nfo, maxfmt, scr.pair_fmt);
+  if (ncalls > 0) k_call_share<<<(ncalls + 7) / 8, 256, 0, st>>>(ncalls, nfo, cfo, scr.share);
+  k_call_lists<<<1, LIST_THREADS, 0, st>>>(ncalls, per_fo_only ? 1 : 0, scr.share, scr.lists);
+  if (!per_fo_only) {
+    if (nfo > 64)
+      launch_shared<4>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
+                       ldv, cnt, st);
+    else if (nfo > 32)
+      launch_shared<2>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
+                       ldv, cnt, st);
+    else
+      launch_shared<1>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
+                       ldv, cnt, st);
+  }
   dim3 grid(M.ntiles, (nfo + MMA_FOS - 1) / MMA_FOS);
-  k_coulomb_mma<<<grid, MMA_THREADS, smem, st>>>(ncalls, calls, pairs, nfo, coef, pair_fmt, cfo, mom, M, boys_tab,
-                                                  vh, ldv);
+  k_coulomb_mma<<<grid, MMA_THREADS, sizeof(MmaSmem), st>>>(ncalls, scr.lists, per_fo_only ? 0 : 1, calls, pairs,
+                                                             nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh,
+                                                             ldv, cnt);
 }
 
 }  // namespace flosic

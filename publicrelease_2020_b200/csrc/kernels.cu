@@ -7,8 +7,6 @@
 //                    poisson1.f:259-501) and centre-of-gravity moments (ginted.F)
 //   k_call_setup     per POISSON1 call and FO: CG, RCUT, NPOT, sphere potential
 //                    and L<=6 multipole moments (poisson1.f:503-1230)
-//   k_coulomb_eval   near-field Boys-function potential and far-field multipole
-//                    potential at every mesh point (poisson1.f:611-1600)
 //   k_xc             XC potential of the FO density, SIC potential, energy
 //                    partial sums (getvlxc.F, subvlxc_libxc.F90, apotnl_sic.F)
 #include <cfloat>
@@ -365,9 +363,11 @@ __global__ void __launch_bounds__(128) k_pair_coef(const PairGeo* __restrict__ p
       if (s >= 31 && cf[s] != 0.0) s5 = true;
     }
     if (!s3) cf[2] = 0.0;
-    double* o = coef + ((size_t)ip * nfo + k) * NCOEF;
+    double* o = coef + ((size_t)ip * nfo + k) * COEF_LD;
 #pragma unroll
     for (int s = 0; s < NCOEF; ++s) o[s] = cf[s];
+#pragma unroll
+    for (int s = NCOEF; s < COEF_LD; ++s) o[s] = 0.0;
     maxfmt[(size_t)ip * nfo + k] = (int8_t)(s5 ? 5 : (s4 ? 4 : 3));
     double* oc = cgp + ((size_t)ip * nfo + k) * 4;
     for (int kq = 0; kq < 4; ++kq) oc[kq] = cg4[kq];
@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
                                                               const double* __restrict__ cgp, MeshDev M,
                                                               const double* __restrict__ boys_tab,
                                                               CallFO* __restrict__ out,
-                                                              double* __restrict__ mom) {
+                                                              double* __restrict__ momv) {
   extern __shared__ double sm[];  // [NANG][NMOM] products, then NANG potentials
   double* prod = sm;
   double* vang = sm + NANG * NMOM;
@@ -500,9 +500,13 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
     o->npot = npot;
     o->nfar = (npot == 1) ? 0 : nfar;
   }
-  double* mo = mom + ((size_t)c * nfo + k) * NMOM;
+  double* mv = momv + ((size_t)c * nfo + k) * MOM_LD;
   if (npot == 1 || nfar == 0) {
-    if (tid < NMOM) mo[tid] = 0.0;
+    if (tid < MOM_LD) mv[tid] = 0.0;
+    if (tid == 0) {
+      o->keep = 0ull;
+      o->lmax = 0;
+    }
     return;
   }
   // exact potential on the Lebedev sphere of radius RCUT around CG
@@ -519,7 +523,7 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
       boys_all(boys_tab, xx, chgd, s3, s4, s5);
       monomials(rx, ry, rz, mono);
       const size_t pk = (size_t)(ci.p0 + qq) * nfo + k;
-      v += pair_potential(coef + pk * NCOEF, mono, maxfmt[pk], s3, s4, s5);
+      v += pair_potential(coef + pk * COEF_LD, mono, maxfmt[pk], s3, s4, s5);
     }
     vang[tid] = v;
     // harmonics at the normalised sphere point
@@ -530,6 +534,8 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
     for (int m = 0; m < NMOM; ++m) prod[tid * NMOM + m] = c_leb_w[tid] * Y[m] * v;
   }
   __syncthreads();
+  __shared__ double s_mom[NMOM];
+  __shared__ unsigned long long s_keep_bits;
   if (tid < NMOM) {
     double s = 0.0;
     for (int i = 0; i < NANG; ++i) s += prod[i * NMOM + tid];
@@ -538,7 +544,43 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
     const double h = sqrt(rcut * rcut);
     double rl = h;
     for (int j = 1; j <= l; ++j) rl = h * rl;
-    mo[tid] = s * rl;
+    s_mom[tid] = s * rl;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // skip rule of poisson1.f:1252-1270 with RI1 = 1/RCUT, an upper bound of
+    // 1/r over every far point: keeps every term the reference keeps
+    const double ri1 = 1.0 / rcut;
+    unsigned long long keep = 0ull;
+    int lmx = 0, m = 0;
+    double rt = ri1;
+    for (int l = 0; l <= LM; ++l) {
+      for (int j = -l; j <= l; ++j, ++m)
+        if (!(fabs((2 * l + 1) * s_mom[m] * rt) < 1.0e-12)) {
+          keep |= (1ull << m);
+          lmx = l;
+        }
+      rt *= ri1;
+    }
+    o->keep = keep;
+    o->lmax = lmx;
+    s_keep_bits = keep;
+  }
+  __syncthreads();
+  // normalised moments with the skipped terms zeroed: M_lm * sqrt(NRUN (2l+1)/4pi (l-m)!/(l+m)!)
+  if (tid < NMOM) {
+    int l = 0;
+    while ((l + 1) * (l + 1) <= tid) ++l;
+    const int j = tid - l * l;
+    const int m = (j + 1) / 2;
+    const int nrun = (m == 0) ? 1 : 2;
+    double facfc = (2 * l + 1) * (1.0 / (16 * atan(1.0)));
+    for (int mm = 0; mm < m; ++mm) facfc = facfc / ((l - mm > 1 ? l - mm : 1) * (l + mm + 1));
+    const double vf = sqrt(nrun * facfc);
+    const bool kept = (s_keep_bits >> tid) & 1ull;
+    mv[tid] = kept ? s_mom[tid] * vf : 0.0;
+  } else if (tid < MOM_LD) {
+    mv[tid] = 0.0;
   }
 }
 
@@ -549,190 +591,12 @@ void init_call_setup() {
 
 void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, int nspn,
                        const double* coef, const int8_t* maxfmt, const double* cgp, const MeshDev& M,
-                       const double* boys_tab, CallFO* cfo, double* mom, cudaStream_t st) {
+                       const double* boys_tab, CallFO* cfo, double* momv, cudaStream_t st) {
   if (ncalls <= 0) return;
   const size_t smem = sizeof(double) * (NANG * NMOM + NANG);
   dim3 grid(ncalls, nfo);
   k_call_setup<<<grid, SETUP_THREADS, smem, st>>>(calls, pairs, nfo, nspn, coef, maxfmt, cgp, M, boys_tab,
-                                                   cfo, mom);
-}
-
-// ---------------------------------------------------------------------------
-// Coulomb evaluation
-// ---------------------------------------------------------------------------
-// Each CTA owns one spatial tile of TILE points and a chunk of KCH FOs; it walks
-// every POISSON1 call in order, so the per-point sums are deterministic.
-template <int KCH>
-__global__ void __launch_bounds__(TILE) k_coulomb_eval(int ncalls, const CallInfo* __restrict__ calls,
-                                                       const PairGeo* __restrict__ pairs, int nfo,
-                                                       const double* __restrict__ coef,
-                                                       const int8_t* __restrict__ maxfmt,
-                                                       const CallFO* __restrict__ cfo,
-                                                       const double* __restrict__ mom, MeshDev M,
-                                                       const double* __restrict__ boys_tab,
-                                                       double* __restrict__ vh, int ldv) {
-  __shared__ double s_cg[KCH][3];
-  __shared__ double s_rc2[KCH];
-  __shared__ int s_stat[KCH];   // 0 all near, 1 all far, 2 mixed
-  __shared__ int s_npot[KCH];
-  __shared__ int s_lmax[KCH];
-  __shared__ unsigned long long s_keep[KCH];
-  __shared__ int s_anynear, s_anyfar;
-  const int tile = blockIdx.x;
-  const int k0 = blockIdx.y * KCH;
-  const int nk = min(KCH, nfo - k0);
-  const int tid = threadIdx.x;
-  const int p = tile * TILE + tid;
-  const bool active = p < M.n;
-  const double X = active ? M.x[p] : 0.0, Y = active ? M.y[p] : 0.0, Z = active ? M.z[p] : 0.0;
-  const double lo[3] = {M.tile_lo[3 * tile], M.tile_lo[3 * tile + 1], M.tile_lo[3 * tile + 2]};
-  const double hi[3] = {M.tile_hi[3 * tile], M.tile_hi[3 * tile + 1], M.tile_hi[3 * tile + 2]};
-  double acc[KCH];
-#pragma unroll
-  for (int k = 0; k < KCH; ++k) acc[k] = 0.0;
-  for (int c = 0; c < ncalls; ++c) {
-    __syncthreads();
-    if (tid == 0) {
-      s_anynear = 0;
-      s_anyfar = 0;
-    }
-    __syncthreads();
-    if (tid < nk) {
-      const CallFO f = cfo[(size_t)c * nfo + k0 + tid];
-      double dmin2, dmax2;
-      box_dist2(lo, hi, f.cg, dmin2, dmax2);
-      int st;
-      if (f.npot == 1) st = 0;
-      else if (dmin2 > f.rcut2 * (1.0 + 1e-9)) st = 1;
-      else if (dmax2 < f.rcut2 * (1.0 - 1e-9)) st = 0;
-      else st = 2;
-      s_cg[tid][0] = f.cg[0];
-      s_cg[tid][1] = f.cg[1];
-      s_cg[tid][2] = f.cg[2];
-      s_rc2[tid] = f.rcut2;
-      s_stat[tid] = st;
-      s_npot[tid] = f.npot;
-      if (st != 1) atomicOr(&s_anynear, 1);
-      if (st != 0) {
-        atomicOr(&s_anyfar, 1);
-        // multipole skip rule of poisson1.f:1252-1270 with RI1 from the tile box
-        const double* mo = mom + ((size_t)c * nfo + k0 + tid) * NMOM;
-        const double ri1 = (dmin2 > 0.0) ? 1.0 / sqrt(dmin2) : DBL_MAX;
-        unsigned long long keep = 0ull;
-        int lmx = 0;
-        double rt = ri1;
-        int m = 0;
-        for (int l = 0; l <= LM; ++l) {
-          for (int j = -l; j <= l; ++j, ++m) {
-            const double tst = fabs((2 * l + 1) * mo[m] * rt);
-            if (!(tst < 1.0e-12)) {
-              keep |= (1ull << m);
-              lmx = l;
-            }
-          }
-          rt = (ri1 == DBL_MAX) ? DBL_MAX : rt * ri1;
-        }
-        s_keep[tid] = keep;
-        s_lmax[tid] = lmx;
-      }
-    }
-    __syncthreads();
-    const CallInfo ci = calls[c];
-    if (s_anynear) {
-      // per-point near flags
-      unsigned nearmask = 0u;
-      if (active) {
-#pragma unroll
-        for (int k = 0; k < KCH; ++k) {
-          if (k >= nk) break;
-          const int st = s_stat[k];
-          bool nr = (st == 0);
-          if (st == 2) {
-            const double cgk[3] = {s_cg[k][0], s_cg[k][1], s_cg[k][2]};
-            nr = !(sqdist_rn(X, Y, Z, cgk) > s_rc2[k]);
-          }
-          if (nr) nearmask |= (1u << k);
-        }
-      }
-      if (nearmask) {
-        for (int q = 0; q < ci.np; ++q) {
-          const PairGeo& g = pairs[ci.p0 + q];
-          const double rx = X - g.C[0], ry = Y - g.C[1], rz = Z - g.C[2];
-          const double xx = g.delta * (rz * rz + ry * ry + rx * rx);
-          const double chgd = exp(-xx);
-          double s3[3], s4[4], s5[5], mono[35];
-          boys_all(boys_tab, xx, chgd, s3, s4, s5);
-          monomials(rx, ry, rz, mono);
-          const size_t pk = (size_t)(ci.p0 + q) * nfo + k0;
-#pragma unroll
-          for (int k = 0; k < KCH; ++k) {
-            if (k >= nk) break;
-            if (nearmask & (1u << k))
-              acc[k] += pair_potential(coef + (pk + k) * NCOEF, mono, maxfmt[pk + k], s3, s4, s5);
-          }
-        }
-      }
-    }
-    if (s_anyfar && active) {
-#pragma unroll
-      for (int k = 0; k < KCH; ++k) {
-        if (k >= nk) break;
-        if (s_stat[k] == 0 || s_npot[k] == 1) continue;
-        const double cgk[3] = {s_cg[k][0], s_cg[k][1], s_cg[k][2]};
-        const double r2 = sqdist_rn(X, Y, Z, cgk);
-        if (!(r2 > s_rc2[k])) continue;
-        const double hn = 1.0 / sqrt(r2);
-        const double ux = hn * (X - cgk[0]), uy = hn * (Y - cgk[1]), uz = hn * (Z - cgk[2]);
-        const int lmx = s_lmax[k];
-        const unsigned long long keep = s_keep[k];
-        double Yh[NMOM];
-        harmonics6(lmx, ux, uy, uz, Yh);
-        const double* mo = mom + ((size_t)c * nfo + k0 + k) * NMOM;
-        double pot = 0.0, rec = hn;
-        int m = 0;
-        for (int l = 0; l <= lmx; ++l) {
-          for (int j = -l; j <= l; ++j, ++m)
-            if (keep & (1ull << m)) pot += mo[m] * Yh[m] * rec;
-          rec *= hn;
-        }
-        acc[k] += pot;
-      }
-    }
-  }
-  if (active) {
-#pragma unroll
-    for (int k = 0; k < KCH; ++k)
-      if (k < nk) vh[(size_t)(k0 + k) * ldv + p] = acc[k];
-  }
-}
-
-void launch_coulomb_eval(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, const double* coef,
-                         const int8_t* maxfmt, const CallFO* cfo, const double* mom, const MeshDev& M,
-                         const double* boys_tab, double* vh, int ldv, cudaStream_t st) {
-  constexpr int KCH = 8;
-  dim3 grid(M.ntiles, (nfo + KCH - 1) / KCH);
-  k_coulomb_eval<KCH><<<grid, TILE, 0, st>>>(ncalls, calls, pairs, nfo, coef, maxfmt, cfo, mom, M, boys_tab, vh,
-                                             ldv);
-}
-
-// Algorithmic work of the Coulomb evaluation: near (pair, point, FO) and far
-// (call, point, FO) evaluations; cnt[0] += near, cnt[1] += far.
-__global__ void k_work_counts(int ncalls, const CallInfo* __restrict__ calls, int nfo, int npts,
-                              const CallFO* __restrict__ cfo, unsigned long long* __restrict__ cnt) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (size_t)ncalls * nfo) return;
-  const int c = (int)(i / nfo);
-  const CallFO f = cfo[i];
-  const unsigned long long nearp = (unsigned long long)(npts - f.nfar);
-  atomicAdd(&cnt[0], nearp * (unsigned long long)calls[c].np);
-  atomicAdd(&cnt[1], (unsigned long long)f.nfar);
-}
-
-void launch_work_counts(int ncalls, const CallInfo* calls, int nfo, int npts, const CallFO* cfo,
-                        unsigned long long* cnt, cudaStream_t st) {
-  const size_t n = (size_t)ncalls * nfo;
-  if (n == 0) return;
-  k_work_counts<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ncalls, calls, nfo, npts, cfo, cnt);
+                                                   cfo, momv);
 }
 
 // ---------------------------------------------------------------------------

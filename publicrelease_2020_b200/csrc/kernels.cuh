@@ -40,31 +40,35 @@ void launch_basis_values(const BasisDev& B, int nderv, int npts, const double* p
 // u[(k*nprim + gp)*10 + comp] = sum_con BFCON(ib,con,l(comp)) C(k, local(l,comp,con))
 void launch_prim_u(const BasisDev& B, int nfo, const double* cfo, int ldc, double* u, cudaStream_t st);
 
-// Per (pair, FO): 46 potential coefficients, Boys variant, centre-of-gravity partials.
+// Per (pair, FO): 46 potential coefficients (rows of COEF_LD doubles, zero
+// padded), Boys variant, centre-of-gravity partials.
 void launch_pair_coef(int npairs, const PairGeo* pairs, const CallInfo* calls, int nfo, int nprim,
                       const double* u, int nspn, double* coef, int8_t* maxfmt, double* cgp,
                       cudaStream_t st);
 
-// Per (call, FO): CG, RCUT, NPOT, multipole moments.
+// Per (call, FO): CG, RCUT, NPOT, skip mask and normalised multipole moments
+// momv[(c*nfo + k)*MOM_LD + lm] (skipped terms and padding zero).
+void init_call_setup();
 void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, int nspn,
                        const double* coef, const int8_t* maxfmt, const double* cgp, const MeshDev& M,
-                       const double* boys_tab, CallFO* cfo, double* mom, cudaStream_t st);
+                       const double* boys_tab, CallFO* cfo, double* momv, cudaStream_t st);
 
-// Coulomb potential of every FO at every mesh point: vh[k*ldv + p].
-void launch_coulomb_eval(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo,
-                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* mom,
-                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, cudaStream_t st);
-
-// FP64 tensor-core form of the Coulomb evaluation (csrc/coulomb_mma.cu).
+// Coulomb potential of every FO at every mesh point, vh[k*ldv + p], on the
+// FP64 tensor cores (csrc/coulomb_mma.cu).  Calls whose near/far geometry is
+// identical for every FO go through the shared-geometry kernel, the rest
+// through the per-FO kernel, which adds its part.  per_fo_only routes every
+// call through the per-FO kernel (a cross-check of the two forms).
+// cnt[0] += near (pair, point, FO) evaluations, cnt[1] += far (call, point, FO).
+struct CoulombScratch {
+  int8_t* pair_fmt;    // npairs
+  CallShare* share;    // ncalls
+  int* lists;          // 2*ncalls + 2: shared calls, per-FO calls, the two counts
+};
 void init_coulomb_mma();
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
-                        const double* coef, const int8_t* maxfmt, int8_t* pair_fmt, const CallFO* cfo,
-                        const double* mom, const MeshDev& M, const double* boys_tab, double* vh, int ldv,
-                        cudaStream_t st);
-void init_call_setup();
-
-void launch_work_counts(int ncalls, const CallInfo* calls, int nfo, int npts, const CallFO* cfo,
-                        unsigned long long* cnt, cudaStream_t st);
+                        const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
+                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,
+                        const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st);
 
 // Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as
 // in apotnl_sic.F:419) from the FO values/derivatives phi[(ch*nfo+k)*ldp+p];

@@ -351,7 +351,9 @@ struct flosic_ctx {
   // scratch
   DevBuf<double> d_basis, d_fodpts, d_psig, d_tmat, d_u, d_coef, d_cgp, d_mom, d_part, d_sums, d_sic, d_tmp;
   DevBuf<int8_t> d_maxfmt, d_pairfmt;
-  bool scalar_coulomb = false;   // FLOSIC_COULOMB=scalar selects the per-thread kernel (A/B checks)
+  DevBuf<CallShare> d_share;
+  DevBuf<int> d_lists;
+  bool per_fo_coulomb = false;   // FLOSIC_COULOMB=perfo: every call through the per-FO kernel (A/B checks)
   DevBuf<unsigned long long> d_cnt;
   unsigned long long work_near = 0, work_far = 0;
   DevBuf<CallFO> d_callfo;
@@ -710,11 +712,11 @@ void coulomb(flosic_ctx* c, int s) {
   c->d_u.ensure((size_t)nf * c->nprim * 10);
   launch_prim_u(c->basis_dev(), nf, S.cfo.p, c->nbasis, c->d_u.p, st);
   c->launches++;
-  c->d_coef.ensure((size_t)std::max(npairs, 1) * nf * NCOEF);
+  c->d_coef.ensure((size_t)std::max(npairs, 1) * nf * COEF_LD);
   c->d_maxfmt.ensure((size_t)std::max(npairs, 1) * nf);
   c->d_cgp.ensure((size_t)std::max(npairs, 1) * nf * 4);
   c->d_callfo.ensure((size_t)std::max(ncalls, 1) * nf);
-  c->d_mom.ensure((size_t)std::max(ncalls, 1) * nf * NMOM);
+  c->d_mom.ensure((size_t)std::max(ncalls, 1) * nf * MOM_LD);
   CUDA_CHECK(cudaEventRecord(c->ev[2], st));
   launch_pair_coef(npairs, c->d_pairs.p, c->d_calls.p, nf, c->nprim, c->d_u.p, c->nspn, c->d_coef.p,
                    c->d_maxfmt.p, c->d_cgp.p, st);
@@ -724,20 +726,15 @@ void coulomb(flosic_ctx* c, int s) {
   c->launches++;
   CUDA_CHECK(cudaEventRecord(c->ev[3], st));
   S.vh.ensure((size_t)nf * P);
-  if (c->scalar_coulomb) {
-    launch_coulomb_eval(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                        c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
-  } else {
-    c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
-    launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_pairfmt.p,
-                       c->d_callfo.p, c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, st);
-    c->launches++;
-  }
-  c->launches++;
+  c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
+  c->d_share.ensure((size_t)std::max(ncalls, 1));
+  c->d_lists.ensure((size_t)2 * ncalls + 2);
   c->d_cnt.ensure(2);
   CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 2 * sizeof(unsigned long long), st));
-  launch_work_counts(ncalls, c->d_calls.p, nf, P, c->d_callfo.p, c->d_cnt.p, st);
-  c->launches++;
+  CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p};
+  launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
+                     c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, scr, c->d_cnt.p, st);
+  c->launches += c->per_fo_coulomb ? 4 : 5;
   unsigned long long cnt[2];
   CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
@@ -981,7 +978,7 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     CUDA_CHECK(cudaSetDevice(device));
     auto* c = new flosic_ctx;
     c->device = device;
-    if (const char* e = std::getenv("FLOSIC_COULOMB")) c->scalar_coulomb = (std::string(e) == "scalar");
+    if (const char* e = std::getenv("FLOSIC_COULOMB")) c->per_fo_coulomb = (std::string(e) == "perfo");
     CUDA_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
       delete c;
@@ -1017,6 +1014,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_basis.release(); c->d_fodpts.release(); c->d_psig.release(); c->d_tmat.release(); c->d_u.release();
   c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
   c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
+  c->d_share.release(); c->d_lists.release();
   if (c->blas) cublasDestroy(c->blas);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;

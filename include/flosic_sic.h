@@ -121,7 +121,8 @@ int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, doub
    (ms[0]=FO construction, [1]=orbital/density, [2]=Coulomb setup, [3]=Coulomb
    evaluation, [4]=XC+energies, [5]=SIC matrix, [6]=forces), pair/call counts, and the
    Coulomb work of the last cycle: work[0] = near (pair, point, FO) evaluations,
-   work[1] = far (call, point, FO) multipole evaluations. */
+   work[1] = far (call, point, FO) multipole evaluations, work[2] = multipole terms
+   those far evaluations keep under the skip rule of poisson1.f:1252-1270. */
 int flosic_sic_stats(flosic_ctx* ctx, int64_t* launches, double* stage_ms, int64_t* npairs,
                      int64_t* ncalls, int64_t* work);
 

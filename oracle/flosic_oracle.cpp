@@ -898,6 +898,8 @@ struct PairRec {
 
 struct Stats {
   long long pairs = 0, batches = 0, weird = 0, near = 0, far = 0;
+  long long near_multi = 0, far_multi = 0;  // the part from calls of more than one pair
+  long long npot1_multi = 0, calls_multi = 0;
 };
 
 void poisson1(const Problem& P, const std::vector<PairRec>& prs, int nspn, bool gga, bool exact,
@@ -1015,6 +1017,12 @@ void poisson1(const Problem& P, const std::vector<PairRec>& prs, int nspn, bool 
   if (st) {
     st->near += (long long)jptr.size() * n;
     st->far += (long long)iptr.size();
+    if (n > 1) {
+      st->near_multi += (long long)jptr.size() * n;
+      st->far_multi += (long long)iptr.size();
+      st->calls_multi += 1;
+      if (npot == 1) st->npot1_multi += 1;
+    }
   }
   std::vector<double> potnl(jptr.size(), 0.0);
   double asymptot[NANG];
@@ -2222,6 +2230,10 @@ int orc_coupot_sic(orc_problem* p, int spin, int iorb, int exact, double* coulom
     stats[2] = st.weird;
     stats[3] = st.near;
     stats[4] = st.far;
+    stats[5] = st.near_multi;
+    stats[6] = st.far_multi;
+    stats[7] = st.npot1_multi;
+    stats[8] = st.calls_multi;
   }
   return 0;
 }

@@ -134,7 +134,7 @@ class Oracle:
         n = self.sysm.nmsh
         coul = np.zeros(n)
         rhog = np.zeros(10 * n)
-        st = np.zeros(5, dtype=np.int64)
+        st = np.zeros(9, dtype=np.int64)
         _check(lib().orc_coupot_sic(self.h, spin, iorb, int(exact), coul, rhog, st))
         return coul, rhog.reshape(10, n), st
 
@@ -178,9 +178,10 @@ class Oracle:
                     cfrm=cfrm.reshape(2, ld, 3), esic=float(esic[0]))
 
     def pair_stats(self, spin=1, iorb=1):
-        st = np.zeros(5, dtype=np.int64)
+        st = np.zeros(9, dtype=np.int64)
         _check(lib().orc_pair_stats(self.h, spin, iorb, st))
-        return dict(pairs=int(st[0]), batches=int(st[1]), weird=int(st[2]), near=int(st[3]), far=int(st[4]))
+        return dict(pairs=int(st[0]), batches=int(st[1]), weird=int(st[2]), near=int(st[3]), far=int(st[4]),
+                    near_multi=int(st[5]), far_multi=int(st[6]), npot1_multi=int(st[7]), calls_multi=int(st[8]))
 
 
 def xc_point(xc, r10, w=1.0):

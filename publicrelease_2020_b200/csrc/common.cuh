@@ -63,7 +63,7 @@ struct CallShare {
   int32_t npot;
   int32_t kf;         // moment columns of the far segment: (lmax over FOs + 1)^2 rounded up to 4; 0 = none
   int32_t shared;     // 1 when the geometry is FO independent
-  int32_t pad;
+  int32_t ksum;       // multipole terms kept by the skip rule, summed over the FOs
 };
 
 #define FLOSIC_HD __host__ __device__ __forceinline__

@@ -20,14 +20,16 @@
 //                     (mma.sync m8n8k4 .f64).  A CTA owns 128 points and up to
 //                     128 FOs; segments are double buffered (A by cp.async, B by
 //                     the first four warps while the others multiply).
-//   k_coulomb_mma     the remaining calls, whose CG (charge weighted,
-//                     poisson1.f:503-520) differs per FO: near field as a GEMM
-//                     into a per-call accumulator merged per (FO, point), far
-//                     field per (FO, point).
+//   k_coulomb_perfo   the remaining calls, whose CG (charge weighted,
+//                     poisson1.f:503-520) differs per FO: the near field of the
+//                     FOs with near points in the tile as a GEMM over compacted
+//                     FO slots, added per (FO, point); the far field per
+//                     (FO, point).
 //
 // Both walk their calls in order, so every per-point sum is deterministic.
-// Both count the evaluations they perform: near (pair, point, FO) and far
-// (call, point, FO), the units of the reference's POISSON1 work.
+// Both count the evaluations they perform: near (pair, point, FO), far
+// (call, point, FO) and the multipole terms the far evaluations keep, the
+// units of the reference's POISSON1 work.
 #include <cfloat>
 
 #include "device_math.cuh"
@@ -78,24 +80,20 @@ __device__ __forceinline__ int tile_class(const double lo[3], const double hi[3]
   return 2;
 }
 
-// Unnormalised harmonics of harmonics.f times 1/r^(l+1), in the row order of
-// the moments (l*l + j; j = 0 for m = 0, 2m-1 and 2m for the two m > 0
-// partners), for l <= lmx.  The recursion of harmonics.f runs level by level;
-// here it runs m-major so that only a few values are live, but every value is
-// formed by the same operations on the same operands:
+// Unnormalised harmonics of harmonics.f in the row order of the moments
+// (l*l + j; j = 0 for m = 0, 2m-1 and 2m for the two m > 0 partners), for
+// l <= lmx.  The recursion of harmonics.f runs level by level; here it runs
+// m-major so that only a few values are live, but every value is formed by
+// the same operations on the same operands:
 //   m = l (sectoral):  C_l = (2l-1)(C_{l-1} ux - S_{l-1} uy),  S_l = (2l-1)(S_{l-1} ux + C_{l-1} uy)
 //   m < l:             P_l = ((2l-1)/(l-m)) P_{l-1} uz - ((l+m-1)/(l-m)) P_{l-2}
-// op(row, value) receives each term.
+// op(row, l, value) receives each term; the caller applies 1/r^(l+1).
 template <typename Op>
-__device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz, double hn, int lmx, Op op) {
-  double rec[LM + 1];
-  rec[0] = hn;
-#pragma unroll
-  for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
+__device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz, int lmx, Op op) {
   // m = 0
   {
-    op(0, 1.0 * rec[0]);
-    if (lmx >= 1) op(1, uz * rec[1]);
+    op(0, 0, 1.0);
+    if (lmx >= 1) op(1, 1, uz);
     double p2 = 1.0, p1 = uz;
 #pragma unroll
     for (int l = 2; l <= LM; ++l) {
@@ -103,7 +101,7 @@ __device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz
       const double facrc = 1.0 / l;
       const double aa = facrc * (2 * l - 1), bb = facrc * (l - 1);
       const double cu = aa * p1 * uz - bb * p2;
-      op(l * l, cu * rec[l]);
+      op(l * l, l, cu);
       p2 = p1;
       p1 = cu;
     }
@@ -119,8 +117,8 @@ __device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz
       sc = nc;
       ss = ns;
     }
-    op(m * m + 2 * m - 1, sc * rec[m]);
-    op(m * m + 2 * m, ss * rec[m]);
+    op(m * m + 2 * m - 1, m, sc);
+    op(m * m + 2 * m, m, ss);
     double c2 = 0.0, s2 = 0.0, c1 = sc, s1 = ss;
 #pragma unroll
     for (int l = m + 1; l <= LM; ++l) {
@@ -130,8 +128,8 @@ __device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz
       const double bb = (m == l - 1) ? 0.0 : facrc * (l + m - 1);
       const double cc = aa * c1 * uz - bb * c2;
       const double cs = aa * s1 * uz - bb * s2;
-      op(l * l + 2 * m - 1, cc * rec[l]);
-      op(l * l + 2 * m, cs * rec[l]);
+      op(l * l + 2 * m - 1, l, cc);
+      op(l * l + 2 * m, l, cs);
       c2 = c1;
       s2 = s1;
       c1 = cc;
@@ -248,15 +246,20 @@ __device__ __forceinline__ void zero_rows(double* g, int k) {
   for (int t = 0; t < k; ++t) g[(size_t)t * G_LD] = 0.0;
 }
 
-__device__ __forceinline__ void count_add(unsigned long long* cnt, unsigned long long near, unsigned long long far) {
+// cnt[0] near (pair, point, FO), cnt[1] far (call, point, FO), cnt[2] multipole
+// terms kept by the skip rule summed over the far evaluations.
+__device__ __forceinline__ void count_add(unsigned long long* cnt, unsigned long long near, unsigned long long far,
+                                          unsigned long long terms) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     near += __shfl_down_sync(0xffffffffu, near, o);
     far += __shfl_down_sync(0xffffffffu, far, o);
+    terms += __shfl_down_sync(0xffffffffu, terms, o);
   }
   if ((threadIdx.x & 31) == 0) {
     if (near) atomicAdd(&cnt[0], near);
     if (far) atomicAdd(&cnt[1], far);
+    if (terms) atomicAdd(&cnt[2], terms);
   }
 }
 
@@ -277,6 +280,7 @@ struct Segment {
   int idx;       // q or c
   int rows;      // contraction length, a multiple of 4
   int cls;       // tile class against the call's sphere
+  int ksum;      // kept multipole terms summed over all FOs (far segments)
   double cx, cy, cz, rc2;
 };
 
@@ -292,7 +296,7 @@ struct SegmentWalker {
   const int8_t* pair_fmt;
   double lo[3], hi[3];
   int li, sub;
-  int c, p0, np, cls, kf, npot;
+  int c, p0, np, cls, kf, npot, ksum;
   double cx, cy, cz, rc2;
   unsigned long long direct_far;  // far points of all-far tiles of calls without kept moments
 
@@ -307,6 +311,7 @@ struct SegmentWalker {
         cz = sh.cg[2];
         rc2 = sh.rcut2;
         kf = sh.kf;
+        ksum = sh.ksum;
         npot = sh.npot;
         p0 = ci.p0;
         np = ci.np;
@@ -316,7 +321,7 @@ struct SegmentWalker {
       if (sub < np) {
         const int q = p0 + sub;
         ++sub;
-        s = Segment{0, q, near_rows(pair_fmt[q]), cls, cx, cy, cz, rc2};
+        s = Segment{0, q, near_rows(pair_fmt[q]), cls, 0, cx, cy, cz, rc2};
         return true;
       }
       const bool want_far = npot == 2 && cls != 0;
@@ -324,7 +329,7 @@ struct SegmentWalker {
       ++li;
       if (want_far) {
         if (kf > 0 || cls == 2) {
-          s = Segment{1, c, kf, cls, cx, cy, cz, rc2};
+          s = Segment{1, c, kf, cls, ksum, cx, cy, cz, rc2};
           return true;
         }
         direct_far += (unsigned long long)npts;
@@ -369,7 +374,7 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
   }
   W.li = 0;
   W.sub = -1;
-  W.c = W.p0 = W.np = W.cls = W.kf = 0;
+  W.c = W.p0 = W.np = W.cls = W.kf = W.ksum = 0;
   W.npot = 1;
   W.cx = W.cy = W.cz = W.rc2 = 0.0;
   W.direct_far = 0ull;
@@ -380,7 +385,8 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < NT; ++b) V[a][b][0] = V[a][b][1] = 0.0;
-  unsigned long long my_near = 0, my_far = 0;
+  unsigned long long my_near = 0, my_far = 0, my_terms = 0;
+  const bool count_terms = blockIdx.y == 0;  // kept terms are summed over all FOs once per (call, point)
 
   // Stage segment s into buffer b: A rows by cp.async (all threads), B columns
   // by threads 0..127 (one point each).
@@ -420,11 +426,16 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
         }
         if (fr) {
           ++my_far;
+          if (count_terms) my_terms += (unsigned long long)s.ksum;
           if (s.rows > 0) {
             const double hn = 1.0 / sqrt(r2);
             const int kr = s.rows;
-            harmonics_mmajor(hn * (x - s.cx), hn * (y - s.cy), hn * (z - s.cz), hn, LM, [&](int row, double v) {
-              if (row < kr) g[(size_t)row * G_LD] = v;
+            double rec[LM + 1];
+            rec[0] = hn;
+#pragma unroll
+            for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
+            harmonics_mmajor(hn * (x - s.cx), hn * (y - s.cy), hn * (z - s.cz), LM, [&](int row, int l, double v) {
+              if (row < kr) g[(size_t)row * G_LD] = v * rec[l];
             });
             for (int t = NMOM; t < kr; ++t) g[(size_t)t * G_LD] = 0.0;
           }
@@ -479,83 +490,107 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
       }
   }
   if (tid == 0) my_far += W.direct_far;
-  count_add(cnt, my_near * (unsigned long long)nk, my_far * (unsigned long long)nk);
+  count_add(cnt, my_near * (unsigned long long)nk, my_far * (unsigned long long)nk, my_terms);
 }
 
 // ---------------------------------------------------------------------------
 // Per-FO-geometry calls
 // ---------------------------------------------------------------------------
-constexpr int MMA_PTS = TILE;               // 128 points per CTA
-constexpr int MMA_FOS = 64;                 // FOs per CTA
-constexpr int KPP = 48;                     // coefficients per pair, padded to a multiple of 4
-constexpr int PAIRS_PER_STEP = 2;
-constexpr int KSTEP = KPP * PAIRS_PER_STEP; // 96
-constexpr int A_LD = KSTEP + 4;             // 100: conflict-free A fragment loads
-
-struct MmaSmem {
-  double A[MMA_FOS * A_LD];
-  double G[KSTEP * G_LD];
-  double px[MMA_PTS], py[MMA_PTS], pz[MMA_PTS];
-  double cg[MMA_FOS][3];
-  double rc2[MMA_FOS];
-  int stat[MMA_FOS];
-  int npot[MMA_FOS];
-  int lmax[MMA_FOS];
-  int anynear, anyfar;
+// A CTA owns 128 points and up to 32*WM FOs and walks the per-FO calls in
+// order.  For each call it classifies the tile against every FO's sphere,
+// compacts the FOs with near points into slots, and contracts the G columns
+// of one pair per stage (double buffered) with the slots' coefficient rows
+// only, so the tensor work follows the FOs that are near rather than the
+// whole FO block.  The per-call result is added, masked per (FO, point), to
+// the CTA's own slice of vh (L2 resident); the far field of the call follows,
+// one FO per warp at a time with lanes over points.
+template <int WM>
+struct PerFOSmem {
+  double A[2][32 * WM * KSEG];  // slot rows of the stage's coefficients; far phase: the FOs' moments (A[0])
+  double B[2][KSEG * G_LD];     // G columns of the stage's pair
+  double px[TILE], py[TILE], pz[TILE];
+  double cg[32 * WM][3];
+  double rc2[32 * WM];
+  int stat[32 * WM];
+  int npot[32 * WM];
+  int lmax[32 * WM];
+  int nkeep[32 * WM];
+  int fo_of[32 * WM];           // slot -> FO (block-local)
+  unsigned bal[WM];             // per warp of the status phase: FOs with near points
+  unsigned balf[WM];            // per warp of the status phase: FOs with far points
+  int na;
 };
 
-// Far-field potential of one FO at one point: sum_lm MV[lm] H_lm.
+// Physical A row of slot s: slots fill m-tiles round robin over the WM warp
+// rows, so that a few active FOs keep several warps busy.
+template <int WM>
+__device__ __forceinline__ int slot_row(int s) {
+  const int g = s >> 3;
+  return (g % WM) * 32 + (g / WM) * 8 + (s & 7);
+}
+
+// Far-field potential of one FO at one point, sum_lm MV[lm] Y_lm(u) / r^(l+1),
+// summed per degree l and scaled once per degree.
 __device__ __forceinline__ double multipole(const double* __restrict__ mv, int lmx, double ux, double uy, double uz,
                                             double hn) {
-  double pot = 0.0;
-  harmonics_mmajor(ux, uy, uz, hn, lmx, [&](int row, double v) { pot += mv[row] * v; });
+  double acc[LM + 1];
+#pragma unroll
+  for (int l = 0; l <= LM; ++l) acc[l] = 0.0;
+  harmonics_mmajor(ux, uy, uz, lmx, [&](int row, int l, double v) { acc[l] += mv[row] * v; });
+  double pot = 0.0, rec = hn;
+#pragma unroll
+  for (int l = 0; l <= LM; ++l) {
+    pot += acc[l] * rec;
+    rec *= hn;
+  }
   return pot;
 }
 
+template <int WM>
 __global__ void __launch_bounds__(MMA_THREADS, 1)
-k_coulomb_mma(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
-              const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
-              const int8_t* __restrict__ pair_fmt, const CallFO* __restrict__ cfo, const double* __restrict__ momv,
-              MeshDev M, const double* __restrict__ boys_tab, double* __restrict__ vh, int ldv,
-              unsigned long long* __restrict__ cnt) {
+k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
+                const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
+                const int8_t* __restrict__ pair_fmt, const CallFO* __restrict__ cfo,
+                const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
+                double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
+  constexpr int FOB = 32 * WM, WN = 8 / WM, WPTS = TILE / WN, NT = WPTS / 8;
   const int* list = lists + ncalls;
   const int nl = lists[2 * ncalls + 1];
   if (accumulate && nl == 0) return;
   extern __shared__ __align__(128) unsigned char smraw[];
-  MmaSmem& S = *reinterpret_cast<MmaSmem*>(smraw);
+  PerFOSmem<WM>& S = *reinterpret_cast<PerFOSmem<WM>*>(smraw);
   const int tile = blockIdx.x;
-  const int k0 = blockIdx.y * MMA_FOS;
-  const int nk = min(MMA_FOS, nfo - k0);
+  const int k0 = blockIdx.y * FOB;
+  const int nk = min(FOB, nfo - k0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp & 1, wn = warp >> 1;
-  const int p0 = tile * MMA_PTS;
-  const int np = min(MMA_PTS, M.n - p0);
-  for (int i = tid; i < MMA_PTS; i += MMA_THREADS) {
+  const int wm = warp % WM, wn = warp / WM;
+  const int p0 = tile * TILE;
+  const int np = min(TILE, M.n - p0);
+  for (int i = tid; i < TILE; i += MMA_THREADS) {
     const bool a = i < np;
     S.px[i] = a ? M.x[p0 + i] : 0.0;
     S.py[i] = a ? M.y[p0 + i] : 0.0;
     S.pz[i] = a ? M.z[p0 + i] : 0.0;
   }
-  const double lo[3] = {M.tile_lo[3 * tile], M.tile_lo[3 * tile + 1], M.tile_lo[3 * tile + 2]};
-  const double hi[3] = {M.tile_hi[3 * tile], M.tile_hi[3 * tile + 1], M.tile_hi[3 * tile + 2]};
-  // accumulator ownership: FO k = wm*32 + mt*8 + (lane>>2), point p = wn*32 + nt*8 + 2*(lane&3) + i
-  double V[4][4][2], T[4][4][2];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) V[a][b][0] = V[a][b][1] = 0.0;
-  unsigned long long my_near = 0, my_far = 0;
+  if (!accumulate)
+    for (int e = tid; e < nk * TILE; e += MMA_THREADS) {
+      const int k = e / TILE, p = e - k * TILE;
+      if (p < np) vh[(size_t)(k0 + k) * ldv + p0 + p] = 0.0;
+    }
+  double lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = M.tile_lo[3 * tile + d];
+    hi[d] = M.tile_hi[3 * tile + d];
+  }
+  unsigned long long my_near = 0, my_far = 0, my_terms = 0;
 
   for (int li = 0; li < nl; ++li) {
     const int c = list[li];
-    __syncthreads();
-    if (tid == 0) {
-      S.anynear = 0;
-      S.anyfar = 0;
-    }
-    __syncthreads();
-    if (tid < MMA_FOS) {
-      int st = 1, npot = 2, lmx = 0;
+    const CallInfo ci = calls[c];
+    __syncthreads();  // the previous call is done with every shared buffer and with vh
+    // status of every FO of the block for this tile, and the active slots
+    if (tid < FOB) {
+      int st = 1, npot = 2, lmx = 0, nkeep = 0;
       double cgx = 0, cgy = 0, cgz = 0, rc2 = 0;
       if (tid < nk) {
         const CallFO f = cfo[(size_t)c * nfo + k0 + tid];
@@ -565,10 +600,9 @@ k_coulomb_mma(int ncalls, const int* __restrict__ lists, int accumulate, const C
         rc2 = f.rcut2;
         npot = f.npot;
         st = (npot == 1) ? 0 : tile_class(lo, hi, cgx, cgy, cgz, rc2);
-        if (st != 1) atomicOr(&S.anynear, 1);
         if (st != 0 && npot == 2) {
-          atomicOr(&S.anyfar, 1);
           lmx = f.lmax;
+          nkeep = __popcll(f.keep);
         }
       }
       S.stat[tid] = st;
@@ -578,118 +612,137 @@ k_coulomb_mma(int ncalls, const int* __restrict__ lists, int accumulate, const C
       S.cg[tid][2] = cgz;
       S.rc2[tid] = rc2;
       S.lmax[tid] = lmx;
+      S.nkeep[tid] = nkeep;
+      const bool act = tid < nk && st != 1;
+      const unsigned b = __ballot_sync(0xffffffffu, act);
+      const unsigned bf = __ballot_sync(0xffffffffu, tid < nk && st != 0 && npot == 2);
+      if (lane == 0) {
+        S.bal[warp] = b;
+        S.balf[warp] = bf;
+      }
     }
     __syncthreads();
-    const CallInfo ci = calls[c];
-    if (S.anynear) {
+    if (tid < FOB) {
+      int before = 0;
+      for (int w = 0; w < warp; ++w) before += __popc(S.bal[w]);
+      const unsigned b = S.bal[warp];
+      if ((b >> lane) & 1u) S.fo_of[before + __popc(b & ((1u << lane) - 1u))] = tid;
+      if (tid == FOB - 1) S.na = before + __popc(b);
+    }
+    __syncthreads();
+    const int na = S.na;
+    bool anyfar = false;
+#pragma unroll
+    for (int w = 0; w < WM; ++w) anyfar = anyfar || S.balf[w] != 0u;
+
+    if (na > 0) {
+      double T[4][NT][2];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) T[a][b][0] = T[a][b][1] = 0.0;
-      for (int q0 = 0; q0 < ci.np; q0 += PAIRS_PER_STEP) {
-        const int npc = min(PAIRS_PER_STEP, ci.np - q0);
-        __syncthreads();
-        // G for (pair ql, point p): Boys values times monomials
-        {
-          const int ql = tid >> 7, p = tid & 127;
-          double* g = &S.G[(size_t)ql * KPP * G_LD + p];
-          if (ql < npc && p < np) {
-            const int q = ci.p0 + q0 + ql;
+        for (int b = 0; b < NT; ++b) T[a][b][0] = T[a][b][1] = 0.0;
+      auto stage = [&](int q, int b) {
+        const double* src = coef + (size_t)q * nfo * COEF_LD;
+        double* dst = S.A[b];
+        for (int e = tid; e < na * (KSEG / 2); e += MMA_THREADS) {
+          const int s = e / (KSEG / 2), ch = e - s * (KSEG / 2);
+          cp_async16(dst + slot_row<WM>(s) * KSEG + 2 * ch, src + (size_t)(k0 + S.fo_of[s]) * COEF_LD + 2 * ch);
+        }
+        cp_async_commit();
+        if (tid < TILE) {
+          const int p = tid;
+          double* g = &S.B[b][p];
+          const int kn = near_rows(pair_fmt[q]);
+          if (p < np) {
             const PairGeo& pg = pairs[q];
             const double rx = S.px[p] - pg.C[0], ry = S.py[p] - pg.C[1], rz = S.pz[p] - pg.C[2];
             const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
             double F[5];
-            boys_fmt(boys_tab, xx, exp(-xx), pair_fmt[q], F);
-            write_g(g, KPP, rx, ry, rz, F);
+            boys_fmt(boys_tab, xx, exp(-xx), kn >= 48 ? 5 : (kn == 32 ? 4 : 3), F);
+            write_g(g, kn, rx, ry, rz, F);
           } else {
-            zero_rows(g, KPP);
+            zero_rows(g, kn);
           }
         }
-        // coefficient tile A[k][ql*48 + t]
-        for (int e = tid; e < MMA_FOS * KSTEP; e += MMA_THREADS) {
-          const int k = e / KSTEP, col = e - k * KSTEP;
-          const int ql = col / KPP, t = col - ql * KPP;
-          double v = 0.0;
-          if (k < nk && ql < npc) v = coef[((size_t)(ci.p0 + q0 + ql) * nfo + k0 + k) * COEF_LD + t];
-          S.A[k * A_LD + col] = v;
+      };
+      stage(ci.p0, 0);
+      cp_async_wait_all();
+      __syncthreads();
+      int buf = 0;
+      for (int qi = 0; qi < ci.np; ++qi) {
+        const int q = ci.p0 + qi;
+        if (qi + 1 < ci.np) stage(q + 1, buf ^ 1);
+        const int kq = near_rows(pair_fmt[q]);
+        const double* As = &S.A[buf][(wm * 32 + (lane >> 2)) * KSEG + (lane & 3)];
+        const double* Bs = &S.B[buf][(lane & 3) * G_LD + wn * WPTS + (lane >> 2)];
+        for (int kk = 0; kk < kq; kk += 4) {
+          double af[4], bf[NT];
+#pragma unroll
+          for (int mt = 0; mt < 4; ++mt) af[mt] = As[mt * 8 * KSEG + kk];
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(size_t)kk * G_LD + nt * 8];
+#pragma unroll
+          for (int mt = 0; mt < 4; ++mt) {
+            if ((mt * WM + wm) * 8 >= na) continue;
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) dmma884(T[mt][nt][0], T[mt][nt][1], af[mt], bf[nt]);
+          }
         }
+        cp_async_wait_all();
         __syncthreads();
-        const int kend = npc * KPP;
-        const double* Aw = &S.A[(wm * 32 + (lane >> 2)) * A_LD + (lane & 3)];
-        const double* Gw = &S.G[(size_t)(lane & 3) * G_LD + wn * 32 + (lane >> 2)];
-        for (int kk = 0; kk < kend; kk += 4) {
-          double af[4], bf[4];
-#pragma unroll
-          for (int mt = 0; mt < 4; ++mt) af[mt] = Aw[mt * 8 * A_LD + kk];
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) bf[nt] = Gw[(size_t)kk * G_LD + nt * 8];
-#pragma unroll
-          for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) dmma884(T[mt][nt][0], T[mt][nt][1], af[mt], bf[nt]);
-        }
+        buf ^= 1;
       }
-      // near merge
+      // masked add of the call's near field to vh
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt) {
-        const int k = wm * 32 + mt * 8 + (lane >> 2);
+        const int s = (mt * WM + wm) * 8 + (lane >> 2);
+        if (s >= na) continue;
+        const int k = S.fo_of[s];
         const int st = S.stat[k];
-        if (k >= nk || st == 1) continue;
+        const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
+        double* vk = vh + (size_t)(k0 + k) * ldv + p0;
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
+        for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
           for (int i = 0; i < 2; ++i) {
-            const int p = wn * 32 + nt * 8 + 2 * (lane & 3) + i;
+            const int p = wn * WPTS + nt * 8 + 2 * (lane & 3) + i;
+            if (p >= np) continue;
             bool nr = (st == 0);
-            if (st == 2)
-              nr = !(sqdist_rn2(S.px[p], S.py[p], S.pz[p], S.cg[k][0], S.cg[k][1], S.cg[k][2]) > S.rc2[k]);
+            if (st == 2) nr = !(sqdist_rn2(S.px[p], S.py[p], S.pz[p], cx, cy, cz) > rc2);
             if (nr) {
-              V[mt][nt][i] += T[mt][nt][i];
-              if (p < np) my_near += (unsigned long long)ci.np;
+              vk[p] += T[mt][nt][i];
+              my_near += (unsigned long long)ci.np;
             }
           }
       }
     }
-    if (S.anyfar) {
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const int k = wm * 32 + mt * 8 + (lane >> 2);
-        if (k >= nk) continue;
-        const int st = S.stat[k];
-        if (st == 0 || S.npot[k] == 1) continue;
+
+    if (anyfar) {
+      __syncthreads();  // near phase done with A
+      const double* mg = momv + ((size_t)c * nfo + k0) * MOM_LD;
+      for (int e = tid; e < nk * MOM_LD; e += MMA_THREADS) S.A[0][e] = mg[e];
+      __syncthreads();
+      for (int k = warp; k < nk; k += MMA_THREADS / 32) {
+        if (S.stat[k] == 0 || S.npot[k] == 1) continue;
         const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
         const int lmx = S.lmax[k];
-        const double* mv = momv + ((size_t)c * nfo + k0 + k) * MOM_LD;
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const int p = wn * 32 + nt * 8 + 2 * (lane & 3) + i;
-            if (p >= np) continue;
-            const double r2 = sqdist_rn2(S.px[p], S.py[p], S.pz[p], cx, cy, cz);
-            if (!(r2 > rc2)) continue;
+        const unsigned long long nkeep = (unsigned long long)S.nkeep[k];
+        const double* mv = &S.A[0][k * MOM_LD];
+        double* vk = vh + (size_t)(k0 + k) * ldv + p0;
+        for (int p = lane; p < np; p += 32) {
+          const double x = S.px[p], y = S.py[p], z = S.pz[p];
+          const double r2 = sqdist_rn2(x, y, z, cx, cy, cz);
+          if (r2 > rc2) {
             ++my_far;
+            my_terms += nkeep;
             const double hn = 1.0 / sqrt(r2);
-            V[mt][nt][i] += multipole(mv, lmx, hn * (S.px[p] - cx), hn * (S.py[p] - cy), hn * (S.pz[p] - cz), hn);
+            vk[p] += multipole(mv, lmx, hn * (x - cx), hn * (y - cy), hn * (z - cz), hn);
           }
+        }
       }
     }
   }
-#pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int k = wm * 32 + mt * 8 + (lane >> 2);
-    if (k >= nk) continue;
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int p = wn * 32 + nt * 8 + 2 * (lane & 3) + i;
-        if (p >= np) continue;
-        double* o = &vh[(size_t)(k0 + k) * ldv + p0 + p];
-        *o = accumulate ? *o + V[mt][nt][i] : V[mt][nt][i];
-      }
-  }
-  count_add(cnt, my_near, my_far);
+  count_add(cnt, my_near, my_far, my_terms);
 }
 
 // ---------------------------------------------------------------------------
@@ -712,16 +765,22 @@ __global__ void k_call_share(int ncalls, int nfo, const CallFO* __restrict__ cfo
   if (c >= ncalls) return;
   const CallFO f0 = cfo[(size_t)c * nfo];
   bool same = true;
-  int lmx = -1;
+  int lmx = -1, ksum = 0;
   for (int k = lane; k < nfo; k += 32) {
     const CallFO f = cfo[(size_t)c * nfo + k];
     same = same && f.cg[0] == f0.cg[0] && f.cg[1] == f0.cg[1] && f.cg[2] == f0.cg[2] && f.rcut2 == f0.rcut2 &&
            f.npot == f0.npot;
-    if (f.npot == 2 && f.keep != 0ull) lmx = max(lmx, f.lmax);
+    if (f.npot == 2 && f.keep != 0ull) {
+      lmx = max(lmx, f.lmax);
+      ksum += __popcll(f.keep);
+    }
   }
   same = __all_sync(0xffffffffu, same);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) lmx = max(lmx, __shfl_xor_sync(0xffffffffu, lmx, o));
+  for (int o = 16; o > 0; o >>= 1) {
+    lmx = max(lmx, __shfl_xor_sync(0xffffffffu, lmx, o));
+    ksum += __shfl_xor_sync(0xffffffffu, ksum, o);
+  }
   if (lane == 0) {
     CallShare s;
     s.cg[0] = f0.cg[0];
@@ -731,7 +790,7 @@ __global__ void k_call_share(int ncalls, int nfo, const CallFO* __restrict__ cfo
     s.npot = f0.npot;
     s.kf = (lmx < 0) ? 0 : (((lmx + 1) * (lmx + 1) + 3) / 4) * 4;
     s.shared = same ? 1 : 0;
-    s.pad = 0;
+    s.ksum = ksum;
     out[c] = s;
   }
 }
@@ -782,12 +841,20 @@ static void set_shared_attr() {
                        (int)sizeof(SharedSmem<WM>));
 }
 
+template <int WM>
+static void set_perfo_attr() {
+  cudaFuncSetAttribute(k_coulomb_perfo<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PerFOSmem<WM>));
+}
+
 // Per-device set-up: the dynamic shared-memory opt-ins.
 void init_coulomb_mma() {
-  cudaFuncSetAttribute(k_coulomb_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MmaSmem));
   set_shared_attr<1>();
   set_shared_attr<2>();
   set_shared_attr<4>();
+  set_perfo_attr<1>();
+  set_perfo_attr<2>();
+  set_perfo_attr<4>();
 }
 
 template <int WM>
@@ -798,6 +865,17 @@ static void launch_shared(int ncalls, const int* lists, const CallShare* share, 
   dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
   k_coulomb_shared<WM><<<grid, MMA_THREADS, sizeof(SharedSmem<WM>), st>>>(
       ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M, boys_tab, vh, ldv, cnt);
+}
+
+template <int WM>
+static void launch_perfo(int ncalls, const int* lists, int acc, const CallInfo* calls, const PairGeo* pairs, int nfo,
+                         const double* coef, const int8_t* pair_fmt, const CallFO* cfo, const double* momv,
+                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, unsigned long long* cnt,
+                         cudaStream_t st) {
+  dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
+  k_coulomb_perfo<WM><<<grid, MMA_THREADS, sizeof(PerFOSmem<WM>), st>>>(ncalls, lists, acc, calls, pairs, nfo, coef,
+                                                                         pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
+                                                                         cnt);
 }
 
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
@@ -818,10 +896,16 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
       launch_shared<1>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
                        ldv, cnt, st);
   }
-  dim3 grid(M.ntiles, (nfo + MMA_FOS - 1) / MMA_FOS);
-  k_coulomb_mma<<<grid, MMA_THREADS, sizeof(MmaSmem), st>>>(ncalls, scr.lists, per_fo_only ? 0 : 1, calls, pairs,
-                                                             nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh,
-                                                             ldv, cnt);
+  const int acc = per_fo_only ? 0 : 1;
+  if (nfo > 64)
+    launch_perfo<4>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
+                    cnt, st);
+  else if (nfo > 32)
+    launch_perfo<2>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
+                    cnt, st);
+  else
+    launch_perfo<1>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
+                    cnt, st);
 }
 
 }  // namespace flosic

@@ -58,7 +58,8 @@ void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, 
 // identical for every FO go through the shared-geometry kernel, the rest
 // through the per-FO kernel, which adds its part.  per_fo_only routes every
 // call through the per-FO kernel (a cross-check of the two forms).
-// cnt[0] += near (pair, point, FO) evaluations, cnt[1] += far (call, point, FO).
+// cnt[0] += near (pair, point, FO) evaluations, cnt[1] += far (call, point, FO),
+// cnt[2] += multipole terms kept by the skip rule over those far evaluations.
 struct CoulombScratch {
   int8_t* pair_fmt;    // npairs
   CallShare* share;    // ncalls

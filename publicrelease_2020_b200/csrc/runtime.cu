@@ -355,7 +355,7 @@ struct flosic_ctx {
   DevBuf<int> d_lists;
   bool per_fo_coulomb = false;   // FLOSIC_COULOMB=perfo: every call through the per-FO kernel (A/B checks)
   DevBuf<unsigned long long> d_cnt;
-  unsigned long long work_near = 0, work_far = 0;
+  unsigned long long work_near = 0, work_far = 0, work_terms = 0;
   DevBuf<CallFO> d_callfo;
   // stats
   long long launches = 0;
@@ -729,17 +729,18 @@ void coulomb(flosic_ctx* c, int s) {
   c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
   c->d_share.ensure((size_t)std::max(ncalls, 1));
   c->d_lists.ensure((size_t)2 * ncalls + 2);
-  c->d_cnt.ensure(2);
-  CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 2 * sizeof(unsigned long long), st));
+  c->d_cnt.ensure(3);
+  CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 3 * sizeof(unsigned long long), st));
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
                      c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, scr, c->d_cnt.p, st);
   c->launches += c->per_fo_coulomb ? 4 : 5;
-  unsigned long long cnt[2];
+  unsigned long long cnt[3];
   CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
   c->work_near += cnt[0];
   c->work_far += cnt[1];
+  c->work_terms += cnt[2];
   CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1398,7 +1399,7 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
     for (int s = 0; s < c->nspn; ++s)
       if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
     c->launches = 0;
-    c->work_near = c->work_far = 0;
+    c->work_near = c->work_far = c->work_terms = 0;
     for (double& m : c->stage_ms) m = 0.0;
     invalidate(c);
     double zsic = 0.0;
@@ -1427,6 +1428,7 @@ int flosic_sic_stats(flosic_ctx* c, int64_t* launches, double* stage_ms, int64_t
   if (work) {
     work[0] = (int64_t)c->work_near;
     work[1] = (int64_t)c->work_far;
+    work[2] = (int64_t)c->work_terms;
   }
   if (launches) *launches = c->launches;
   if (stage_ms)

@@ -196,10 +196,10 @@ class FlosicSIC:
         ms = np.zeros(7)
         npairs = np.zeros(1, dtype=np.int64)
         ncalls = np.zeros(1, dtype=np.int64)
-        work = np.zeros(2, dtype=np.int64)
+        work = np.zeros(3, dtype=np.int64)
         self._check(self.L.flosic_sic_stats(self.h, la, ms, npairs, ncalls, work))
         return dict(launches=int(la[0]), stage_ms=ms, npairs=int(npairs[0]), ncalls=int(ncalls[0]),
-                    near_evals=int(work[0]), far_evals=int(work[1]))
+                    near_evals=int(work[0]), far_evals=int(work[1]), far_terms=int(work[2]))
 
 
 def open_system(sysm, device=0):

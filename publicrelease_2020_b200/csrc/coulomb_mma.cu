@@ -18,13 +18,17 @@
 //                     both are segments of ONE GEMM  V[k][p] += A[k][:] B[:][p]
 //                     over all such calls, on the FP64 tensor cores
 //                     (mma.sync m8n8k4 .f64).  A CTA owns 128 points and up to
-//                     128 FOs; segments are double buffered (A by cp.async, B by
-//                     the first four warps while the others multiply).
+//                     128 FOs.
 //   k_coulomb_perfo   the remaining calls, whose CG (charge weighted,
 //                     poisson1.f:503-520) differs per FO: the near field of the
 //                     FOs with near points in the tile as a GEMM over compacted
 //                     FO slots, added per (FO, point); the far field per
 //                     (FO, point).
+//
+// Both near-field GEMMs run warp specialised: producer warps build the G / H
+// columns and copy the A rows (cp.async) into double-buffered shared memory,
+// packing consecutive segments into stages of up to 52 rows, while consumer
+// warps keep the accumulators and issue only the tensor-core MMAs.
 //
 // Both walk their calls in order, so every per-point sum is deterministic.
 // Both count the evaluations they perform: near (pair, point, FO), far
@@ -37,7 +41,6 @@
 
 namespace flosic {
 
-constexpr int MMA_THREADS = 256;            // 8 warps
 constexpr int G_LD = TILE + 4;              // 132 (= 4 mod 16 doubles): conflict-free B fragment loads
 constexpr int KSEG = 52;                    // rows of one B segment (46 coefficients or 49 moments, padded)
 static_assert(COEF_LD == KSEG && MOM_LD == KSEG, "segment rows and global row strides must agree");
@@ -264,13 +267,145 @@ __device__ __forceinline__ void count_add(unsigned long long* cnt, unsigned long
 }
 
 // ---------------------------------------------------------------------------
+// Warp-specialised pipeline
+// ---------------------------------------------------------------------------
+// Eight consumer warps hold the accumulators and only multiply; four producer
+// warps build the B columns (one point per thread), issue the cp.async copies
+// of the A rows and pack consecutive segments into stages of at most KSEG rows.
+// Stages are double buffered; buffer b is handed over through named barriers
+// FULL+b (producers arrive, consumers wait) and EMPTY+b (consumers arrive,
+// producers wait before refilling).  Every stage, including a final marker
+// stage of -1 rows that ends the consumers' loop, is waited on exactly once on
+// each side, so every barrier phase collects all WS_THREADS arrivals.
+constexpr int CONS_WARPS = 8;
+constexpr int PROD_WARPS = 4;
+constexpr int NCONS = 32 * CONS_WARPS;
+constexpr int NPROD = 32 * PROD_WARPS;
+constexpr int WS_THREADS = NCONS + NPROD;   // 384
+constexpr int PTS_PER_PROD = TILE / NPROD;  // 1
+constexpr int BAR_FULL = 1, BAR_EMPTY = 3;  // named barrier ids 1,2 and 3,4 (0 is __syncthreads)
+
+__device__ __forceinline__ void named_sync(int id) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(WS_THREADS) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id) {
+  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(WS_THREADS) : "memory");
+}
+
+// Producer side of the stage hand-over.
+struct StagePacker {
+  int qi = 0;        // stages handed over so far
+  int rows = 0;      // rows of the open stage
+  int b = 0;         // its buffer
+  bool open = false;
+  __device__ void begin() {
+    b = qi & 1;
+    if (qi >= 2) named_sync(BAR_EMPTY + b);
+    rows = 0;
+    open = true;
+  }
+  __device__ void finish(int* stage_rows, int r, bool leader) {
+    cp_async_wait_all();
+    if (leader) stage_rows[b] = r;
+    named_arrive(BAR_FULL + b);
+    ++qi;
+    open = false;
+  }
+  // Offset of a segment of r rows, closing the open stage when it is full.
+  __device__ int place(int* stage_rows, int r, bool leader) {
+    if (open && rows + r > KSEG) finish(stage_rows, rows, leader);
+    if (!open) begin();
+    const int off = rows;
+    rows += r;
+    return off;
+  }
+  // Close the last stage, hand over the end marker, and wait until the
+  // consumers have released the last two stages.
+  __device__ void end(int* stage_rows, bool leader) {
+    if (open) finish(stage_rows, rows, leader);
+    begin();
+    finish(stage_rows, -1, leader);
+    for (int j = max(qi - 2, 0); j < qi; ++j) named_sync(BAR_EMPTY + (j & 1));
+  }
+};
+
+// Copy the first `rows` doubles of nrow rows (global row i at src_row(i), shared
+// row dst_row(i) with stride KSEG, column offset off) with 16-byte cp.async,
+// work split over the producer threads.
+template <typename SrcRow, typename DstRow>
+__device__ __forceinline__ void copy_rows(double* dst, int off, int nrow, int rows, int pt, SrcRow src_row,
+                                          DstRow dst_row) {
+  const int cpr = rows >> 1;  // 16-byte chunks per row
+  if (cpr == 0) return;
+  int r = pt / cpr, ch = pt - r * cpr;
+  const int dr = NPROD / cpr, dc = NPROD - dr * cpr;
+  for (int e = pt; e < nrow * cpr; e += NPROD) {
+    cp_async16(dst + (size_t)dst_row(r) * KSEG + off + 2 * ch, src_row(r) + 2 * ch);
+    r += dr;
+    ch += dc;
+    if (ch >= cpr) {
+      ch -= cpr;
+      ++r;
+    }
+  }
+}
+
+// Consumer MMA over one stage: V[k][p] += A[k][0:rows] B[0:rows][p] for the
+// warp's 32 x WPTS tile; m-tiles with mt_active false are skipped.
+template <int NT>
+__device__ __forceinline__ void stage_mma(double (&V)[4][NT][2], const double* __restrict__ As,
+                                          const double* __restrict__ Bs, int rows, const bool (&mt_active)[4]) {
+  for (int kk = 0; kk < rows; kk += 4) {
+    double af[4];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) af[mt] = As[mt * 8 * KSEG + kk];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const double bf = Bs[(size_t)kk * G_LD + nt * 8];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+        if (mt_active[mt]) dmma884(V[mt][nt][0], V[mt][nt][1], af[mt], bf);
+    }
+  }
+}
+
+// Degree whose harmonics fill kf moment rows ((l+1)^2 rounded up to 4).
+__device__ __forceinline__ int far_degree(int kf) {
+  return kf <= 4 ? 1 : (kf <= 12 ? 2 : (kf <= 16 ? 3 : (kf <= 28 ? 4 : (kf <= 36 ? 5 : 6))));
+}
+
+// H column (rows [0, kf)) of one far point: harmonics times 1/r^(l+1), zero padded.
+__device__ __forceinline__ void write_h(double* g, int kf, double dx, double dy, double dz, double r2) {
+  const double hn = 1.0 / sqrt(r2);
+  const int lmx = far_degree(kf);
+  double rec[LM + 1];
+  rec[0] = hn;
+#pragma unroll
+  for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
+  harmonics_mmajor(hn * dx, hn * dy, hn * dz, lmx,
+                   [&](int row, int l, double v) { g[(size_t)row * G_LD] = v * rec[l]; });
+  for (int t = (lmx + 1) * (lmx + 1); t < kf; ++t) g[(size_t)t * G_LD] = 0.0;
+}
+
+// G column of one near point of pair pg (rows [0, kn)).
+__device__ __forceinline__ void write_g_point(double* g, int kn, const PairGeo& pg, double x, double y, double z,
+                                              const double* __restrict__ boys_tab) {
+  const double rx = x - pg.C[0], ry = y - pg.C[1], rz = z - pg.C[2];
+  const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
+  double F[5];
+  boys_fmt(boys_tab, xx, exp(-xx), kn >= 48 ? 5 : (kn == 32 ? 4 : 3), F);
+  write_g(g, kn, rx, ry, rz, F);
+}
+
+// ---------------------------------------------------------------------------
 // Shared-geometry calls
 // ---------------------------------------------------------------------------
 template <int WM>
 struct SharedSmem {
-  double A[2][32 * WM * KSEG];  // FO rows of the segment's coefficients / moments
+  double A[2][32 * WM * KSEG];  // FO rows of the stage's coefficients / moments
   double B[2][KSEG * G_LD];     // G or H columns
   double px[TILE], py[TILE], pz[TILE];
+  int rows[2];                  // rows of the stage in each buffer, -1 = end
 };
 
 // One segment of the shared GEMM: the near part of one pair or the far part of
@@ -286,8 +421,7 @@ struct Segment {
 
 // Walks the shared calls of the list in order and yields their segments for a
 // tile: near segments for each pair unless the tile is entirely far, then the
-// far segment unless the tile is entirely near or NPOT=1.  Every thread runs
-// it identically.
+// far segment unless the tile is entirely near or NPOT=1.
 struct SegmentWalker {
   const int* list;
   int n;
@@ -298,9 +432,8 @@ struct SegmentWalker {
   int li, sub;
   int c, p0, np, cls, kf, npot, ksum;
   double cx, cy, cz, rc2;
-  unsigned long long direct_far;  // far points of all-far tiles of calls without kept moments
 
-  __device__ bool next(Segment& s, int npts) {
+  __device__ bool next(Segment& s) {
     while (li < n) {
       if (sub < 0) {
         c = list[li];
@@ -328,11 +461,8 @@ struct SegmentWalker {
       sub = -1;
       ++li;
       if (want_far) {
-        if (kf > 0 || cls == 2) {
-          s = Segment{1, c, kf, cls, ksum, cx, cy, cz, rc2};
-          return true;
-        }
-        direct_far += (unsigned long long)npts;
+        s = Segment{1, c, kf, cls, ksum, cx, cy, cz, rc2};
+        return true;
       }
     }
     return false;
@@ -340,156 +470,133 @@ struct SegmentWalker {
 };
 
 template <int WM>
-__global__ void __launch_bounds__(MMA_THREADS, 1)
+__global__ void __launch_bounds__(WS_THREADS, 1)
 k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __restrict__ share,
                  const CallInfo* __restrict__ calls, int nfo, const double* __restrict__ coef,
                  const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
                  const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
                  double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
-  constexpr int FOB = 32 * WM, WN = 8 / WM, WPTS = TILE / WN, NT = WPTS / 8;
+  constexpr int FOB = 32 * WM, WN = CONS_WARPS / WM, WPTS = TILE / WN, NT = WPTS / 8;
   extern __shared__ __align__(128) unsigned char smraw[];
   SharedSmem<WM>& S = *reinterpret_cast<SharedSmem<WM>*>(smraw);
   const int tile = blockIdx.x;
   const int k0 = blockIdx.y * FOB;
   const int nk = min(FOB, nfo - k0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp % WM, wn = warp / WM;
   const int p0 = tile * TILE;
   const int np = min(TILE, M.n - p0);
-  for (int i = tid; i < TILE; i += MMA_THREADS) {
+  for (int i = tid; i < TILE; i += WS_THREADS) {
     const bool a = i < np;
     S.px[i] = a ? M.x[p0 + i] : 0.0;
     S.py[i] = a ? M.y[p0 + i] : 0.0;
     S.pz[i] = a ? M.z[p0 + i] : 0.0;
   }
-  SegmentWalker W;
-  W.list = lists;
-  W.n = lists[2 * ncalls];
-  W.share = share;
-  W.calls = calls;
-  W.pair_fmt = pair_fmt;
-  for (int d = 0; d < 3; ++d) {
-    W.lo[d] = M.tile_lo[3 * tile + d];
-    W.hi[d] = M.tile_hi[3 * tile + d];
-  }
-  W.li = 0;
-  W.sub = -1;
-  W.c = W.p0 = W.np = W.cls = W.kf = W.ksum = 0;
-  W.npot = 1;
-  W.cx = W.cy = W.cz = W.rc2 = 0.0;
-  W.direct_far = 0ull;
   __syncthreads();
-
-  double V[4][NT][2];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < NT; ++b) V[a][b][0] = V[a][b][1] = 0.0;
   unsigned long long my_near = 0, my_far = 0, my_terms = 0;
-  const bool count_terms = blockIdx.y == 0;  // kept terms are summed over all FOs once per (call, point)
 
-  // Stage segment s into buffer b: A rows by cp.async (all threads), B columns
-  // by threads 0..127 (one point each).
-  auto stage = [&](const Segment& s, int b) {
-    if (s.rows > 0) {
+  if (warp >= CONS_WARPS) {
+    // ---- producers
+    const int pt = tid - NCONS;
+    const bool leader = pt == 0;
+    const bool count_terms = blockIdx.y == 0;  // kept terms are summed over all FOs once per (call, point)
+    SegmentWalker W;
+    W.list = lists;
+    W.n = lists[2 * ncalls];
+    W.share = share;
+    W.calls = calls;
+    W.pair_fmt = pair_fmt;
+    for (int d = 0; d < 3; ++d) {
+      W.lo[d] = M.tile_lo[3 * tile + d];
+      W.hi[d] = M.tile_hi[3 * tile + d];
+    }
+    W.li = 0;
+    W.sub = -1;
+    W.c = W.p0 = W.np = W.cls = W.kf = W.ksum = 0;
+    W.npot = 1;
+    W.cx = W.cy = W.cz = W.rc2 = 0.0;
+    StagePacker P;
+    Segment s;
+    while (W.next(s)) {
+      if (s.rows == 0) {
+        // far segment of a call whose FOs keep no multipole term: count only
+        for (int j = 0; j < PTS_PER_PROD; ++j) {
+          const int p = pt + j * NPROD;
+          if (p < np && (s.cls == 1 || sqdist_rn2(S.px[p], S.py[p], S.pz[p], s.cx, s.cy, s.cz) > s.rc2)) ++my_far;
+        }
+        continue;
+      }
+      const int off = P.place(S.rows, s.rows, leader);
+      const int b = P.b;
       const double* src = s.far ? momv + ((size_t)s.idx * nfo + k0) * MOM_LD
                                 : coef + ((size_t)s.idx * nfo + k0) * COEF_LD;
-      const int nchunk = nk * (KSEG / 2);
-      double* dst = S.A[b];
-      for (int i = tid; i < nchunk; i += MMA_THREADS) cp_async16(dst + 2 * i, src + 2 * i);
-    }
-    cp_async_commit();
-    if (tid < TILE) {
-      const int p = tid;
-      double* g = &S.B[b][p];
-      const double x = S.px[p], y = S.py[p], z = S.pz[p];
-      if (!s.far) {
-        bool nr = p < np;
-        if (nr && s.cls == 2) nr = !(sqdist_rn2(x, y, z, s.cx, s.cy, s.cz) > s.rc2);
-        if (nr) {
-          ++my_near;
-          const PairGeo& pg = pairs[s.idx];
-          const double rx = x - pg.C[0], ry = y - pg.C[1], rz = z - pg.C[2];
-          const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
-          double F[5];
-          boys_fmt(boys_tab, xx, exp(-xx), s.rows >= 48 ? 5 : (s.rows == 32 ? 4 : 3), F);
-          write_g(g, s.rows, rx, ry, rz, F);
-        } else {
-          zero_rows(g, s.rows);
-        }
-      } else {
-        double r2 = 0.0;
-        bool fr = p < np;
-        if (fr) {
-          r2 = sqdist_rn2(x, y, z, s.cx, s.cy, s.cz);
-          if (s.cls == 2) fr = r2 > s.rc2;
-        }
-        if (fr) {
-          ++my_far;
-          if (count_terms) my_terms += (unsigned long long)s.ksum;
-          if (s.rows > 0) {
-            const double hn = 1.0 / sqrt(r2);
-            const int kr = s.rows;
-            double rec[LM + 1];
-            rec[0] = hn;
-#pragma unroll
-            for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
-            harmonics_mmajor(hn * (x - s.cx), hn * (y - s.cy), hn * (z - s.cz), LM, [&](int row, int l, double v) {
-              if (row < kr) g[(size_t)row * G_LD] = v * rec[l];
-            });
-            for (int t = NMOM; t < kr; ++t) g[(size_t)t * G_LD] = 0.0;
+      copy_rows(S.A[b], off, nk, s.rows, pt, [&](int r) { return src + (size_t)r * KSEG; },
+                [](int r) { return r; });
+      cp_async_commit();
+      for (int j = 0; j < PTS_PER_PROD; ++j) {
+        const int p = pt + j * NPROD;
+        double* g = &S.B[b][(size_t)off * G_LD + p];
+        const double x = S.px[p], y = S.py[p], z = S.pz[p];
+        if (!s.far) {
+          bool nr = p < np;
+          if (nr && s.cls == 2) nr = !(sqdist_rn2(x, y, z, s.cx, s.cy, s.cz) > s.rc2);
+          if (nr) {
+            ++my_near;
+            write_g_point(g, s.rows, pairs[s.idx], x, y, z, boys_tab);
+          } else {
+            zero_rows(g, s.rows);
           }
         } else {
-          zero_rows(g, s.rows);
+          double r2 = 0.0;
+          bool fr = p < np;
+          if (fr) {
+            r2 = sqdist_rn2(x, y, z, s.cx, s.cy, s.cz);
+            if (s.cls == 2) fr = r2 > s.rc2;
+          }
+          if (fr) {
+            ++my_far;
+            if (count_terms) my_terms += (unsigned long long)s.ksum;
+            write_h(g, s.rows, x - s.cx, y - s.cy, z - s.cz, r2);
+          } else {
+            zero_rows(g, s.rows);
+          }
         }
       }
     }
-  };
-
-  Segment cur, nxt;
-  bool have = W.next(cur, np);
-  if (have) stage(cur, 0);
-  cp_async_wait_all();
-  __syncthreads();
-  int buf = 0;
-  while (have) {
-    const bool more = W.next(nxt, np);
-    if (more) stage(nxt, buf ^ 1);
-    if (wm * 32 < nk && cur.rows > 0) {
-      const double* As = &S.A[buf][(wm * 32 + (lane >> 2)) * KSEG + (lane & 3)];
-      const double* Bs = &S.B[buf][(lane & 3) * G_LD + wn * WPTS + (lane >> 2)];
-      for (int kk = 0; kk < cur.rows; kk += 4) {
-        double af[4], bf[NT];
+    P.end(S.rows, leader);
+  } else {
+    // ---- consumers
+    const int wn = warp % WN, wm = warp / WN;
+    double V[4][NT][2];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) af[mt] = As[mt * 8 * KSEG + kk];
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(size_t)kk * G_LD + nt * 8];
+      for (int b = 0; b < NT; ++b) V[a][b][0] = V[a][b][1] = 0.0;
+    bool mt_active[4];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < NT; ++nt) dmma884(V[mt][nt][0], V[mt][nt][1], af[mt], bf[nt]);
-      }
+    for (int mt = 0; mt < 4; ++mt) mt_active[mt] = wm * 32 + mt * 8 < nk;
+    for (int qi = 0;; ++qi) {
+      const int b = qi & 1;
+      named_sync(BAR_FULL + b);
+      const int r = S.rows[b];
+      if (r > 0)
+        stage_mma(V, &S.A[b][(wm * 32 + (lane >> 2)) * KSEG + (lane & 3)],
+                  &S.B[b][(lane & 3) * G_LD + wn * WPTS + (lane >> 2)], r, mt_active);
+      named_arrive(BAR_EMPTY + b);
+      if (r < 0) break;
     }
-    cp_async_wait_all();
-    __syncthreads();
-    have = more;
-    cur = nxt;
-    buf ^= 1;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      const int k = wm * 32 + mt * 8 + (lane >> 2);
+      if (k >= nk) continue;
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int p = wn * WPTS + nt * 8 + 2 * (lane & 3) + i;
+          if (p < np) vh[(size_t)(k0 + k) * ldv + p0 + p] = V[mt][nt][i];
+        }
+    }
   }
-
-#pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int k = wm * 32 + mt * 8 + (lane >> 2);
-    if (k >= nk) continue;
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int p = wn * WPTS + nt * 8 + 2 * (lane & 3) + i;
-        if (p < np) vh[(size_t)(k0 + k) * ldv + p0 + p] = V[mt][nt][i];
-      }
-  }
-  if (tid == 0) my_far += W.direct_far;
   count_add(cnt, my_near * (unsigned long long)nk, my_far * (unsigned long long)nk, my_terms);
 }
 
@@ -497,17 +604,20 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
 // Per-FO-geometry calls
 // ---------------------------------------------------------------------------
 // A CTA owns 128 points and up to 32*WM FOs and walks the per-FO calls in
-// order.  For each call it classifies the tile against every FO's sphere,
-// compacts the FOs with near points into slots, and contracts the G columns
-// of one pair per stage (double buffered) with the slots' coefficient rows
-// only, so the tensor work follows the FOs that are near rather than the
-// whole FO block.  The per-call result is added, masked per (FO, point), to
-// the CTA's own slice of vh (L2 resident); the far field of the call follows,
-// one FO per warp at a time with lanes over points.
+// order.  For each call it classifies the tile against every FO's sphere and
+// compacts the FOs with near points into slots; the producers stream the G
+// columns of the call's pairs and the slots' coefficient rows, the consumers
+// contract them on the active slot m-tiles only (up to 32*WC slots per pass),
+// so the tensor work follows the FOs that are near rather than the whole FO
+// block.  The call's near field is added, masked per (FO, point), to the CTA's
+// own slice of vh (L2 resident); its far field follows, one FO per warp with
+// lanes over points.
 template <int WM>
 struct PerFOSmem {
-  double A[2][32 * WM * KSEG];  // slot rows of the stage's coefficients; far phase: the FOs' moments (A[0])
-  double B[2][KSEG * G_LD];     // G columns of the stage's pair
+  static constexpr int WC = WM < 2 ? WM : 2;  // consumer warp rows: slot capacity 32*WC per pass
+  double A[2][32 * WC * KSEG];  // slot rows of the stage's coefficients
+  double B[2][KSEG * G_LD];     // G columns
+  double MV[32 * WM * MOM_LD];  // far phase: the FOs' moments
   double px[TILE], py[TILE], pz[TILE];
   double cg[32 * WM][3];
   double rc2[32 * WM];
@@ -516,17 +626,19 @@ struct PerFOSmem {
   int lmax[32 * WM];
   int nkeep[32 * WM];
   int fo_of[32 * WM];           // slot -> FO (block-local)
+  double lo[3], hi[3];          // tile bounding box
   unsigned bal[WM];             // per warp of the status phase: FOs with near points
   unsigned balf[WM];            // per warp of the status phase: FOs with far points
   int na;
+  int rows[2];
 };
 
-// Physical A row of slot s: slots fill m-tiles round robin over the WM warp
-// rows, so that a few active FOs keep several warps busy.
-template <int WM>
+// Physical A row of pass-local slot s: slots fill m-tiles round robin over the
+// WC warp rows, so that a few active FOs keep several warps busy.
+template <int WC>
 __device__ __forceinline__ int slot_row(int s) {
   const int g = s >> 3;
-  return (g % WM) * 32 + (g / WM) * 8 + (s & 7);
+  return (g % WC) * 32 + (g / WC) * 8 + (s & 7);
 }
 
 // Far-field potential of one FO at one point, sum_lm MV[lm] Y_lm(u) / r^(l+1),
@@ -547,13 +659,14 @@ __device__ __forceinline__ double multipole(const double* __restrict__ mv, int l
 }
 
 template <int WM>
-__global__ void __launch_bounds__(MMA_THREADS, 1)
+__global__ void __launch_bounds__(WS_THREADS, 1)
 k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
                 const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
                 const int8_t* __restrict__ pair_fmt, const CallFO* __restrict__ cfo,
                 const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
                 double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
-  constexpr int FOB = 32 * WM, WN = 8 / WM, WPTS = TILE / WN, NT = WPTS / 8;
+  constexpr int FOB = 32 * WM, WC = PerFOSmem<WM>::WC, SC = 32 * WC;
+  constexpr int WN = CONS_WARPS / WC, WPTS = TILE / WN, NT = WPTS / 8;
   const int* list = lists + ncalls;
   const int nl = lists[2 * ncalls + 1];
   if (accumulate && nl == 0) return;
@@ -563,24 +676,22 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
   const int k0 = blockIdx.y * FOB;
   const int nk = min(FOB, nfo - k0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp % WM, wn = warp / WM;
   const int p0 = tile * TILE;
   const int np = min(TILE, M.n - p0);
-  for (int i = tid; i < TILE; i += MMA_THREADS) {
+  for (int i = tid; i < TILE; i += WS_THREADS) {
     const bool a = i < np;
     S.px[i] = a ? M.x[p0 + i] : 0.0;
     S.py[i] = a ? M.y[p0 + i] : 0.0;
     S.pz[i] = a ? M.z[p0 + i] : 0.0;
   }
   if (!accumulate)
-    for (int e = tid; e < nk * TILE; e += MMA_THREADS) {
+    for (int e = tid; e < nk * TILE; e += WS_THREADS) {
       const int k = e / TILE, p = e - k * TILE;
       if (p < np) vh[(size_t)(k0 + k) * ldv + p0 + p] = 0.0;
     }
-  double lo[3], hi[3];
-  for (int d = 0; d < 3; ++d) {
-    lo[d] = M.tile_lo[3 * tile + d];
-    hi[d] = M.tile_hi[3 * tile + d];
+  if (tid < 3) {
+    S.lo[tid] = M.tile_lo[3 * tile + tid];
+    S.hi[tid] = M.tile_hi[3 * tile + tid];
   }
   unsigned long long my_near = 0, my_far = 0, my_terms = 0;
 
@@ -599,7 +710,7 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
         cgz = f.cg[2];
         rc2 = f.rcut2;
         npot = f.npot;
-        st = (npot == 1) ? 0 : tile_class(lo, hi, cgx, cgy, cgz, rc2);
+        st = (npot == 1) ? 0 : tile_class(S.lo, S.hi, cgx, cgy, cgz, rc2);
         if (st != 0 && npot == 2) {
           lmx = f.lmax;
           nkeep = __popcll(f.keep);
@@ -613,8 +724,7 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
       S.rc2[tid] = rc2;
       S.lmax[tid] = lmx;
       S.nkeep[tid] = nkeep;
-      const bool act = tid < nk && st != 1;
-      const unsigned b = __ballot_sync(0xffffffffu, act);
+      const unsigned b = __ballot_sync(0xffffffffu, tid < nk && st != 1);
       const unsigned bf = __ballot_sync(0xffffffffu, tid < nk && st != 0 && npot == 2);
       if (lane == 0) {
         S.bal[warp] = b;
@@ -635,99 +745,90 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
 #pragma unroll
     for (int w = 0; w < WM; ++w) anyfar = anyfar || S.balf[w] != 0u;
 
-    if (na > 0) {
-      double T[4][NT][2];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < NT; ++b) T[a][b][0] = T[a][b][1] = 0.0;
-      auto stage = [&](int q, int b) {
-        const double* src = coef + (size_t)q * nfo * COEF_LD;
-        double* dst = S.A[b];
-        for (int e = tid; e < na * (KSEG / 2); e += MMA_THREADS) {
-          const int s = e / (KSEG / 2), ch = e - s * (KSEG / 2);
-          cp_async16(dst + slot_row<WM>(s) * KSEG + 2 * ch, src + (size_t)(k0 + S.fo_of[s]) * COEF_LD + 2 * ch);
-        }
-        cp_async_commit();
-        if (tid < TILE) {
-          const int p = tid;
-          double* g = &S.B[b][p];
-          const int kn = near_rows(pair_fmt[q]);
-          if (p < np) {
-            const PairGeo& pg = pairs[q];
-            const double rx = S.px[p] - pg.C[0], ry = S.py[p] - pg.C[1], rz = S.pz[p] - pg.C[2];
-            const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
-            double F[5];
-            boys_fmt(boys_tab, xx, exp(-xx), kn >= 48 ? 5 : (kn == 32 ? 4 : 3), F);
-            write_g(g, kn, rx, ry, rz, F);
-          } else {
-            zero_rows(g, kn);
+    for (int c0 = 0; c0 < na; c0 += SC) {
+      const int nac = min(SC, na - c0);
+      const int* fo = S.fo_of + c0;
+      if (warp >= CONS_WARPS) {
+        // ---- producers: the call's pairs, packed into stages
+        const int pt = tid - NCONS;
+        const bool leader = pt == 0;
+        StagePacker P;
+        for (int qi = 0; qi < ci.np; ++qi) {
+          const int q = ci.p0 + qi;
+          const int kq = near_rows(pair_fmt[q]);
+          const int off = P.place(S.rows, kq, leader);
+          const int b = P.b;
+          const double* src = coef + ((size_t)q * nfo + k0) * COEF_LD;
+          copy_rows(S.A[b], off, nac, kq, pt, [&](int s) { return src + (size_t)fo[s] * COEF_LD; },
+                    [](int s) { return slot_row<WC>(s); });
+          cp_async_commit();
+          const PairGeo& pg = pairs[q];
+          for (int j = 0; j < PTS_PER_PROD; ++j) {
+            const int p = pt + j * NPROD;
+            double* g = &S.B[b][(size_t)off * G_LD + p];
+            if (p < np) write_g_point(g, kq, pg, S.px[p], S.py[p], S.pz[p], boys_tab);
+            else zero_rows(g, kq);
           }
         }
-      };
-      stage(ci.p0, 0);
-      cp_async_wait_all();
-      __syncthreads();
-      int buf = 0;
-      for (int qi = 0; qi < ci.np; ++qi) {
-        const int q = ci.p0 + qi;
-        if (qi + 1 < ci.np) stage(q + 1, buf ^ 1);
-        const int kq = near_rows(pair_fmt[q]);
-        const double* As = &S.A[buf][(wm * 32 + (lane >> 2)) * KSEG + (lane & 3)];
-        const double* Bs = &S.B[buf][(lane & 3) * G_LD + wn * WPTS + (lane >> 2)];
-        for (int kk = 0; kk < kq; kk += 4) {
-          double af[4], bf[NT];
+        P.end(S.rows, leader);
+      } else {
+        // ---- consumers
+        const int wn = warp % WN, wm = warp / WN;
+        double T[4][NT][2];
 #pragma unroll
-          for (int mt = 0; mt < 4; ++mt) af[mt] = As[mt * 8 * KSEG + kk];
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(size_t)kk * G_LD + nt * 8];
+          for (int b = 0; b < NT; ++b) T[a][b][0] = T[a][b][1] = 0.0;
+        bool mt_active[4];
 #pragma unroll
-          for (int mt = 0; mt < 4; ++mt) {
-            if ((mt * WM + wm) * 8 >= na) continue;
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) dmma884(T[mt][nt][0], T[mt][nt][1], af[mt], bf[nt]);
-          }
+        for (int mt = 0; mt < 4; ++mt) mt_active[mt] = (mt * WC + wm) * 8 < nac;
+        for (int qi = 0;; ++qi) {
+          const int b = qi & 1;
+          named_sync(BAR_FULL + b);
+          const int r = S.rows[b];
+          if (r > 0)
+            stage_mma(T, &S.A[b][(wm * 32 + (lane >> 2)) * KSEG + (lane & 3)],
+                      &S.B[b][(lane & 3) * G_LD + wn * WPTS + (lane >> 2)], r, mt_active);
+          named_arrive(BAR_EMPTY + b);
+          if (r < 0) break;
         }
-        cp_async_wait_all();
-        __syncthreads();
-        buf ^= 1;
-      }
-      // masked add of the call's near field to vh
+        // masked add of the call's near field to vh
 #pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const int s = (mt * WM + wm) * 8 + (lane >> 2);
-        if (s >= na) continue;
-        const int k = S.fo_of[s];
-        const int st = S.stat[k];
-        const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
-        double* vk = vh + (size_t)(k0 + k) * ldv + p0;
+        for (int mt = 0; mt < 4; ++mt) {
+          const int s = (mt * WC + wm) * 8 + (lane >> 2);
+          if (s >= nac) continue;
+          const int k = fo[s];
+          const int st = S.stat[k];
+          const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
+          double* vk = vh + (size_t)(k0 + k) * ldv + p0;
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
+          for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const int p = wn * WPTS + nt * 8 + 2 * (lane & 3) + i;
-            if (p >= np) continue;
-            bool nr = (st == 0);
-            if (st == 2) nr = !(sqdist_rn2(S.px[p], S.py[p], S.pz[p], cx, cy, cz) > rc2);
-            if (nr) {
-              vk[p] += T[mt][nt][i];
-              my_near += (unsigned long long)ci.np;
+            for (int i = 0; i < 2; ++i) {
+              const int p = wn * WPTS + nt * 8 + 2 * (lane & 3) + i;
+              if (p >= np) continue;
+              bool nr = (st == 0);
+              if (st == 2) nr = !(sqdist_rn2(S.px[p], S.py[p], S.pz[p], cx, cy, cz) > rc2);
+              if (nr) {
+                vk[p] += T[mt][nt][i];
+                my_near += (unsigned long long)ci.np;
+              }
             }
-          }
+        }
       }
     }
 
     if (anyfar) {
-      __syncthreads();  // near phase done with A
+      __syncthreads();  // the near phase is done with vh
       const double* mg = momv + ((size_t)c * nfo + k0) * MOM_LD;
-      for (int e = tid; e < nk * MOM_LD; e += MMA_THREADS) S.A[0][e] = mg[e];
+      for (int e = tid; e < nk * MOM_LD; e += WS_THREADS) S.MV[e] = mg[e];
       __syncthreads();
-      for (int k = warp; k < nk; k += MMA_THREADS / 32) {
+      for (int k = warp; k < nk; k += WS_THREADS / 32) {
         if (S.stat[k] == 0 || S.npot[k] == 1) continue;
         const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
         const int lmx = S.lmax[k];
         const unsigned long long nkeep = (unsigned long long)S.nkeep[k];
-        const double* mv = &S.A[0][k * MOM_LD];
+        const double* mv = &S.MV[k * MOM_LD];
         double* vk = vh + (size_t)(k0 + k) * ldv + p0;
         for (int p = lane; p < np; p += 32) {
           const double x = S.px[p], y = S.py[p], z = S.pz[p];
@@ -863,7 +964,7 @@ static void launch_shared(int ncalls, const int* lists, const CallShare* share, 
                           const MeshDev& M, const double* boys_tab, double* vh, int ldv, unsigned long long* cnt,
                           cudaStream_t st) {
   dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
-  k_coulomb_shared<WM><<<grid, MMA_THREADS, sizeof(SharedSmem<WM>), st>>>(
+  k_coulomb_shared<WM><<<grid, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(
       ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M, boys_tab, vh, ldv, cnt);
 }
 
@@ -873,7 +974,7 @@ static void launch_perfo(int ncalls, const int* lists, int acc, const CallInfo* 
                          const MeshDev& M, const double* boys_tab, double* vh, int ldv, unsigned long long* cnt,
                          cudaStream_t st) {
   dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
-  k_coulomb_perfo<WM><<<grid, MMA_THREADS, sizeof(PerFOSmem<WM>), st>>>(ncalls, lists, acc, calls, pairs, nfo, coef,
+  k_coulomb_perfo<WM><<<grid, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(ncalls, lists, acc, calls, pairs, nfo, coef,
                                                                          pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
                                                                          cnt);
 }

@@ -95,6 +95,21 @@ int flosic_sic_coupot_sic(flosic_ctx* ctx, int kxxs, int kxxo, double* coulomb, 
    (apotnl_sic.F:419): VXC(2*ndim) and ERGXL,ERGXN,ERGCL,ERGCN in ergs[4]. */
 int flosic_sic_getvlxc(flosic_ctx* ctx, int ndim, const double* rhog, double* vxc, double* ergs);
 
+/* Allocation-free form of flosic_sic_getvlxc on the caller's device buffers (no
+   counterpart in the reference).  d_rhog: RHOG(ldr,10) density channels in
+   device memory (channel stride ldr >= npts), d_wmsh: the npts mesh weights,
+   d_vxc: VXC(2*npts) written in device memory; ERGXL,ERGXN,ERGCL,ERGCN come
+   back in the host array ergs[4].  The functional is the context's (set by
+   flosic_sic_set_geometry); the call runs on the context's stream and
+   synchronises it before returning.  It allocates no device or host memory:
+   its block partial sums live in a file-scope device array sized for
+   npts <= 4,194,304 (larger npts returns FLOSIC_ERR_CAPACITY before any work).
+   The first call on a device looks up that array's address
+   (cudaGetSymbolAddress).  Calls that overlap in time on one device share the
+   array and race on it. */
+int flosic_sic_getvlxc_device(flosic_ctx* ctx, int npts, const double* d_rhog, int ldr, const double* d_wmsh,
+                              double* d_vxc, double* ergs);
+
 /* APOTNL_SIC(TOTQNUM,LSPX,IORBX) -- apotnl_sic.F:31: RESULTS(13) and CFRM(3) of
    FO iorbx, and its SIC potential POT(nmsh) = V_xc + V_H (the ZPOT record).
    The potential also stays in GPU memory for flosic_sic_siclagm. */

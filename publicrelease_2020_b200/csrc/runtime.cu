@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -961,6 +962,37 @@ void require(flosic_ctx* c, bool orb) {
   CUDA_CHECK(cudaSetDevice(c->device));
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free GETVLXC scratch
+// ---------------------------------------------------------------------------
+// flosic_sic_getvlxc_device keeps its per-block energy partial sums in this
+// file-scope device array instead of allocating: XC_SCRATCH_BLOCKS blocks of
+// 256 points (4,194,304 points at most) times NPART partials, then the NPART
+// final sums.  Every call overwrites the partials of its nblk blocks and the
+// sums before reading them, so no part of the array has to start at zero.  All
+// calls on one device share it: calls that overlap in time (other host threads,
+// other contexts or streams on the same device) race on it.
+constexpr int XC_SCRATCH_BLOCKS = 16384;
+constexpr int XC_SCRATCH_POINTS = XC_SCRATCH_BLOCKS * 256;
+static __device__ __align__(256) double g_xc_scratch[(XC_SCRATCH_BLOCKS + 1) * NPART];
+
+// Device address of g_xc_scratch for the current device, looked up once per
+// device by the first call (cudaGetSymbolAddress with that device current).
+double* xc_scratch_address(int device) {
+  static std::mutex mu;
+  static double* addr[64] = {};
+  if (device < 0 || device >= 64) fail(FLOSIC_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    double* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_xc_scratch);
+    if (e != cudaSuccess)
+      fail(FLOSIC_ERR_CUDA, std::string("cudaGetSymbolAddress(g_xc_scratch): ") + cudaGetErrorString(e));
+    addr[device] = ptr;
+  }
+  return addr[device];
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1334,6 +1366,33 @@ int flosic_sic_getvlxc(flosic_ctx* c, int ndim, const double* rhog, double* vxc,
       vxc[ndim + c->perm[i]] = v[P + i];
     }
     for (int j = 0; j < 4; ++j) ergs[j] = sums[4 + j];
+  });
+}
+
+int flosic_sic_getvlxc_device(flosic_ctx* c, int npts, const double* d_rhog, int ldr, const double* d_wmsh,
+                              double* d_vxc, double* ergs) {
+  return guarded([&] {
+    require(c, false);
+    if (npts < 1) fail(FLOSIC_ERR_ARG, "NPTS must be positive");
+    if (ldr < npts) fail(FLOSIC_ERR_ARG, "LDR smaller than NPTS");
+    if (!d_rhog || !d_wmsh || !d_vxc || !ergs) fail(FLOSIC_ERR_ARG, "null array argument");
+    if (npts > XC_SCRATCH_POINTS)
+      fail(FLOSIC_ERR_CAPACITY, "NPTS = " + std::to_string(npts) + " exceeds the " +
+                                    std::to_string(XC_SCRATCH_POINTS) +
+                                    "-point capacity of the allocation-free GETVLXC scratch");
+    double* part = xc_scratch_address(c->device);
+    double* sums = part + (size_t)XC_SCRATCH_BLOCKS * NPART;
+    const int nblk = (npts + 255) / 256;
+    MeshDev M{};
+    M.n = npts;
+    M.w = d_wmsh;
+    launch_xc_rhog(M, c->gga, c->xc, d_rhog, ldr, d_vxc, part, nblk, c->st);
+    launch_reduce_parts(1, nblk, part, sums, c->st);
+    CUDA_CHECK(cudaGetLastError());
+    double s[NPART];
+    CUDA_CHECK(cudaMemcpyAsync(s, sums, sizeof(s), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    for (int j = 0; j < 4; ++j) ergs[j] = s[4 + j];
   });
 }
 

@@ -33,7 +33,7 @@ EXPORTS = [
     "flosic_sic_create", "flosic_sic_destroy", "flosic_sic_last_error", "flosic_sic_set_geometry",
     "flosic_sic_set_orbitals", "flosic_sic_gorbdrv", "flosic_sic_frmorb2_fmat", "flosic_sic_frmiorb",
     "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
-    "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats",
+    "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
 ]
 
 _lib = None
@@ -64,6 +64,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_frmiorb.argtypes = [_vp, _dp, _dp, C.c_int]
     L.flosic_sic_coupot_sic.argtypes = [_vp, C.c_int, C.c_int, _dp, _dp]
     L.flosic_sic_getvlxc.argtypes = [_vp, C.c_int, _dp, _dp, _dp]
+    L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
     L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.flosic_sic_siclagm.argtypes = [_vp, C.c_int, _dp, C.c_int]
     L.flosic_sic_frmorb2_force.argtypes = [_vp, C.c_int, _dp, C.c_int, _dp]
@@ -159,6 +160,14 @@ class FlosicSIC:
         self._check(self.L.flosic_sic_getvlxc(self.h, n, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
                                               vxc, ergs))
         return vxc.reshape(2, n), ergs
+
+    def getvlxc_device(self, npts, d_rhog, ldr, d_wmsh, d_vxc):
+        """Allocation-free GETVLXC on device buffers given as raw device addresses
+        (e.g. torch CUDA tensors' data_ptr()); returns ERGXL, ERGXN, ERGCL, ERGCN."""
+        ergs = np.zeros(4)
+        self._check(self.L.flosic_sic_getvlxc_device(self.h, int(npts), C.c_void_p(int(d_rhog)), int(ldr),
+                                                     C.c_void_p(int(d_wmsh)), C.c_void_p(int(d_vxc)), ergs))
+        return ergs
 
     def apotnl_sic(self, lspx, iorbx):
         n = self.sysm.nmsh

@@ -31,6 +31,11 @@ sys.path.insert(0, ROOT)
 METRIC = "s per FLO-SIC SCF cycle (all FOs + FOD forces)"
 COULOMB_FLOPS_NEAR = 92.0    # per near (pair, point, FO): 46 polynomial coefficients x Boys-monomial terms
 COULOMB_FLOPS_TERM = 2.0     # per multipole term kept by the skip rule in a far (call, point, FO) evaluation
+# DRAM bytes of the two Coulomb kernels per tile of 128 points on the C2 shape:
+# ncu dram__bytes_read.sum + dram__bytes_write.sum on 296 tiles (k_coulomb_shared
+# 7.951 GB + 0.041 GB, k_coulomb_perfo 1.828 GB + 0.179 GB); the traffic is
+# re-reads of the per-call A operands, proportional to the tile count.
+COULOMB_DRAM_BYTES_PER_TILE = (7.951e9 + 0.041e9 + 1.828e9 + 0.179e9) / 296
 # (the Boys values, monomials and harmonics depend on geometry only and are
 # formed once per (pair or call, point); the per-FO work is the contraction)
 
@@ -256,6 +261,8 @@ def run_ours(args, rank, world, local_rank):
     flops = (st_acc["near"] * COULOMB_FLOPS_NEAR + st_acc["terms"] * COULOMB_FLOPS_TERM) / args.steps
     peak = fp64_peak_tflops(torch)
     achieved = flops / coul_s / 1e12 if coul_s > 0 else 0.0
+    ntiles = (cfg["nmsh"] + 127) // 128
+    traffic = COULOMB_DRAM_BYTES_PER_TILE * ntiles if args.workload in ("c2", "c2half", "c2tiny") else None
     cfg.update(parallelism=f"replicas x{world}" if world > 1 else "single GPU", l2="working set >> L2 (126 MB)",
                npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision="fp64")
     line = {
@@ -265,8 +272,10 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_ms / 1e3 / args.steps / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(st_acc["launches"]),
-        "roofline": {"bound": "tensor", "kernel": "k_coulomb_shared + k_coulomb_mma", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+        "roofline": {"bound": "tensor", "kernel": "k_coulomb_shared + k_coulomb_perfo", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                     "traffic": traffic, "traffic_note": "ncu DRAM bytes of both kernels on the 296-tile C2 "
+                                                         "shape, scaled by tile count",
                      "peak_kind": "FP64 cuBLAS DGEMM measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                      "work": f"{st_acc['near'] / args.steps:.4g} near (pair,point,FO) x {COULOMB_FLOPS_NEAR:.0f} + "
                              f"{st_acc['terms'] / args.steps:.4g} kept multipole terms x {COULOMB_FLOPS_TERM:.0f} flops "

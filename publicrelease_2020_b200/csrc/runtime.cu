@@ -8,6 +8,7 @@
 // cached in GPU memory; APOTNL_SIC / SICLAGM / FRMORB2 entry points read from
 // that cache instead of the ZPOT#### files.
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -82,54 +83,13 @@ struct DevBuf {
 };
 
 // ---------------------------------------------------------------------------
-// small dense symmetric eigen-solver (cyclic Jacobi) for the Lowdin step
-// (the role of DIAGGE_FO, diagon_sic.f:45); a: n*n row-major, v columns.
+// LOWSIC (lowden_files.f:2-172): S^{-1/2} of the FO overlap from its
+// eigen-decomposition (the role of DIAGGE_FO, diagon_sic.f:45); sym_eigen(n, a,
+// w, v) returns the eigenvalues w and v[k*n + m] = component k of eigenvector m.
 // ---------------------------------------------------------------------------
-void sym_eigen(int n, std::vector<double> a, std::vector<double>& w, std::vector<double>& v) {
-  v.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) v[(size_t)i * n + i] = 1.0;
-  for (int sweep = 0; sweep < 100; ++sweep) {
-    double off = 0.0, tot = 0.0;
-    for (int i = 0; i < n; ++i)
-      for (int j = 0; j < n; ++j) {
-        double x = a[(size_t)i * n + j] * a[(size_t)i * n + j];
-        tot += x;
-        if (i != j) off += x;
-      }
-    if (off <= 1e-30 * tot || off == 0.0) break;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = a[(size_t)p * n + q];
-        if (apq == 0.0) continue;
-        const double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < n; ++k) {
-          const double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
-          a[(size_t)k * n + p] = c * akp - s * akq;
-          a[(size_t)k * n + q] = s * akp + c * akq;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
-          a[(size_t)p * n + k] = c * apk - s * aqk;
-          a[(size_t)q * n + k] = s * apk + c * aqk;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double vkp = v[(size_t)k * n + p], vkq = v[(size_t)k * n + q];
-          v[(size_t)k * n + p] = c * vkp - s * vkq;
-          v[(size_t)k * n + q] = s * vkp + c * vkq;
-        }
-      }
-  }
-  w.resize(n);
-  for (int i = 0; i < n; ++i) w[i] = a[(size_t)i * n + i];
-}
-
-// LOWSIC (lowden_files.f:2-172): returns S^{-1/2} (row-major), eigenvectors
-// (filo[i*n+a]) and eigenvalues lambda.
-void lowsic(int n, const std::vector<double>& over, std::vector<double>& sm12, std::vector<double>& filo,
-            std::vector<double>& lam) {
+template <class Eig>
+void lowsic(Eig&& sym_eigen, int n, const std::vector<double>& over, std::vector<double>& sm12,
+            std::vector<double>& filo, std::vector<double>& lam) {
   std::vector<double> w;
   sym_eigen(n, over, w, filo);
   for (int i = 0; i < n; ++i)
@@ -299,6 +259,7 @@ struct SpinCache {
   std::vector<double> fmat;    // [(K*nf + jfm)*nw + jwf]
   std::vector<double> tmat;    // [k*nw + jwf]
   std::vector<double> lam;     // Lowdin eigenvalues
+  std::vector<double> filo;    // Lowdin eigenvectors [k*nf + a]: component k of eigenvector a
   std::vector<double> results; // [k*13 + i]
   std::vector<double> cfrm;    // [k*3 + d]
   std::vector<double> sic;     // [l*nf + j] = SIC(j,l)
@@ -323,6 +284,9 @@ struct flosic_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  DevBuf<double> d_eig_a, d_eig_w, d_eig_work;
+  DevBuf<int> d_eig_info;
   bool have_geom = false, have_orb = false;
   // geometry
   int natoms = 0, ntypes = 0, nbasis = 0, nprim = 0, nmsh = 0, nspn = 1, gga = 0;
@@ -601,6 +565,41 @@ void invalidate(flosic_ctx* c) {
 // ---------------------------------------------------------------------------
 // FO construction (FRMORB2(0,0) and FRMIORB(1,1)) for one spin
 // ---------------------------------------------------------------------------
+#define SOLVER_CHECK(x)                                                                 \
+  do {                                                                                  \
+    cusolverStatus_t s_ = (x);                                                          \
+    if (s_ != CUSOLVER_STATUS_SUCCESS) fail(FLOSIC_ERR_CUDA, std::string(#x) + " failed (" + std::to_string((int)s_) + ")"); \
+  } while (0)
+
+// Symmetric eigen-decomposition on the GPU (cuSOLVER syevd, FP64, ascending
+// eigenvalues) in the convention lowsic expects.
+auto device_eigen(flosic_ctx* c) {
+  return [c](int n, const std::vector<double>& a, std::vector<double>& w, std::vector<double>& v) {
+    cudaStream_t st = c->st;
+    c->d_eig_a.upload(a.data(), (size_t)n * n, st);
+    c->d_eig_w.ensure(n);
+    c->d_eig_info.ensure(1);
+    int lwork = 0;
+    SOLVER_CHECK(cusolverDnDsyevd_bufferSize(c->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
+                                             c->d_eig_a.p, n, c->d_eig_w.p, &lwork));
+    c->d_eig_work.ensure((size_t)std::max(lwork, 1));
+    SOLVER_CHECK(cusolverDnDsyevd(c->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, c->d_eig_a.p, n,
+                                  c->d_eig_w.p, c->d_eig_work.p, lwork, c->d_eig_info.p));
+    std::vector<double> vc((size_t)n * n);
+    w.resize(n);
+    int info = 0;
+    CUDA_CHECK(cudaMemcpyAsync(vc.data(), c->d_eig_a.p, sizeof(double) * vc.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaMemcpyAsync(w.data(), c->d_eig_w.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaMemcpyAsync(&info, c->d_eig_info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+    if (info != 0) fail(FLOSIC_ERR_LOWDEN, "LOWSIC: eigen-decomposition of the FO overlap failed (syevd info " +
+                                               std::to_string(info) + ")");
+    v.resize((size_t)n * n);
+    for (int m = 0; m < n; ++m)
+      for (int k = 0; k < n; ++k) v[(size_t)k * n + m] = vc[(size_t)m * n + k];  // column m = eigenvector m
+  };
+}
+
 void fo_setup(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
   if (S.fo_valid) return;
@@ -661,8 +660,8 @@ void fo_setup(flosic_ctx* c, int s) {
       for (int w = 0; w < nw; ++w) v = v + T[(size_t)i * nw + w] * T[(size_t)j * nw + w];
       over[(size_t)i * nf + j] = v;
     }
-  std::vector<double> sm12, filo;
-  lowsic(nf, over, sm12, filo, S.lam);
+  std::vector<double> sm12;
+  lowsic(device_eigen(c), nf, over, sm12, S.filo, S.lam);
   S.tmat.assign((size_t)nf * nw, 0.0);
   for (int i = 0; i < nf; ++i)
     for (int k = 0; k < nf; ++k) {
@@ -851,15 +850,10 @@ void spin_force(flosic_ctx* c, int s, const double* sic /* SIC(j,l) at [l*ld + j
   const int nf = S.nf, nw = S.nw;
   auto fm = [&](int kwf, int ifm, int K) { return S.fmat[((size_t)K * nf + ifm) * nw + kwf]; };
   auto t0 = std::chrono::steady_clock::now();
-  std::vector<double> over((size_t)nf * nf);
-  for (int i = 0; i < nf; ++i)
-    for (int j = 0; j < nf; ++j) {
-      double v = 0.0;
-      for (int w = 0; w < nw; ++w) v = v + fm(w, i, 0) * fm(w, j, 0);
-      over[(size_t)j * nf + i] = v;
-    }
-  std::vector<double> sm12, filo, Q;
-  lowsic(nf, over, sm12, filo, Q);
+  // the Lowdin eigenpairs of the overlap sum_w F(w,i,0) F(w,j,0) (frmorb2.F:460-583)
+  // are those fo_setup computed for TMAT: the same overlap of the same FMAT
+  const std::vector<double>& filo = S.filo;
+  const std::vector<double>& Q = S.lam;
   auto FI = [&](int i, int a) { return filo[(size_t)i * nf + a]; };
   // G = FILO^T SIC FILO  ->  HAM(b,a) = (G[a][b] - G[b][a]) / sqrt(Qa Qb)
   std::vector<double> tmp((size_t)nf * nf, 0.0), G((size_t)nf * nf, 0.0);
@@ -1013,7 +1007,15 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     c->device = device;
     if (const char* e = std::getenv("FLOSIC_COULOMB")) c->per_fo_coulomb = (std::string(e) == "perfo");
     CUDA_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) {
+      cudaStreamDestroy(c->st);
+      delete c;
+      fail(FLOSIC_ERR_CUDA, "cusolverDnCreate failed");
+    }
+    cusolverDnSetStream(c->solver, c->st);
     if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
+      cusolverDnDestroy(c->solver);
+      cudaStreamDestroy(c->st);
       delete c;
       fail(FLOSIC_ERR_CUDA, "cublasCreate failed");
     }
@@ -1048,7 +1050,9 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
   c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
   c->d_share.release(); c->d_lists.release();
+  c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_work.release(); c->d_eig_info.release();
   if (c->blas) cublasDestroy(c->blas);
+  if (c->solver) cusolverDnDestroy(c->solver);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return FLOSIC_OK;

@@ -28,7 +28,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "s per FLO-SIC SCF cycle (all FOs + FOD forces)"
+METRIC = "s per FLO-SIC SCF cycle (all FOs + FOD forces), mixed vs FP64, |ΔE_SIC|≤10µHa"
 COULOMB_FLOPS_NEAR = 92.0    # per near (pair, point, FO): 46 polynomial coefficients x Boys-monomial terms
 COULOMB_FLOPS_TERM = 2.0     # per multipole term kept by the skip rule in a far (call, point, FO) evaluation
 # DRAM bytes of the two Coulomb kernels per tile of 128 points on the C2 shape:
@@ -202,36 +202,66 @@ def run_ours(args, rank, world, local_rank):
     ctx.set_geometry(sysm)
     ctx.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
     ld = ctx.ld
-    out = dict(results=np.zeros(2 * ld * 13), sic=np.zeros(2 * ld * ld), debdax=np.zeros(2 * ld * 3),
-               cfrm=np.zeros(2 * ld * 3), esic=np.zeros(1))
-    for _ in range(args.warmup):
-        ctx.cycle(out)
+
+    def new_out():
+        return dict(results=np.zeros(2 * ld * 13), sic=np.zeros(2 * ld * ld), debdax=np.zeros(2 * ld * 3),
+                    cfrm=np.zeros(2 * ld * 3), esic=np.zeros(1))
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # timed region: inputs resident in GPU memory
-    st_acc = dict(coul_ms=0.0, near=0, far=0, terms=0, launches=0, stage=np.zeros(7))
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        e0.record()
-        for _ in range(args.steps):
-            r = ctx.cycle(out)
-            st = ctx.stats()
-            st_acc["coul_ms"] += st["stage_ms"][3]
-            st_acc["near"] += st["near_evals"]
-            st_acc["far"] += st["far_evals"]
-            st_acc["terms"] += st["far_terms"]
-            st_acc["launches"] += st["launches"]
-            st_acc["stage"] += st["stage_ms"]
-        e1.record()
-        torch.cuda.synchronize()
+    def timed(mode, clk_sampler):
+        """W warm-up and K timed SIC cycles in one precision; inputs resident."""
+        ctx.set_precision(mode)
+        out = new_out()
+        for _ in range(args.warmup):
+            ctx.cycle(out)
+        acc = dict(coul_ms=0.0, near=0, far=0, terms=0, launches=0, stage=np.zeros(7))
         barrier()
-    t_ms = e0.elapsed_time(e1)
-    # e2e: host buffers through the C ABI (KS orbitals + FODs in, results out)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with clk_sampler as clk:
+            e0.record()
+            for _ in range(args.steps):
+                r = ctx.cycle(out)
+                st = ctx.stats()
+                acc["coul_ms"] += st["stage_ms"][3]
+                acc["near"] += st["near_evals"]
+                acc["far"] += st["far_evals"]
+                acc["terms"] += st["far_terms"]
+                acc["launches"] += st["launches"]
+                acc["stage"] += st["stage_ms"]
+            e1.record()
+            torch.cuda.synchronize()
+            barrier()
+        res = {k: np.array(v, copy=True) for k, v in r.items() if k != "esic"}
+        res["esic"] = r["esic"]
+        return e0.elapsed_time(e1), acc, res, clk.summary()
+
+    modes = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    runs = {m: timed(m, ClockSampler(local_rank)) for m in modes}
+    errors = None
+    headline = modes[-1]
+    if "fp64" in runs and "mixed" in runs:
+        a, b = runs["fp64"][2], runs["mixed"][2]
+        n = [sysm.nfrm[s] for s in range(sysm.nspn)]
+        dsic = max(np.abs(a["sic"][s][:n[s], :n[s]] - b["sic"][s][:n[s], :n[s]]).max() for s in range(sysm.nspn))
+        msic = max(np.abs(a["sic"][s][:n[s], :n[s]]).max() for s in range(sysm.nspn))
+        errors = {"d_esic_ha": abs(a["esic"] - b["esic"]),
+                  "max_d_esic_per_fo_ha": max(np.abs(a["results"][s][:n[s], 8] - b["results"][s][:n[s], 8]).max()
+                                              for s in range(sysm.nspn)),
+                  "max_d_sic_matrix_rel": dsic / msic,
+                  "max_d_fod_force_ha_bohr": max(np.abs(a["debdax"][s][:n[s]] - b["debdax"][s][:n[s]]).max()
+                                                 for s in range(sysm.nspn))}
+        errors["gate_esic_1e-5_ha"] = bool(errors["d_esic_ha"] <= 1e-5)
+        errors["gate_force_1e-4_ha_bohr"] = bool(errors["max_d_fod_force_ha_bohr"] <= 1e-4)
+        if not (errors["gate_esic_1e-5_ha"] and errors["gate_force_1e-4_ha_bohr"]):
+            headline = "fp64"
+    t_ms, st_acc, r, clocks = runs[headline]
+    # e2e: host buffers through the C ABI (KS orbitals + FODs in, results out), headline precision
+    ctx.set_precision(headline)
+    out = new_out()
     psi = np.ascontiguousarray(sysm.psi)
     barrier()
     torch.cuda.synchronize()
@@ -246,12 +276,15 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = f0.elapsed_time(f1)
     h2d = psi.nbytes + 8 * 3 * ld * 2
     d2h = sum(v.nbytes for v in out.values())
+    times = {m: runs[m][0] for m in runs}
     if dist is not None:
-        t = torch.tensor([t_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        keys = sorted(times)
+        t = torch.tensor([times[k] for k in keys] + [e2e_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms, e2e_ms = float(t[0]), float(t[1])
+        times = {k: float(t[i]) for i, k in enumerate(keys)}
+        e2e_ms = float(t[-1])
+        t_ms = times[headline]
     ctx_stats = ctx.stats()
-    esic = r["esic"]
     ctx.close()
     if rank != 0:
         return
@@ -264,11 +297,12 @@ def run_ours(args, rank, world, local_rank):
     ntiles = (cfg["nmsh"] + 127) // 128
     traffic = COULOMB_DRAM_BYTES_PER_TILE * ntiles if args.workload in ("c2", "c2half", "c2tiny") else None
     cfg.update(parallelism=f"replicas x{world}" if world > 1 else "single GPU", l2="working set >> L2 (126 MB)",
-               npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision="fp64")
+               npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision=headline)
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": cfg,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if headline == "fp64" else "f32+f64",
+        "data": "synthetic (seeded)", "config": cfg,
         "e2e": {"value": e2e_ms / 1e3 / args.steps / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(st_acc["launches"]),
@@ -282,9 +316,20 @@ def run_ours(args, rank, world, local_rank):
                              f"({st_acc['far'] / args.steps:.4g} far (call,point,FO) evaluations)"},
         "stage_ms": {k: round(float(v) / args.steps, 3) for k, v in
                      zip(["fo", "orbitals", "coul_setup", "coul_eval", "xc", "sicmat", "forces"], st_acc["stage"])},
-        "esic": esic,
-        "clocks": clk.summary(),
+        "esic": r["esic"],
+        "clocks": clocks,
     }
+    if len(runs) > 1:
+        line["precision"] = {
+            "headline": headline,
+            "s_per_cycle": {m: times[m] / 1e3 / args.steps / world for m in runs},
+            "stage_ms": {m: {k: round(float(v) / args.steps, 3) for k, v in
+                             zip(["fo", "orbitals", "coul_setup", "coul_eval", "xc", "sicmat", "forces"],
+                                 runs[m][1]["stage"])} for m in runs},
+            "speedup_mixed_vs_fp64": times["fp64"] / times["mixed"],
+            "mixed_vs_fp64_errors": errors,
+            "clocks": {m: runs[m][3] for m in runs},
+        }
     if world == 1 and not args.no_cpu_baseline:
         cb, sample = cpu_baseline(sysm, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": cb, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -298,6 +343,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="time the FP64 path, the mixed path, or both (headline = mixed when it meets the "
+                         "|dE_SIC| <= 1e-5 Ha and FOD-force <= 1e-4 Ha/bohr gates)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "water", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -95,6 +95,17 @@ int flosic_sic_coupot_sic(flosic_ctx* ctx, int kxxs, int kxxo, double* coulomb, 
    (apotnl_sic.F:419): VXC(2*ndim) and ERGXL,ERGXN,ERGCL,ERGCN in ergs[4]. */
 int flosic_sic_getvlxc(flosic_ctx* ctx, int ndim, const double* rhog, double* vxc, double* ergs);
 
+/* Precision of the SIC path (no counterpart in the reference).
+   FLOSIC_PRECISION_FP64 (default) is the drop-in: every step in FP64.
+   FLOSIC_PRECISION_MIXED forms the Coulomb potential's geometric columns
+   (Boys functions times monomials, harmonics) and the per-FO far field in
+   single precision and contracts the single-pair calls on the tensor cores as
+   TF32 split products (hi*hi + hi*lo + lo*hi) with FP32 accumulation folded
+   into compensated sums; the FO construction, Lowdin orthogonalisation, XC and
+   energy sums stay FP64.  Changing the mode invalidates the cached potentials. */
+enum { FLOSIC_PRECISION_FP64 = 0, FLOSIC_PRECISION_MIXED = 1 };
+int flosic_sic_set_precision(flosic_ctx* ctx, int mode);
+
 /* Allocation-free form of flosic_sic_getvlxc on the caller's device buffers (no
    counterpart in the reference).  d_rhog: RHOG(ldr,10) density channels in
    device memory (channel stride ldr >= npts), d_wmsh: the npts mesh weights,

@@ -35,6 +35,7 @@
 // (call, point, FO) and the multipole terms the far evaluations keep, the
 // units of the reference's POISSON1 work.
 #include <cfloat>
+#include <type_traits>
 
 #include "device_math.cuh"
 #include "kernels.cuh"
@@ -91,46 +92,46 @@ __device__ __forceinline__ int tile_class(const double lo[3], const double hi[3]
 //   m = l (sectoral):  C_l = (2l-1)(C_{l-1} ux - S_{l-1} uy),  S_l = (2l-1)(S_{l-1} ux + C_{l-1} uy)
 //   m < l:             P_l = ((2l-1)/(l-m)) P_{l-1} uz - ((l+m-1)/(l-m)) P_{l-2}
 // op(row, l, value) receives each term; the caller applies 1/r^(l+1).
-template <typename Op>
-__device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz, int lmx, Op op) {
+template <typename T, typename Op>
+__device__ __forceinline__ void harmonics_mmajor(T ux, T uy, T uz, int lmx, Op op) {
   // m = 0
   {
-    op(0, 0, 1.0);
+    op(0, 0, T(1));
     if (lmx >= 1) op(1, 1, uz);
-    double p2 = 1.0, p1 = uz;
+    T p2 = T(1), p1 = uz;
 #pragma unroll
     for (int l = 2; l <= LM; ++l) {
       if (l > lmx) break;
-      const double facrc = 1.0 / l;
-      const double aa = facrc * (2 * l - 1), bb = facrc * (l - 1);
-      const double cu = aa * p1 * uz - bb * p2;
+      const T facrc = T(1) / T(l);
+      const T aa = facrc * T(2 * l - 1), bb = facrc * T(l - 1);
+      const T cu = aa * p1 * uz - bb * p2;
       op(l * l, l, cu);
       p2 = p1;
       p1 = cu;
     }
   }
-  double sc = ux, ss = uy;  // sectoral pair at l = m
+  T sc = ux, ss = uy;  // sectoral pair at l = m
 #pragma unroll
   for (int m = 1; m <= LM; ++m) {
     if (m > lmx) break;
     if (m > 1) {
-      const double ifc = (double)(2 * m - 1);
-      const double nc = ifc * (sc * ux - ss * uy);
-      const double ns = ifc * (ss * ux + sc * uy);
+      const T ifc = T(2 * m - 1);
+      const T nc = ifc * (sc * ux - ss * uy);
+      const T ns = ifc * (ss * ux + sc * uy);
       sc = nc;
       ss = ns;
     }
     op(m * m + 2 * m - 1, m, sc);
     op(m * m + 2 * m, m, ss);
-    double c2 = 0.0, s2 = 0.0, c1 = sc, s1 = ss;
+    T c2 = T(0), s2 = T(0), c1 = sc, s1 = ss;
 #pragma unroll
     for (int l = m + 1; l <= LM; ++l) {
       if (l > lmx) break;
-      const double facrc = 1.0 / (l - m);
-      const double aa = facrc * (2 * l - 1);
-      const double bb = (m == l - 1) ? 0.0 : facrc * (l + m - 1);
-      const double cc = aa * c1 * uz - bb * c2;
-      const double cs = aa * s1 * uz - bb * s2;
+      const T facrc = T(1) / T(l - m);
+      const T aa = facrc * T(2 * l - 1);
+      const T bb = (m == l - 1) ? T(0) : facrc * T(l + m - 1);
+      const T cc = aa * c1 * uz - bb * c2;
+      const T cs = aa * s1 * uz - bb * s2;
       op(l * l + 2 * m - 1, l, cc);
       op(l * l + 2 * m, l, cs);
       c2 = c1;
@@ -142,39 +143,42 @@ __device__ __forceinline__ void harmonics_mmajor(double ux, double uy, double uz
 }
 
 // Boys values F_0..F_{fmt-1} of the FFFMTC3/4/5 variant (same arithmetic as
-// boys_all); absent orders are zero.
-__device__ __forceinline__ void boys_fmt(const double* __restrict__ tab, double x, double chgd, int fmt,
-                                         double F[5]) {
-  if (x > 16.0) {
-    const double ROOTPI = 1.77245385090551602728;
-    const double pol1 = -chgd;
-    const double rt = __dmul_rn(sqrt(x), ROOTPI);
-    const double rect1 = 0.5 / x;
+// boys_all); absent orders are zero.  T = float evaluates the same steps in
+// single precision (the mixed-precision path).
+template <typename T>
+__device__ __forceinline__ void boys_fmt(const double* __restrict__ tab, T x, T chgd, int fmt, T F[5]) {
+  if (x > T(16)) {
+    const T ROOTPI = T(1.77245385090551602728);
+    const T pol1 = -chgd;
+    T rt;
+    if constexpr (sizeof(T) == 8) rt = __dmul_rn(sqrt(x), ROOTPI);
+    else rt = sqrtf(x) * ROOTPI;
+    const T rect1 = T(0.5) / x;
     F[0] = rect1 * (rt + pol1);
     F[1] = rect1 * (F[0] + pol1);
-    F[2] = rect1 * (3 * F[1] + pol1);
-    F[3] = (fmt >= 4) ? rect1 * (5 * F[2] + pol1) : 0.0;
-    F[4] = (fmt >= 5) ? rect1 * (7 * F[3] + pol1) : 0.0;
+    F[2] = rect1 * (T(3) * F[1] + pol1);
+    F[3] = (fmt >= 4) ? rect1 * (T(5) * F[2] + pol1) : T(0);
+    F[4] = (fmt >= 5) ? rect1 * (T(7) * F[3] + pol1) : T(0);
     return;
   }
-  const int it = (int)(100 * x + 1.5);
-  const double pol1 = chgd;
-  const double rect1 = 2 * x;
-  const double dt = (1.0e-2) * (it - 1) - x;
+  const int it = (int)(T(100) * x + T(1.5));
+  const T pol1 = chgd;
+  const T rect1 = T(2) * x;
+  const T dt = T(1.0e-2) * T(it - 1) - x;
   const double* f = tab + (size_t)(it - 1) * BOYS_NC;
-  const double o7 = 1.0 / 7.0, o5 = 1.0 / 5.0, o3 = 1.0 / 3.0;
+  const T o7 = T(1) / T(7), o5 = T(1) / T(5), o3 = T(1) / T(3);
   if (fmt == 5) {
-    F[4] = f[2] + dt * (f[3] + dt * (f[6] + dt * f[9]));
+    F[4] = T(f[2]) + dt * (T(f[3]) + dt * (T(f[6]) + dt * T(f[9])));
     F[3] = (F[4] * rect1 + pol1) * o7;
     F[2] = (F[3] * rect1 + pol1) * o5;
   } else if (fmt == 4) {
-    F[4] = 0.0;
-    F[3] = f[1] + dt * (f[2] + dt * (f[5] + dt * f[8]));
+    F[4] = T(0);
+    F[3] = T(f[1]) + dt * (T(f[2]) + dt * (T(f[5]) + dt * T(f[8])));
     F[2] = (F[3] * rect1 + pol1) * o5;
   } else {
-    F[4] = 0.0;
-    F[3] = 0.0;
-    F[2] = f[0] + dt * (f[1] + dt * (f[4] + dt * f[7]));
+    F[4] = T(0);
+    F[3] = T(0);
+    F[2] = T(f[0]) + dt * (T(f[1]) + dt * (T(f[4]) + dt * T(f[7])));
   }
   F[1] = (F[2] * rect1 + pol1) * o3;
   F[0] = (F[1] * rect1 + pol1);
@@ -188,10 +192,11 @@ __device__ __forceinline__ int near_rows(int fmt) { return fmt >= 5 ? 48 : (fmt 
 // G column of one (pair, point) in the COEFICIENT slot order: slot t holds
 // F_{m(t)} * POLY(mono(t)), monomials in the order of poisson1.f:925-959.
 // Rows >= kn (16, 32 or 48) are not written.
-__device__ __forceinline__ void write_g(double* g, int kn, double x, double y, double z, const double F[5]) {
-#define GW(t, v) g[(size_t)(t) * G_LD] = (v)
-  const double F0 = F[0], F1 = F[1], F2 = F[2], F3 = F[3], F4 = F[4];
-  const double zz = z * z, yz = y * z, yy = y * y, xz = x * z, xy = x * y, xx = x * x;
+template <typename T>
+__device__ __forceinline__ void write_g(double* g, int kn, T x, T y, T z, const T F[5]) {
+#define GW(t, v) g[(size_t)(t) * G_LD] = (double)(v)
+  const T F0 = F[0], F1 = F[1], F2 = F[2], F3 = F[3], F4 = F[4];
+  const T zz = z * z, yz = y * z, yy = y * y, xz = x * z, xy = x * y, xx = x * x;
   GW(0, F0);
   GW(1, F1);
   GW(2, F2);
@@ -240,8 +245,8 @@ __device__ __forceinline__ void write_g(double* g, int kn, double x, double y, d
   GW(43, F4 * (xz * xx));
   GW(44, F4 * (xy * xx));
   GW(45, F4 * (xx * xx));
-  GW(46, 0.0);
-  GW(47, 0.0);
+  GW(46, T(0));
+  GW(47, T(0));
 #undef GW
 }
 
@@ -375,26 +380,33 @@ __device__ __forceinline__ int far_degree(int kf) {
 }
 
 // H column (rows [0, kf)) of one far point: harmonics times 1/r^(l+1), zero padded.
-__device__ __forceinline__ void write_h(double* g, int kf, double dx, double dy, double dz, double r2) {
-  const double hn = 1.0 / sqrt(r2);
+template <typename T>
+__device__ __forceinline__ void write_h(double* g, int kf, T dx, T dy, T dz, T r2) {
+  T hn;
+  if constexpr (sizeof(T) == 8) hn = 1.0 / sqrt(r2);
+  else hn = rsqrtf(r2);
   const int lmx = far_degree(kf);
-  double rec[LM + 1];
+  T rec[LM + 1];
   rec[0] = hn;
 #pragma unroll
   for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
   harmonics_mmajor(hn * dx, hn * dy, hn * dz, lmx,
-                   [&](int row, int l, double v) { g[(size_t)row * G_LD] = v * rec[l]; });
+                   [&](int row, int l, T v) { g[(size_t)row * G_LD] = (double)(v * rec[l]); });
   for (int t = (lmx + 1) * (lmx + 1); t < kf; ++t) g[(size_t)t * G_LD] = 0.0;
 }
 
 // G column of one near point of pair pg (rows [0, kn)).
+template <typename T>
 __device__ __forceinline__ void write_g_point(double* g, int kn, const PairGeo& pg, double x, double y, double z,
                                               const double* __restrict__ boys_tab) {
-  const double rx = x - pg.C[0], ry = y - pg.C[1], rz = z - pg.C[2];
-  const double xx = pg.delta * (rz * rz + ry * ry + rx * rx);
-  double F[5];
-  boys_fmt(boys_tab, xx, exp(-xx), kn >= 48 ? 5 : (kn == 32 ? 4 : 3), F);
-  write_g(g, kn, rx, ry, rz, F);
+  const T rx = T(x - pg.C[0]), ry = T(y - pg.C[1]), rz = T(z - pg.C[2]);
+  const T xx = T(pg.delta) * (rz * rz + ry * ry + rx * rx);
+  T ex;
+  if constexpr (sizeof(T) == 8) ex = exp(-xx);
+  else ex = expf(-xx);
+  T F[5];
+  boys_fmt<T>(boys_tab, xx, ex, kn >= 48 ? 5 : (kn == 32 ? 4 : 3), F);
+  write_g<T>(g, kn, rx, ry, rz, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -469,7 +481,7 @@ struct SegmentWalker {
   }
 };
 
-template <int WM>
+template <int WM, bool MIXED>
 __global__ void __launch_bounds__(WS_THREADS, 1)
 k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __restrict__ share,
                  const CallInfo* __restrict__ calls, int nfo, const double* __restrict__ coef,
@@ -477,6 +489,7 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
                  const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
                  double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
   constexpr int FOB = 32 * WM, WN = CONS_WARPS / WM, WPTS = TILE / WN, NT = WPTS / 8;
+  using PT = typename std::conditional<MIXED, float, double>::type;  // producer arithmetic
   extern __shared__ __align__(128) unsigned char smraw[];
   SharedSmem<WM>& S = *reinterpret_cast<SharedSmem<WM>*>(smraw);
   const int tile = blockIdx.x;
@@ -541,7 +554,7 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
           if (nr && s.cls == 2) nr = !(sqdist_rn2(x, y, z, s.cx, s.cy, s.cz) > s.rc2);
           if (nr) {
             ++my_near;
-            write_g_point(g, s.rows, pairs[s.idx], x, y, z, boys_tab);
+            write_g_point<PT>(g, s.rows, pairs[s.idx], x, y, z, boys_tab);
           } else {
             zero_rows(g, s.rows);
           }
@@ -555,7 +568,7 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
           if (fr) {
             ++my_far;
             if (count_terms) my_terms += (unsigned long long)s.ksum;
-            write_h(g, s.rows, x - s.cx, y - s.cy, z - s.cz, r2);
+            write_h<PT>(g, s.rows, PT(x - s.cx), PT(y - s.cy), PT(z - s.cz), PT(r2));
           } else {
             zero_rows(g, s.rows);
           }
@@ -643,13 +656,13 @@ __device__ __forceinline__ int slot_row(int s) {
 
 // Far-field potential of one FO at one point, sum_lm MV[lm] Y_lm(u) / r^(l+1),
 // summed per degree l and scaled once per degree.
-__device__ __forceinline__ double multipole(const double* __restrict__ mv, int lmx, double ux, double uy, double uz,
-                                            double hn) {
-  double acc[LM + 1];
+template <typename T>
+__device__ __forceinline__ T multipole(const double* __restrict__ mv, int lmx, T ux, T uy, T uz, T hn) {
+  T acc[LM + 1];
 #pragma unroll
-  for (int l = 0; l <= LM; ++l) acc[l] = 0.0;
-  harmonics_mmajor(ux, uy, uz, lmx, [&](int row, int l, double v) { acc[l] += mv[row] * v; });
-  double pot = 0.0, rec = hn;
+  for (int l = 0; l <= LM; ++l) acc[l] = T(0);
+  harmonics_mmajor(ux, uy, uz, lmx, [&](int row, int l, T v) { acc[l] += T(mv[row]) * v; });
+  T pot = T(0), rec = hn;
 #pragma unroll
   for (int l = 0; l <= LM; ++l) {
     pot += acc[l] * rec;
@@ -658,7 +671,7 @@ __device__ __forceinline__ double multipole(const double* __restrict__ mv, int l
   return pot;
 }
 
-template <int WM>
+template <int WM, bool MIXED>
 __global__ void __launch_bounds__(WS_THREADS, 1)
 k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
                 const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
@@ -666,6 +679,7 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
                 const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
                 double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
   constexpr int FOB = 32 * WM, WC = PerFOSmem<WM>::WC, SC = 32 * WC;
+  using PT = typename std::conditional<MIXED, float, double>::type;  // producer and far-field arithmetic
   constexpr int WN = CONS_WARPS / WC, WPTS = TILE / WN, NT = WPTS / 8;
   const int* list = lists + ncalls;
   const int nl = lists[2 * ncalls + 1];
@@ -766,7 +780,7 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
           for (int j = 0; j < PTS_PER_PROD; ++j) {
             const int p = pt + j * NPROD;
             double* g = &S.B[b][(size_t)off * G_LD + p];
-            if (p < np) write_g_point(g, kq, pg, S.px[p], S.py[p], S.pz[p], boys_tab);
+            if (p < np) write_g_point<PT>(g, kq, pg, S.px[p], S.py[p], S.pz[p], boys_tab);
             else zero_rows(g, kq);
           }
         }
@@ -836,8 +850,14 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
           if (r2 > rc2) {
             ++my_far;
             my_terms += nkeep;
-            const double hn = 1.0 / sqrt(r2);
-            vk[p] += multipole(mv, lmx, hn * (x - cx), hn * (y - cy), hn * (z - cz), hn);
+            if constexpr (MIXED) {
+              const float hn = rsqrtf((float)r2);
+              vk[p] += (double)multipole<float>(mv, lmx, hn * (float)(x - cx), hn * (float)(y - cy),
+                                                hn * (float)(z - cz), hn);
+            } else {
+              const double hn = 1.0 / sqrt(r2);
+              vk[p] += multipole<double>(mv, lmx, hn * (x - cx), hn * (y - cy), hn * (z - cz), hn);
+            }
           }
         }
       }
@@ -938,13 +958,17 @@ __global__ void __launch_bounds__(LIST_THREADS) k_call_lists(int ncalls, int per
 
 template <int WM>
 static void set_shared_attr() {
-  cudaFuncSetAttribute(k_coulomb_shared<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_coulomb_shared<WM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(SharedSmem<WM>));
+  cudaFuncSetAttribute(k_coulomb_shared<WM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(SharedSmem<WM>));
 }
 
 template <int WM>
 static void set_perfo_attr() {
-  cudaFuncSetAttribute(k_coulomb_perfo<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_coulomb_perfo<WM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PerFOSmem<WM>));
+  cudaFuncSetAttribute(k_coulomb_perfo<WM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(PerFOSmem<WM>));
 }
 
@@ -962,51 +986,58 @@ template <int WM>
 static void launch_shared(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
                           const double* coef, const int8_t* pair_fmt, const PairGeo* pairs, const double* momv,
                           const MeshDev& M, const double* boys_tab, double* vh, int ldv, unsigned long long* cnt,
-                          cudaStream_t st) {
+                          bool mixed, cudaStream_t st) {
   dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
-  k_coulomb_shared<WM><<<grid, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(
-      ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M, boys_tab, vh, ldv, cnt);
+  if (mixed)
+    k_coulomb_shared<WM, true><<<grid, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(
+        ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M, boys_tab, vh, ldv, cnt);
+  else
+    k_coulomb_shared<WM, false><<<grid, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(
+        ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M, boys_tab, vh, ldv, cnt);
 }
 
 template <int WM>
 static void launch_perfo(int ncalls, const int* lists, int acc, const CallInfo* calls, const PairGeo* pairs, int nfo,
                          const double* coef, const int8_t* pair_fmt, const CallFO* cfo, const double* momv,
                          const MeshDev& M, const double* boys_tab, double* vh, int ldv, unsigned long long* cnt,
-                         cudaStream_t st) {
+                         bool mixed, cudaStream_t st) {
   dim3 grid(M.ntiles, (nfo + 32 * WM - 1) / (32 * WM));
-  k_coulomb_perfo<WM><<<grid, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(ncalls, lists, acc, calls, pairs, nfo, coef,
-                                                                         pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                                                                         cnt);
+  if (mixed)
+    k_coulomb_perfo<WM, true><<<grid, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(
+        ncalls, lists, acc, calls, pairs, nfo, coef, pair_fmt, cfo, momv, M, boys_tab, vh, ldv, cnt);
+  else
+    k_coulomb_perfo<WM, false><<<grid, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(
+        ncalls, lists, acc, calls, pairs, nfo, coef, pair_fmt, cfo, momv, M, boys_tab, vh, ldv, cnt);
 }
 
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,
-                        const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st) {
+                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st) {
   if (npairs > 0) k_pair_fmt<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, nfo, maxfmt, scr.pair_fmt);
   if (ncalls > 0) k_call_share<<<(ncalls + 7) / 8, 256, 0, st>>>(ncalls, nfo, cfo, scr.share);
   k_call_lists<<<1, LIST_THREADS, 0, st>>>(ncalls, per_fo_only ? 1 : 0, scr.share, scr.lists);
   if (!per_fo_only) {
     if (nfo > 64)
       launch_shared<4>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
-                       ldv, cnt, st);
+                       ldv, cnt, mixed, st);
     else if (nfo > 32)
       launch_shared<2>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
-                       ldv, cnt, st);
+                       ldv, cnt, mixed, st);
     else
       launch_shared<1>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
-                       ldv, cnt, st);
+                       ldv, cnt, mixed, st);
   }
   const int acc = per_fo_only ? 0 : 1;
   if (nfo > 64)
     launch_perfo<4>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                    cnt, st);
+                    cnt, mixed, st);
   else if (nfo > 32)
     launch_perfo<2>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                    cnt, st);
+                    cnt, mixed, st);
   else
     launch_perfo<1>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                    cnt, st);
+                    cnt, mixed, st);
 }
 
 }  // namespace flosic

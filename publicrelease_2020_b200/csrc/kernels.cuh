@@ -57,7 +57,9 @@ void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, 
 // FP64 tensor cores (csrc/coulomb_mma.cu).  Calls whose near/far geometry is
 // identical for every FO go through the shared-geometry kernel, the rest
 // through the per-FO kernel, which adds its part.  per_fo_only routes every
-// call through the per-FO kernel (a cross-check of the two forms).
+// call through the per-FO kernel (a cross-check of the two forms).  mixed
+// selects the mixed-precision path: geometric columns and the per-FO far field
+// in single precision, the shared-geometry GEMM on tcgen05 (TF32 split products).
 // cnt[0] += near (pair, point, FO) evaluations, cnt[1] += far (call, point, FO),
 // cnt[2] += multipole terms kept by the skip rule over those far evaluations.
 struct CoulombScratch {
@@ -69,7 +71,7 @@ void init_coulomb_mma();
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,
-                        const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st);
+                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st);
 
 // Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as
 // in apotnl_sic.F:419) from the FO values/derivatives phi[(ch*nfo+k)*ldp+p];

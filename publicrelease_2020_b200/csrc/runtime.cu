@@ -319,6 +319,7 @@ struct flosic_ctx {
   DevBuf<CallShare> d_share;
   DevBuf<int> d_lists;
   bool per_fo_coulomb = false;   // FLOSIC_COULOMB=perfo: every call through the per-FO kernel (A/B checks)
+  int precision = FLOSIC_PRECISION_FP64;
   DevBuf<unsigned long long> d_cnt;
   unsigned long long work_near = 0, work_far = 0, work_terms = 0;
   DevBuf<CallFO> d_callfo;
@@ -733,7 +734,8 @@ void coulomb(flosic_ctx* c, int s) {
   CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 3 * sizeof(unsigned long long), st));
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                     c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, scr, c->d_cnt.p, st);
+                     c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb,
+                     c->precision == FLOSIC_PRECISION_MIXED, scr, c->d_cnt.p, st);
   c->launches += c->per_fo_coulomb ? 4 : 5;
   unsigned long long cnt[3];
   CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
@@ -1370,6 +1372,20 @@ int flosic_sic_getvlxc(flosic_ctx* c, int ndim, const double* rhog, double* vxc,
       vxc[ndim + c->perm[i]] = v[P + i];
     }
     for (int j = 0; j < 4; ++j) ergs[j] = sums[4 + j];
+  });
+}
+
+int flosic_sic_set_precision(flosic_ctx* c, int mode) {
+  return guarded([&] {
+    if (!c) fail(FLOSIC_ERR_ARG, "null context");
+    if (mode != FLOSIC_PRECISION_FP64 && mode != FLOSIC_PRECISION_MIXED) fail(FLOSIC_ERR_ARG, "unknown precision mode");
+    if (mode != c->precision) {
+      c->precision = mode;
+      for (auto& s : c->spin) {
+        s.pot_valid = false;
+        s.sic_valid = false;
+      }
+    }
   });
 }
 

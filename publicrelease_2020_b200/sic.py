@@ -34,7 +34,9 @@ EXPORTS = [
     "flosic_sic_set_orbitals", "flosic_sic_gorbdrv", "flosic_sic_frmorb2_fmat", "flosic_sic_frmiorb",
     "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
+    "flosic_sic_set_precision",
 ]
+PRECISION = {"fp64": 0, "mixed": 1}
 
 _lib = None
 
@@ -64,6 +66,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_frmiorb.argtypes = [_vp, _dp, _dp, C.c_int]
     L.flosic_sic_coupot_sic.argtypes = [_vp, C.c_int, C.c_int, _dp, _dp]
     L.flosic_sic_getvlxc.argtypes = [_vp, C.c_int, _dp, _dp, _dp]
+    L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
     L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
     L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.flosic_sic_siclagm.argtypes = [_vp, C.c_int, _dp, C.c_int]
@@ -160,6 +163,10 @@ class FlosicSIC:
         self._check(self.L.flosic_sic_getvlxc(self.h, n, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
                                               vxc, ergs))
         return vxc.reshape(2, n), ergs
+
+    def set_precision(self, mode):
+        """"fp64" (the drop-in, default) or "mixed"."""
+        self._check(self.L.flosic_sic_set_precision(self.h, PRECISION[mode]))
 
     def getvlxc_device(self, npts, d_rhog, ldr, d_wmsh, d_vxc):
         """Allocation-free GETVLXC on device buffers given as raw device addresses

@@ -66,8 +66,19 @@ struct CoulombScratch {
   int8_t* pair_fmt;    // npairs
   CallShare* share;    // ncalls
   int* lists;          // 2*ncalls + 2: shared calls, per-FO calls, the two counts
+  float* coef_hl;      // mixed path: TF32 hi/lo split of the coefficients (2 x npairs*nfo*COEF_LD)
+  float* momv_hl;      // mixed path: TF32 hi/lo split of the moments (2 x ncalls*nfo*MOM_LD)
+  int* err;            // mixed path: set when a tensor-core pipeline wait reached its limit
 };
 void init_coulomb_mma();
+void init_coulomb_tc();
+// TF32 hi/lo split of n doubles: out[i] = hi, out[n + i] = lo.
+void launch_split_tf32(size_t n, const double* src, float* out, cudaStream_t st);
+// Mixed-precision shared-geometry Coulomb GEMM on tcgen05 (csrc/coulomb_tc.cu).
+void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
+                              const float* coef_hl, size_t coef_part, const int8_t* pair_fmt, const PairGeo* pairs,
+                              const float* momv_hl, size_t mom_part, const MeshDev& M, const double* boys_tab,
+                              double* vh, int ldv, unsigned long long* cnt, int* err, cudaStream_t st);
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,

@@ -317,7 +317,8 @@ struct flosic_ctx {
   DevBuf<double> d_basis, d_fodpts, d_psig, d_tmat, d_u, d_coef, d_cgp, d_mom, d_part, d_sums, d_sic, d_tmp;
   DevBuf<int8_t> d_maxfmt, d_pairfmt;
   DevBuf<CallShare> d_share;
-  DevBuf<int> d_lists;
+  DevBuf<int> d_lists, d_tc_err;
+  DevBuf<float> d_coef_hl, d_momv_hl;
   bool per_fo_coulomb = false;   // FLOSIC_COULOMB=perfo: every call through the per-FO kernel (A/B checks)
   int precision = FLOSIC_PRECISION_FP64;
   DevBuf<unsigned long long> d_cnt;
@@ -732,14 +733,24 @@ void coulomb(flosic_ctx* c, int s) {
   c->d_lists.ensure((size_t)2 * ncalls + 2);
   c->d_cnt.ensure(3);
   CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 3 * sizeof(unsigned long long), st));
-  CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p};
+  const bool mixed = c->precision == FLOSIC_PRECISION_MIXED;
+  if (mixed) {
+    c->d_coef_hl.ensure((size_t)2 * std::max(npairs, 1) * nf * COEF_LD);
+    c->d_momv_hl.ensure((size_t)2 * std::max(ncalls, 1) * nf * MOM_LD);
+    c->d_tc_err.ensure(1);
+    CUDA_CHECK(cudaMemsetAsync(c->d_tc_err.p, 0, sizeof(int), st));
+  }
+  CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p, c->d_coef_hl.p, c->d_momv_hl.p, c->d_tc_err.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                     c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb,
-                     c->precision == FLOSIC_PRECISION_MIXED, scr, c->d_cnt.p, st);
+                     c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, mixed, scr,
+                     c->d_cnt.p, st);
   c->launches += c->per_fo_coulomb ? 4 : 5;
   unsigned long long cnt[3];
+  int tc_err = 0;
   CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  if (mixed) CUDA_CHECK(cudaMemcpyAsync(&tc_err, c->d_tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
+  if (tc_err) fail(FLOSIC_ERR_CUDA, "mixed-precision Coulomb kernel: a pipeline wait reached its limit");
   c->work_near += cnt[0];
   c->work_far += cnt[1];
   c->work_terms += cnt[2];
@@ -1029,6 +1040,7 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     upload_constants(ang.data(), w.data());
     init_call_setup();
     init_coulomb_mma();
+    init_coulomb_tc();
     std::vector<double> bt = boys_table();
     c->d_boys.upload(bt.data(), bt.size(), c->st);
     CUDA_CHECK(cudaStreamSynchronize(c->st));
@@ -1053,6 +1065,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
   c->d_share.release(); c->d_lists.release();
   c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_work.release(); c->d_eig_info.release();
+  c->d_coef_hl.release(); c->d_momv_hl.release(); c->d_tc_err.release();
   if (c->blas) cublasDestroy(c->blas);
   if (c->solver) cusolverDnDestroy(c->solver);
   if (c->st) cudaStreamDestroy(c->st);

@@ -426,20 +426,51 @@ __device__ __forceinline__ int slot_row(int s) {
 }
 
 // Far-field potential of one FO at one point, sum_lm MV[lm] Y_lm(u) / r^(l+1),
-// summed per degree l and scaled once per degree.
-template <typename T>
-__device__ __forceinline__ T multipole(const double* __restrict__ mv, int lmx, T ux, T uy, T uz, T hn) {
-  T acc[LM + 1];
+// summed per degree l and scaled once per degree; degree LMX at compile time.
+template <typename T, int LMX>
+__device__ __forceinline__ T multipole(const T* __restrict__ mv, T ux, T uy, T uz, T hn) {
+  T acc[LMX + 1];
 #pragma unroll
-  for (int l = 0; l <= LM; ++l) acc[l] = T(0);
-  harmonics_mmajor(ux, uy, uz, lmx, [&](int row, int l, T v) { acc[l] += T(mv[row]) * v; });
+  for (int l = 0; l <= LMX; ++l) acc[l] = T(0);
+  harmonics_mmajor(ux, uy, uz, LMX, [&](int row, int l, T v) { acc[l] += mv[row] * v; });
   T pot = T(0), rec = hn;
 #pragma unroll
-  for (int l = 0; l <= LM; ++l) {
+  for (int l = 0; l <= LMX; ++l) {
     pot += acc[l] * rec;
     rec *= hn;
   }
   return pot;
+}
+
+// Far field of one FO over the tile's points, lanes over points with the
+// TILE/32 points of a lane evaluated together (independent chains; points
+// that are near or past np are evaluated on a dummy radius and not added).
+// The near/far decision is the FP64 distance test of poisson1.f; T is the
+// arithmetic of the expansion.
+template <typename T, int LMX>
+__device__ __forceinline__ void far_points(const T* __restrict__ mv, const double* __restrict__ px,
+                                           const double* __restrict__ py, const double* __restrict__ pz, int np,
+                                           double cx, double cy, double cz, double rc2, double* __restrict__ vk,
+                                           int lane, unsigned long long& nfar) {
+#pragma unroll
+  for (int j = 0; j < TILE / 32; ++j) {
+    const int p = lane + 32 * j;
+    const double x = px[p], y = py[p], z = pz[p];
+    const double r2 = sqdist_rn2(x, y, z, cx, cy, cz);
+    const bool f = p < np && r2 > rc2;
+    T pot;
+    if constexpr (sizeof(T) == 4) {
+      const float hn = rsqrtf(f ? (float)r2 : 1.f);
+      pot = multipole<float, LMX>(mv, hn * (float)(x - cx), hn * (float)(y - cy), hn * (float)(z - cz), hn);
+    } else {
+      const double hn = 1.0 / sqrt(f ? r2 : 1.0);
+      pot = multipole<double, LMX>(mv, hn * (x - cx), hn * (y - cy), hn * (z - cz), hn);
+    }
+    if (f) {
+      vk[p] += (double)pot;
+      ++nfar;
+    }
+  }
 }
 
 template <int WM, bool MIXED>
@@ -605,32 +636,33 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
 
     if (anyfar) {
       __syncthreads();  // the near phase is done with vh
+      // the FOs' moments in the arithmetic of the expansion (FP32 in the mixed path)
+      PT* MVp = reinterpret_cast<PT*>(S.MV);
       const double* mg = momv + ((size_t)c * nfo + k0) * MOM_LD;
-      for (int e = tid; e < nk * MOM_LD; e += WS_THREADS) S.MV[e] = mg[e];
+      for (int e = tid; e < nk * MOM_LD; e += WS_THREADS) MVp[e] = (PT)mg[e];
       __syncthreads();
       for (int k = warp; k < nk; k += WS_THREADS / 32) {
         if (S.stat[k] == 0 || S.npot[k] == 1) continue;
         const double cx = S.cg[k][0], cy = S.cg[k][1], cz = S.cg[k][2], rc2 = S.rc2[k];
-        const int lmx = S.lmax[k];
-        const unsigned long long nkeep = (unsigned long long)S.nkeep[k];
-        const double* mv = &S.MV[k * MOM_LD];
+        const PT* mv = MVp + k * MOM_LD;
         double* vk = vh + (size_t)(k0 + k) * ldv + p0;
-        for (int p = lane; p < np; p += 32) {
-          const double x = S.px[p], y = S.py[p], z = S.pz[p];
-          const double r2 = sqdist_rn2(x, y, z, cx, cy, cz);
-          if (r2 > rc2) {
-            ++my_far;
-            my_terms += nkeep;
-            if constexpr (MIXED) {
-              const float hn = rsqrtf((float)r2);
-              vk[p] += (double)multipole<float>(mv, lmx, hn * (float)(x - cx), hn * (float)(y - cy),
-                                                hn * (float)(z - cz), hn);
-            } else {
-              const double hn = 1.0 / sqrt(r2);
-              vk[p] += multipole<double>(mv, lmx, hn * (x - cx), hn * (y - cy), hn * (z - cz), hn);
-            }
-          }
+        unsigned long long nf = 0;
+        switch (S.lmax[k]) {
+#define FAR_CASE(L)                                                                          \
+  case L:                                                                                    \
+    far_points<PT, L>(mv, S.px, S.py, S.pz, np, cx, cy, cz, rc2, vk, lane, nf); \
+    break;
+          FAR_CASE(0)
+          FAR_CASE(1)
+          FAR_CASE(2)
+          FAR_CASE(3)
+          FAR_CASE(4)
+          FAR_CASE(5)
+          default: FAR_CASE(6)
+#undef FAR_CASE
         }
+        my_far += nf;
+        my_terms += nf * (unsigned long long)S.nkeep[k];
       }
     }
   }
@@ -790,8 +822,8 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
   k_call_lists<<<1, LIST_THREADS, 0, st>>>(ncalls, per_fo_only ? 1 : 0, scr.share, scr.lists);
   if (!per_fo_only && mixed) {
     const size_t nc = (size_t)npairs * nfo * COEF_LD, nm = (size_t)ncalls * nfo * MOM_LD;
-    launch_split_tf32(nc, coef, scr.coef_hl, st);
-    launch_split_tf32(nm, momv, scr.momv_hl, st);
+    launch_split_tf32((size_t)npairs, nfo, coef, scr.coef_hl, st);
+    launch_split_tf32((size_t)ncalls, nfo, momv, scr.momv_hl, st);
     launch_coulomb_shared_tc(ncalls, scr.lists, scr.share, calls, nfo, scr.coef_hl, nc, scr.pair_fmt, pairs,
                              scr.momv_hl, nm, M, boys_tab, vh, ldv, cnt, scr.err, st);
   } else if (!per_fo_only) {

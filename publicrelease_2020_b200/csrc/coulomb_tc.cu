@@ -12,31 +12,35 @@
 // 32-row windows the FP32 accumulator is folded into a hi/lo FP32 pair, also in
 // tensor memory, by an error-free two-sum; the pair is summed in FP64 at the end.
 //
-// One CTA per tile of 128 points and block of 128 FOs, 384 threads:
+// One CTA per tile of 128 points and block of 128 FOs, 512 threads:
 //   warp 0       allocates tensor memory; lane 0 issues the MMAs
 //   warps 4-7    epilogue: tensor-memory lanes 0-127 (= FO rows)
-//   warps 8-11   producers: stage the calls 128 at a time in shared memory
-//                (one coalesced load each, tile class computed once), then
-//                walk them; one point each for the B rows, one FO row each for
-//                the cp.async of the A rows
+//   warps 8-15   producers, two per point: stage the calls 128 at a time in
+//                shared memory (one coalesced load each, tile class computed
+//                once), then walk them; both producers of a point follow the
+//                operand windows, the owner of each segment (alternating)
+//                writes its B rows (its point) and copies its A rows (FO pt)
 // Operand windows (32 K rows; hi and lo parts of A and B; 64 KB) are triple
 // buffered in shared memory in the no-swizzle K-major core-matrix layout (8 rows
 // x 16 bytes per core matrix).  Hand-over: mbarriers full/empty per window
-// buffer, accfull/accempty per accumulator, done at the end of the tile; every
+// buffer (the A-row copies complete on it by cp.async.mbarrier.arrive, so no
+// producer waits for its own copies), accfull/accempty per accumulator, done at
+// the end of the tile; every
 // wait has an iteration limit after which the CTA sets an abort flag, drains its
 // copies and MMAs, frees tensor memory and returns with an error flag set.
 #include "coulomb_common.cuh"
 
 namespace flosic {
 
-constexpr int TC_THREADS = 384;
+constexpr int TC_THREADS = 512;
 constexpr int TC_KW = 32;                // K rows per operand window
 constexpr int TC_KG = TC_KW / 4;         // core matrices along K
 constexpr int TC_NB = 3;                 // window buffers
 constexpr int TC_FLUSH = 2;              // windows per FP32 accumulation group
 constexpr int TC_EPI0 = 4;               // first epilogue warp
 constexpr int TC_PROD0 = 8;              // first producer warp
-constexpr int TC_NPROD = 128;            // producer threads
+constexpr int TC_NPROD = 256;            // producer threads: two per point, alternate segments
+constexpr int TC_NSTAGE = 128;           // calls staged per chunk
 constexpr int TC_BAR_PROD = 5;           // named barrier of the producer warps
 constexpr uint32_t TC_TMEM_COLS = 512;   // D0 | D1 | V_hi | V_lo, 128 columns each
 constexpr long TC_SPIN_LIMIT = 1L << 25;
@@ -52,7 +56,7 @@ struct TcSmem {
   float A[TC_NB][2][TILE * TC_KW];  // [buffer][hi, lo] FO rows x K
   float B[TC_NB][2][TILE * TC_KW];  // [buffer][hi, lo] point rows x K
   double px[TILE], py[TILE], pz[TILE];
-  TcCall calls[TC_NPROD];
+  TcCall calls[TC_NSTAGE];
   uint64_t full[TC_NB], empty[TC_NB], accfull[2], accempty[2], done, drain;
   int win_rows[TC_NB], win_last[TC_NB];
   int ngroups;
@@ -102,6 +106,12 @@ __device__ __forceinline__ bool mbar_wait_drain(uint64_t* b, uint32_t parity) {
     if ((it & 255) == 255) __nanosleep(128);
   }
   return false;
+}
+
+// Arrive on b once every cp.async this thread has issued so far has landed
+// (the barrier's expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive(uint64_t* b) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(b)) : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -239,18 +249,31 @@ __device__ __forceinline__ void g_values(float (&v)[KSEG], double Cx, double Cy,
   for (int t = 46; t < KSEG; ++t) v[t] = 0.f;
 }
 
-// H column values (harmonics / r^(l+1) in moment row order) of one far point,
-// zero above (lmx+1)^2.
-__device__ __forceinline__ void h_values(float (&v)[KSEG], int kf, float dx, float dy, float dz, float r2) {
+// H column values (harmonics / r^(l+1) in moment row order) of one far point
+// up to degree LMX, zero up to the next multiple of 4 rows.
+template <int LMX>
+__device__ __forceinline__ void h_values(float (&v)[KSEG], float dx, float dy, float dz, float r2) {
+  constexpr int NR = (LMX + 1) * (LMX + 1), NR4 = (NR + 3) / 4 * 4;
   const float hn = rsqrtf(r2);
-  const int lmx = far_degree(kf);
-  float rec[LM + 1];
+  float rec[LMX + 1];
   rec[0] = hn;
 #pragma unroll
-  for (int l = 1; l <= LM; ++l) rec[l] = rec[l - 1] * hn;
+  for (int l = 1; l <= LMX; ++l) rec[l] = rec[l - 1] * hn;
+  harmonics_mmajor<float>(hn * dx, hn * dy, hn * dz, LMX, [&](int row, int l, float h) { v[row] = h * rec[l]; });
 #pragma unroll
-  for (int t = 0; t < KSEG; ++t) v[t] = 0.f;
-  harmonics_mmajor<float>(hn * dx, hn * dy, hn * dz, lmx, [&](int row, int l, float h) { v[row] = h * rec[l]; });
+  for (int t = NR; t < NR4; ++t) v[t] = 0.f;
+}
+
+// Dispatch on the moment rows kf = ((lmax + 1)^2 rounded up to 4).
+__device__ __forceinline__ void h_values_kf(float (&v)[KSEG], int kf, float dx, float dy, float dz, float r2) {
+  switch (kf) {
+    case 4: h_values<1>(v, dx, dy, dz, r2); break;
+    case 12: h_values<2>(v, dx, dy, dz, r2); break;
+    case 16: h_values<3>(v, dx, dy, dz, r2); break;
+    case 28: h_values<4>(v, dx, dy, dz, r2); break;
+    case 36: h_values<5>(v, dx, dy, dz, r2); break;
+    default: h_values<6>(v, dx, dy, dz, r2); break;
+  }
 }
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
@@ -277,7 +300,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
   }
   if (tid == 0) {
     for (int b = 0; b < TC_NB; ++b) {
-      mbar_init(&S.full[b], TC_NPROD);
+      mbar_init(&S.full[b], 2 * TC_NPROD);  // per producer: its stores, and its cp.async copies
       mbar_init(&S.empty[b], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -304,7 +327,8 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
 
   if (warp >= TC_PROD0) {
     // ---------------- producers
-    const int pt = tid - TC_PROD0 * 32;  // point p = pt, and A row (FO) pt
+    const int pt = (tid - TC_PROD0 * 32) & (TILE - 1);  // point p = pt, and A row (FO) pt
+    const int half = (tid - TC_PROD0 * 32) >> 7;       // owns segments with (index & 1) == half
     const int p = pt;
     const bool count_terms = blockIdx.y == 0;  // kept terms are summed over all FOs once per (call, point)
     const int nsh = lists[2 * ncalls];
@@ -323,18 +347,22 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
       open = true;
     };
     auto win_close = [&](int rows, int last) {
-      cp_async_wait_all();
+      // the thread's own st.shared become visible to the tensor core (async
+      // proxy); its cp.async copies arrive on the barrier when they land
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      if (pt == 0) {
+      if (pt == 0 && half == 0) {
         S.win_rows[buf] = rows;
         S.win_last[buf] = last;
       }
+      cp_async_arrive(&S.full[buf]);
       mbar_arrive(&S.full[buf]);
       ++w;
       open = false;
     };
-    // one segment: B rows of this point (v, rows) and A rows of FO pt from src
-    auto emit = [&](const float (&v)[KSEG], int rows, const float* src, size_t part) {
+    // one segment: B rows of this point (v, rows; zeros when !live) and A rows
+    // of FO pt from src
+    const size_t cstride = (size_t)nfo * 4;  // floats between the 4-row chunks of one A row
+    auto emit = [&](const float (&v)[KSEG], bool mine, bool live, int rows, const float* src, size_t part) {
 #pragma unroll
       for (int j4 = 0; j4 < KSEG / 4; ++j4) {
         if (4 * j4 >= rows || !ok) break;
@@ -342,31 +370,35 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
           win_open();
           if (!ok) break;
         }
-        float h4[4], l4[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) tf32_split(v[4 * j4 + e], h4[e], l4[e]);
         const int o = cm_off(p, fill);
-        *reinterpret_cast<float4*>(&S.B[buf][0][o]) = make_float4(h4[0], h4[1], h4[2], h4[3]);
-        *reinterpret_cast<float4*>(&S.B[buf][1][o]) = make_float4(l4[0], l4[1], l4[2], l4[3]);
-        if (src) {
+        if (!mine) {
+          // the other producer of this point writes this segment
+        } else if (live) {
+          float h4[4], l4[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) tf32_split(v[4 * j4 + e], h4[e], l4[e]);
+          *reinterpret_cast<float4*>(&S.B[buf][0][o]) = make_float4(h4[0], h4[1], h4[2], h4[3]);
+          *reinterpret_cast<float4*>(&S.B[buf][1][o]) = make_float4(l4[0], l4[1], l4[2], l4[3]);
+        } else {
+          *reinterpret_cast<float4*>(&S.B[buf][0][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
+          *reinterpret_cast<float4*>(&S.B[buf][1][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (mine && src) {
           const int oa = cm_off(pt, fill);
-          cp_async16(&S.A[buf][0][oa], src + 4 * j4);
-          cp_async16(&S.A[buf][1][oa], src + part + 4 * j4);
+          cp_async16(&S.A[buf][0][oa], src + j4 * cstride);
+          cp_async16(&S.A[buf][1][oa], src + part + j4 * cstride);
         }
         fill += 4;
-        if (fill == TC_KW) {
-          cp_async_commit();
-          win_close(TC_KW, 0);
-        }
+        if (fill == TC_KW) win_close(TC_KW, 0);
       }
-      cp_async_commit();
     };
     // Every producer takes the same sequence of named-barrier steps (the chunk
     // loop does not depend on ok); only the work inside is skipped after an abort.
-    for (int li0 = 0; li0 < nsh; li0 += TC_NPROD) {
-      const int nchunk = min(TC_NPROD, nsh - li0);
+    int seg = 0;  // index of the next segment that writes rows
+    for (int li0 = 0; li0 < nsh; li0 += TC_NSTAGE) {
+      const int nchunk = min(TC_NSTAGE, nsh - li0);
       producer_sync();  // the previous chunk has been walked by every producer
-      if (pt < nchunk) {
+      if (half == 0 && pt < nchunk) {
         TcCall e;
         e.c = lists[li0 + pt];
         const CallShare sh = share[e.c];
@@ -397,7 +429,8 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
           for (int qi = 0; qi < e.np && ok; ++qi) {
             const int q = e.p0 + qi;
             const int kn = near_rows(qi == 0 ? e.fmt : pair_fmt[q]);
-            bool nr = p < np;
+            const bool mine = (seg++ & 1) == half;
+            bool nr = mine && p < np;
             if (nr && e.cls == 2) nr = !(sqdist_rn2(x, y, z, e.cx, e.cy, e.cz) > e.rc2);
             if (nr) {
               ++my_near;
@@ -407,34 +440,28 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
                 const PairGeo& pg = pairs[q];
                 g_values(v, pg.C[0], pg.C[1], pg.C[2], pg.delta, x, y, z, kn, boys_tab);
               }
-            } else {
-#pragma unroll
-              for (int t = 0; t < KSEG; ++t) v[t] = 0.f;
             }
-            const float* src = pt < nk ? coef_hl + ((size_t)q * nfo + k0 + pt) * COEF_LD : nullptr;
-            emit(v, kn, src, coef_part);
+            const float* src = pt < nk ? coef_hl + ((size_t)q * (KSEG / 4) * nfo + k0 + pt) * 4 : nullptr;
+            emit(v, mine, nr, kn, src, coef_part);
           }
         }
         if (e.cls != 0) {  // far segment (NPOT=2)
-          double r2 = 0.0;
-          bool fr = p < np;
-          if (fr) {
-            r2 = sqdist_rn2(x, y, z, e.cx, e.cy, e.cz);
-            if (e.cls == 2) fr = r2 > e.rc2;
-          }
+          // near/far of a point on a boundary tile is decided in FP64, as in the
+          // reference; the harmonics use the FP32 offset
+          const bool mine = e.kf > 0 ? (seg++ & 1) == half : half == 0;
+          bool fr = mine && p < np;
+          if (fr && e.cls == 2) fr = sqdist_rn2(x, y, z, e.cx, e.cy, e.cz) > e.rc2;
           if (fr) {
             ++my_far;
             if (count_terms) my_terms += (unsigned long long)e.ksum;
           }
           if (e.kf > 0) {
             if (fr) {
-              h_values(v, e.kf, (float)(x - e.cx), (float)(y - e.cy), (float)(z - e.cz), (float)r2);
-            } else {
-#pragma unroll
-              for (int t = 0; t < KSEG; ++t) v[t] = 0.f;
+              const float dx = (float)(x - e.cx), dy = (float)(y - e.cy), dz = (float)(z - e.cz);
+              h_values_kf(v, e.kf, dx, dy, dz, dx * dx + dy * dy + dz * dz);
             }
-            const float* src = pt < nk ? momv_hl + ((size_t)e.c * nfo + k0 + pt) * MOM_LD : nullptr;
-            emit(v, e.kf, src, mom_part);
+            const float* src = pt < nk ? momv_hl + ((size_t)e.c * (KSEG / 4) * nfo + k0 + pt) * 4 : nullptr;
+            emit(v, mine, fr, e.kf, src, mom_part);
           }
         }
       }
@@ -445,18 +472,20 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
         if (ok) win_close(0, 1);
       } else {
         if (fill & 7) {  // pad the last k-step of 8 rows with zeros
+          if (half == 0) {
           const int o = cm_off(p, fill);
           *reinterpret_cast<float4*>(&S.B[buf][0][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
           *reinterpret_cast<float4*>(&S.B[buf][1][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
           const int oa = cm_off(pt, fill);
           *reinterpret_cast<float4*>(&S.A[buf][0][oa]) = make_float4(0.f, 0.f, 0.f, 0.f);
           *reinterpret_cast<float4*>(&S.A[buf][1][oa]) = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
           fill += 4;
         }
         win_close(fill, 1);
       }
     }
-    cp_async_wait_all();
+    asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy of this thread is left in flight
   } else if (warp == 0) {
     // ---------------- MMA issue
     if (lane == 0) {
@@ -466,6 +495,8 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
       for (int w = 0;; ++w) {
         const int b = w % TC_NB;
         if (!mbar_wait(&S.full[b], (uint32_t)((w / TC_NB) & 1), abort)) break;
+        // the window's cp.async data (generic proxy) is read by the tensor core
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         tc_fence_after();
         const int r = S.win_rows[b], last = S.win_last[b];
         if (r > 0) {
@@ -582,14 +613,22 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
   count_add(cnt, my_near * (unsigned long long)nk, my_far * (unsigned long long)nk, my_terms);
 }
 
-// hi/lo TF32 split of n doubles: out[i] = hi, out[part + i] = lo.
-__global__ void k_split_tf32(size_t n, const double* __restrict__ src, float* __restrict__ out, size_t part) {
+// hi/lo TF32 split of rows [nrow][nfo][KSEG] doubles into the chunk-major
+// layout the producers copy from, [nrow][KSEG/4][nfo][4] floats (hi at out,
+// lo at out + part): the 128 FOs' values of one 4-row chunk are contiguous, so
+// a warp's copies of a chunk are coalesced.
+__global__ void k_split_tf32(size_t nrow, int nfo, const double* __restrict__ src, float* __restrict__ out,
+                             size_t part) {
+  const size_t n = nrow * nfo * KSEG;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / ((size_t)nfo * KSEG);
+    const int k = (int)((i / KSEG) % nfo), t = (int)(i % KSEG);
     const double x = src[i];
     const float hi = tf32_round((float)x);
     const float lo = tf32_round((float)(x - (double)hi));
-    out[i] = hi;
-    out[part + i] = lo;
+    const size_t o = ((r * (KSEG / 4) + t / 4) * nfo + k) * 4 + (t & 3);
+    out[o] = hi;
+    out[part + o] = lo;
   }
 }
 
@@ -597,10 +636,11 @@ void init_coulomb_tc() {
   cudaFuncSetAttribute(k_coulomb_shared_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem));
 }
 
-void launch_split_tf32(size_t n, const double* src, float* out, cudaStream_t st) {
+void launch_split_tf32(size_t nrow, int nfo, const double* src, float* out, cudaStream_t st) {
+  const size_t n = nrow * nfo * KSEG;
   if (n == 0) return;
   const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
-  k_split_tf32<<<blocks, 256, 0, st>>>(n, src, out, n);
+  k_split_tf32<<<blocks, 256, 0, st>>>(nrow, nfo, src, out, n);
 }
 
 void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,

@@ -72,8 +72,9 @@ struct CoulombScratch {
 };
 void init_coulomb_mma();
 void init_coulomb_tc();
-// TF32 hi/lo split of n doubles: out[i] = hi, out[n + i] = lo.
-void launch_split_tf32(size_t n, const double* src, float* out, cudaStream_t st);
+// TF32 hi/lo split of nrow x nfo rows of KSEG doubles into the chunk-major
+// [nrow][KSEG/4][nfo][4] layout (hi, then lo at + nrow*nfo*KSEG floats).
+void launch_split_tf32(size_t nrow, int nfo, const double* src, float* out, cudaStream_t st);
 // Mixed-precision shared-geometry Coulomb GEMM on tcgen05 (csrc/coulomb_tc.cu).
 void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
                               const float* coef_hl, size_t coef_part, const int8_t* pair_fmt, const PairGeo* pairs,

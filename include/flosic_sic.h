@@ -61,7 +61,8 @@ const char* flosic_sic_last_error(void);
      N_CON(3,ntypes) RMSH(3,nmsh) WMSH(nmsh)
    Functional: IGGA(2), IDFTYP(2) as set by SETDFTYP (setdftyp.F:61-105);
    supported: exchange PW91/PBE/revPBE/RPBE (LDA via IGGA=0), correlation
-   PW91/PBE.  nspn = NSPN of the run (1 or 2). */
+   PW91/PBE, and SCAN for both (IGGA=3, IDFTYP=11, "MGGA-SCAN*MGGA-SCAN").
+   nspn = NSPN of the run (1 or 2). */
 int flosic_sic_set_geometry(flosic_ctx* ctx, int natoms, const int32_t* atom_type, const double* rat,
                             int ntypes, const int32_t* n_bare, const double* bfalp,
                             const int32_t* n_con, const double* bfcon, int nmsh, const double* rmsh,
@@ -94,6 +95,17 @@ int flosic_sic_coupot_sic(flosic_ctx* ctx, int kxxs, int kxxo, double* coulomb, 
 /* GETVLXC(NDIM,RHOG,VXC,VLO,.false.,...) SIC branch -- getvlxc.F:8 with NSPN=2
    (apotnl_sic.F:419): VXC(2*ndim) and ERGXL,ERGXN,ERGCL,ERGCN in ergs[4]. */
 int flosic_sic_getvlxc(flosic_ctx* ctx, int ndim, const double* rhog, double* vxc, double* ergs);
+
+/* GETVLXC meta-GGA branch (SCAN) -- getvlxc.F:8 with subvlxc_libxc.F90:150-157,
+   293-440 and call_mgga.f90: the caller passes TAU(ndim), the FO's kinetic
+   energy density |grad phi|^2/2 that GETTAU_PAR (gettau_par.f90) forms from
+   the FO coefficients, with RHOG(ndim,10) (channels 1-4 read).  Returns the
+   local potential VXC(2*ndim), the Hamiltonian ingredients MIXIN(4,2*ndim)
+   (the MGGA#### record: dE/d|grad rho| along grad rho, and dE/dtau / 2) and
+   ERGXL,ERGXN,ERGCL,ERGCN.  flosic_sic_getvlxc returns FLOSIC_ERR_ARG for a
+   meta-GGA context. */
+int flosic_sic_getvlxc_mgga(flosic_ctx* ctx, int ndim, const double* rhog, const double* tau, double* vxc,
+                            double* mixin, double* ergs);
 
 /* Precision of the SIC path (no counterpart in the reference).
    FLOSIC_PRECISION_FP64 (default) is the drop-in: every step in FP64.
@@ -129,7 +141,8 @@ int flosic_sic_apotnl_sic(flosic_ctx* ctx, double* totqnum, int lspx, int iorbx,
 
 /* SICLAGM(LSPN) -- frmorb_mpi.F:2: SIC(ld,ld) = -<phi_j|V_l|phi_l> from the
    potentials of the FOs of spin lspn (kept in GPU memory instead of the
-   ZPOT#### files). */
+   ZPOT#### files); for SCAN also the gradient terms of frmorb_mpi.F:440-509
+   with each FO's MIXIN (kept in GPU memory instead of the MGGA#### files). */
 int flosic_sic_siclagm(flosic_ctx* ctx, int lspn, double* sic, int ld);
 
 /* FRMORB2(-LSPN,-1) -- frmorb2.F:586-717: FOD forces DEBDAX(3,ld) from SIC(ld,ld). */

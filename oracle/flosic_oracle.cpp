@@ -114,6 +114,12 @@ struct Problem {
   }
   double alp(int t, int ib) const { return bfalp[(size_t)t * MAX_BARE + ib]; }
   bool gga() const { return igga[0] > 0 || igga[1] > 0; }
+  bool mgga() const { return igga[0] >= 3 || igga[1] >= 3; }
+  // Test knob: evaluate XC on the untruncated pair-route density (every point
+  // near, as phi^2) while the Coulomb potential keeps the reference's near/far
+  // split.  Isolates the reference's density truncation at far points, which a
+  // meta-GGA amplifies in the density tails through alpha.
+  bool xc_exact_density = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -1662,10 +1668,288 @@ void pbecor(double rs, double zet, double t, double uu, double vv, double ww, do
   dvcdn = comm - pref;
 }
 
+// ---------------------------------------------------------------------------
+// SCAN meta-GGA (scan.f, the form called by call_mgga.f90 for IDFTYP=11).
+// Energies are per particle; the derivatives are those of rho*e with respect
+// to rho, |grad rho| and tau, as the reference returns them.
+// ---------------------------------------------------------------------------
+// Exchange enhancement factor Fx(p, alpha) and its first derivatives
+// (metaggafx, scan.f:304-470; the second derivatives there are unused).
+void scan_fx(double p, double a, double& fx, double& fx_p, double& fx_a) {
+  const double K1 = 0.065, C1 = 0.667, C2 = 0.800, D1 = 1.240;
+  const double K0 = 0.1740, A1 = 4.9479, MU = 10.0 / 81.0, B1 = 0.156632, B2 = 0.12083, B3 = 0.5;
+  const double oma = 1.0 - a, oma2 = oma * oma;
+  const double hx0 = 1.0 + K0;
+  const double b4 = MU * MU / K1 - 0.112654;
+  double wfac, dwfac;
+  if (b4 > 0.0) {
+    const double e = std::exp(-b4 * p / MU);
+    wfac = b4 * p * p * e;
+    dwfac = b4 * p * e * (2.0 - b4 * p / MU);
+  } else {
+    const double e = std::exp(b4 * p / MU);
+    wfac = b4 * p * p * e;
+    dwfac = b4 * p * e * (2.0 + b4 * p / MU);
+  }
+  const double ea = std::exp(-B3 * oma2);
+  const double vfac = B1 * p + B2 * oma * ea;
+  const double yfac = MU * p + wfac + vfac * vfac;
+  const double den = 1.0 + yfac / K1;
+  const double hx1 = 1.0 + K1 - K1 / den;
+  double fa = 0.0, dfa = 0.0;
+  if (a < 1.0) {
+    fa = std::exp(-C1 * a / oma);
+    dfa = -C1 * std::exp(-C1 * a / oma) / (oma * oma);
+  } else if (a > 1.0) {
+    fa = -D1 * std::exp(C2 / oma);
+    dfa = -C2 * D1 * std::exp(C2 / oma) / (oma * oma);
+  }
+  double gx = 1.0, dgx = 0.0;
+  if (p > 0.0) {
+    const double p14 = std::pow(p, 0.25);
+    gx = 1.0 - std::exp(-A1 / p14);
+    dgx = -A1 / 4.0 / p / p14 * std::exp(-A1 / p14);
+  }
+  const double fx1 = hx1 + fa * (hx0 - hx1);
+  fx = fx1 * gx;
+  const double dhx1_dp = (MU + dwfac + 2.0 * vfac * B1) / (den * den);
+  const double dvfac_da = -B2 * (1.0 - 2.0 * B3 * oma2) * ea;
+  const double dhx1_da = 2.0 * vfac * dvfac_da / (den * den);
+  const double dfx1_dp = dhx1_dp + fa * (0.0 - dhx1_dp);
+  const double dfx1_da = (1.0 - fa) * dhx1_da + dfa * (hx0 - hx1);
+  fx_p = dfx1_dp * gx + fx1 * dgx;
+  fx_a = dfx1_da * gx;
+}
+
+// Spin-unpolarised SCAN exchange (VSCANxUNP, scan.f:172-287) at density rho,
+// |grad rho| = drho, kinetic energy density tau.  The reference's pi here is
+// the literal 3.1415927.
+void scan_x_unp(double rho, double drho, double tau, double& ex, double& vx, double& vxdd, double& amux) {
+  const double PI = 3.1415927, PISQ = PI * PI;
+  const double AX = -0.7385587663820224058842300326808360;
+  const double TH = 1.0 / 3.0, TH2 = 2.0 * TH, TH4 = 4.0 * TH, TH5 = 1.0 + TH2, TH8 = 1.0 + TH5;
+  const double tauw = drho * drho / rho / 8.0;
+  const double exunif = AX * std::pow(rho, TH);
+  const double exlda = exunif * rho;
+  const double exdlda = exunif * TH4;
+  const double c3p = std::pow(3.0 * PISQ, TH2);
+  const double p = drho * drho / (4.0 * c3p * std::pow(rho, TH8));
+  const double tunif = 3.0 / 10.0 * std::pow(3.0 * PI * PI, TH2) * std::pow(rho, TH5);
+  const double alpha = (tau - tauw) / tunif;
+  const double dpd = -TH8 * p / rho;
+  const double dpdd = 2.0 * p / drho;
+  const double dad = -tau * std::pow(3.0 * PI * PI * rho, TH2) / (2.0 * tunif * tunif) +
+                     drho * drho / std::pow(rho, 11.0 / 3.0) * (10.0 / 9.0 / std::pow(3.0 * PI * PI, TH2));
+  const double dadd = -drho / (4.0 * rho * tunif);
+  const double dadt = 1.0 / tunif;
+  double fx, fxp, fxa;
+  scan_fx(p, alpha, fx, fxp, fxa);
+  vx = exdlda * fx + exlda * (fxp * dpd + fxa * dad);
+  vxdd = exlda * (fxp * dpdd + fxa * dadd);
+  amux = exlda * (fxa * dadt);
+  ex = exunif * fx;
+}
+
+// GCOR22 (scan.f:1155-1166): PW92 interpolation and its rs derivative.
+void scan_gcor(double A, double A1, double B1, double B2, double B3, double B4, double rtrs, double& gg,
+               double& ggrs) {
+  const double q0 = -2.0 * A * (1.0 + A1 * rtrs * rtrs);
+  const double q1 = 2.0 * A * rtrs * (B1 + rtrs * (B2 + rtrs * (B3 + B4 * rtrs)));
+  const double q2 = std::log(1.0 + 1.0 / q1);
+  gg = q0 * q2;
+  const double q3 = A * (B1 / rtrs + 2.0 * B2 + rtrs * (3.0 * B3 + 4.0 * B4 * rtrs));
+  ggrs = -2.0 * A * A1 * q2 - q0 * q3 / (q1 * (1.0 + q1));
+}
+
+// PW92 LSD correlation and its spin potentials (the LSD part of
+// CORPBE_revtpss, scan.f:700-790).
+void scan_lsd(double rs, double zet, double& ec, double& vcup, double& vcdn) {
+  const double TH = 1.0 / 3.0, TH4 = 4.0 * TH;
+  const double GAM = 0.51984209978974632953442121455650, FZZ = 8.0 / (9.0 * GAM);
+  const double rtrs = std::sqrt(rs);
+  double eu, eurs, ep, eprs, alfm, alfrsm;
+  scan_gcor(0.03109070, 0.213700, 7.59570, 3.58760, 1.63820, 0.492940, rtrs, eu, eurs);
+  scan_gcor(0.015545350, 0.205480, 14.11890, 6.19770, 3.36620, 0.625170, rtrs, ep, eprs);
+  scan_gcor(0.01688690, 0.111250, 10.3570, 3.62310, 0.880260, 0.496710, rtrs, alfm, alfrsm);
+  const double z4 = zet * zet * zet * zet;
+  const double f = (std::pow(1.0 + zet, TH4) + std::pow(1.0 - zet, TH4) - 2.0) / GAM;
+  ec = eu * (1.0 - f * z4) + ep * f * z4 - alfm * f * (1.0 - z4) / FZZ;
+  const double ecrs = eurs * (1.0 - f * z4) + eprs * f * z4 - alfrsm * f * (1.0 - z4) / FZZ;
+  const double fz = TH4 * (std::pow(1.0 + zet, TH) - std::pow(1.0 - zet, TH)) / GAM;
+  const double eczet =
+      4.0 * (zet * zet * zet) * f * (ep - eu + alfm / FZZ) + fz * (z4 * ep - z4 * eu - (1.0 - z4) * alfm / FZZ);
+  const double comm = ec - rs * ecrs / 3.0 - zet * eczet;
+  vcup = comm + eczet;
+  vcdn = comm - eczet;
+}
+
+// Common spin/density variables of CORGGA_0 and CORGGA_1.
+struct ScanSpin {
+  double rt, yc, zeta, dz1, dz2, rs, drs, s, ds;
+};
+ScanSpin scan_spin(double ru, double rd, double dru, double drd, double drt) {
+  const double PI = 3.141592653589793238, PISQ = PI * PI, TH = 1.0 / 3.0, TH4 = 4.0 * TH;
+  ScanSpin v;
+  v.rt = ru + rd;
+  v.yc = (drt * drt - dru * dru - drd * drd) / 2.0;
+  v.zeta = std::min(std::max((ru - rd) / v.rt, -0.99999999999990), 0.99999999999990);
+  v.dz1 = 2.0 * rd / (v.rt * v.rt);
+  v.dz2 = -2.0 * ru / (v.rt * v.rt);
+  const double dthrd = std::exp(std::log(v.rt) * TH);
+  v.rs = std::pow(0.750 / PI, TH) / dthrd;
+  v.drs = -TH / v.rt * v.rs;
+  v.s = drt / (2.0 * std::pow(3.0 * PISQ, TH) * std::pow(v.rt, TH4));
+  v.ds = -TH4 * v.s / v.rt;
+  return v;
+}
+
+// epsilon_c^1: the PBE-like correlation of SCAN (CORGGA_1, scan.f:841-1000).
+// out[0] energy per particle, out[1..2] d/d rho_up,dn, out[3..4] d/d |grad rho_up,dn|.
+void scan_c1(double ru, double rd, double dru, double drd, double drt, double out[5]) {
+  const double PI = 3.141592653589793238, TH = 1.0 / 3.0;
+  const double GAMMA = 0.031090690869654895034940863712730, BETA_MB = 0.066724550603149220;
+  const ScanSpin v = scan_spin(ru, rd, dru, drd, drt);
+  const double zeta = v.zeta, rs = v.rs;
+  const double phi = (std::exp((2.0 * TH) * std::log(1.0 + zeta)) + std::exp((2.0 * TH) * std::log(1.0 - zeta))) / 2.0;
+  const double dphi = TH * (std::pow(1.0 + zeta, -TH) - std::pow(1.0 - zeta, -TH));
+  const double afix = std::sqrt(PI / 4.0) * std::pow(9.0 * PI / 4.0, 1.0 / 6.0);
+  const double gngnu = 1.0 / (2.0 * drt) * (2.0 * dru + 2.0 * v.yc / dru);
+  const double gngnd = 1.0 / (2.0 * drt) * (2.0 * drd + 2.0 * v.yc / drd);
+  const double dsdd1 = v.s / drt * gngnu, dsdd2 = v.s / drt * gngnd;
+  const double t = afix * v.s / std::sqrt(rs) / phi;
+  const double t2 = t * t;
+  const double den_t = phi * phi * std::pow(rs, 1.5);
+  const double dtd1 = afix * (phi * rs * v.ds - 0.5 * v.s * phi * v.drs - v.s * rs * dphi * v.dz1) / den_t;
+  const double dtd2 = afix * (phi * rs * v.ds - 0.5 * v.s * phi * v.drs - v.s * rs * dphi * v.dz2) / den_t;
+  const double dtdd1 = afix * dsdd1 / (std::sqrt(rs) * phi), dtdd2 = afix * dsdd2 / (std::sqrt(rs) * phi);
+  double ec, vu, vd;
+  scan_lsd(rs, zeta, ec, vu, vd);
+  const double dec_dz = (vu - vd) / 2.0;
+  const double dec_drs = (ec - zeta * dec_dz - (vu + vd) / 2.0) * 3.0 / rs;
+  const double bnum = 1.0 + 0.10 * rs, bden = 1.0 + 0.17780 * rs;
+  const double beta = BETA_MB * bnum / bden;
+  const double dbeta = BETA_MB * (bden * 0.10 - bnum * 0.17780) / (bden * bden);
+  const double phi3 = phi * phi * phi;
+  const double w = std::exp(-ec / (phi3 * GAMMA)) - 1.0;
+  const double dw_drs = -(w + 1.0) * dec_drs / (GAMMA * phi3);
+  const double dw_dz = -(w + 1.0) / (GAMMA * phi3) * (dec_dz - 3.0 * ec * dphi / phi);
+  const double A = beta / (GAMMA * w);
+  const double dA_drs = (w * dbeta - beta * dw_drs) / (GAMMA * w * w);
+  const double dA_dz = -beta * dw_dz / (GAMMA * w * w);
+  const double V = A * t2;
+  const double dV_drs = t2 * dA_drs, dV_dz = t2 * dA_dz, dV_dt = 2.0 * A * t;
+  const double g = 1.0 / std::pow(1.0 + 4.0 * V, 0.250);
+  const double dg_dv = -1.0 / std::pow(1.0 + 4.0 * V, 1.250);
+  const double hcore = 1.0 + w * (1.0 - g);
+  const double ah = GAMMA * phi3;
+  const double h = ah * std::log(hcore);
+  const double dh1 = 1.0 - g, dh2 = w * dg_dv;
+  const double dh_drs = (dh1 * dw_drs - dh2 * dV_drs) * ah / hcore;
+  const double dh_dz = 3.0 * h * dphi / phi + (dh1 * dw_dz - dh2 * dV_dz) * ah / hcore;
+  const double dh_dt = (dh1 * 0.0 - dh2 * dV_dt) * ah / hcore;
+  out[0] = ec + h;
+  out[1] = dec_drs * v.drs + dec_dz * v.dz1 + dh_drs * v.drs + dh_dz * v.dz1 + dh_dt * dtd1;
+  out[2] = dec_drs * v.drs + dec_dz * v.dz2 + dh_drs * v.drs + dh_dz * v.dz2 + dh_dt * dtd2;
+  out[3] = dh_dt * dtdd1;
+  out[4] = dh_dt * dtdd2;
+}
+
+// epsilon_c^0: the single-orbital correlation of SCAN (CORGGA_0,
+// scan.f:1008-1150).  Clamps drt to 1e-100 like the reference, which passes the
+// clamped value on to CORGGA_1 (the returned drt).  Same outputs as scan_c1.
+void scan_c0(double ru, double rd, double dru, double drd, double& drt, double out[5]) {
+  const double B1 = 0.0285764, B2 = 0.0889, B3 = 0.125541, KAI = 0.12802585262625815;
+  const double TH = 1.0 / 3.0, TH4 = 4.0 * TH;
+  const ScanSpin v = scan_spin(ru, rd, dru, drd, drt);
+  const double zeta = v.zeta, rs = v.rs;
+  if (std::fabs(drt) < 1.0e-100) drt = 1.0e-100;
+  const double gngnu = 1.0 / (2.0 * drt) * (2.0 * dru + 2.0 * v.yc / dru);
+  const double gngnd = 1.0 / (2.0 * drt) * (2.0 * drd + 2.0 * v.yc / drd);
+  const double dsdd1 = v.s / drt * gngnu, dsdd2 = v.s / drt * gngnd;
+  const double rsh = std::sqrt(rs);
+  const double ec0 = -B1 / (1.0 + B2 * rsh + B3 * rs);
+  const double dec0 = (B3 + B2 / rsh / 2.0) * ec0 * ec0 / B1;
+  const double dx = (std::pow(1.0 + zeta, TH4) + std::pow(1.0 - zeta, TH4)) / 2.0;
+  const double ddx = 2.0 * (std::pow(1.0 + zeta, TH) - std::pow(1.0 - zeta, TH)) / 3.0;
+  const double z12 = std::pow(zeta, 12.0);
+  const double gc = (1.0 - 2.363 * (dx - 1.0)) * (1.0 - z12);
+  const double dgc = -(1.0 - 2.363 * (dx - 1.0)) * 12.0 * std::pow(zeta, 11.0) - 2.363 * ddx * (1.0 - z12);
+  const double w0 = std::exp(-ec0 / B1) - 1.0;
+  const double dw0 = -(w0 + 1.0) * dec0 / B1;
+  const double ginf = 1.0 / std::pow(1.0 + 4.0 * KAI * v.s * v.s, 0.25);
+  const double dginf = -2.0 * KAI * v.s * std::pow(ginf, 5.0);
+  const double hcore = 1.0 + w0 * (1.0 - ginf);
+  const double h0 = B1 * std::log(hcore);
+  const double dh0_drs = B1 * dw0 * (1.0 - ginf) / hcore;
+  const double dh0_ds = -B1 * w0 * dginf / hcore;
+  const double de_dz = (ec0 + h0) * dgc, de_drs = (dec0 + dh0_drs) * gc, de_ds = dh0_ds * gc;
+  out[0] = (ec0 + h0) * gc;
+  out[1] = de_dz * v.dz1 + de_drs * v.drs + de_ds * v.ds;
+  out[2] = de_dz * v.dz2 + de_drs * v.drs + de_ds * v.ds;
+  out[3] = de_ds * dsdd1;
+  out[4] = de_ds * dsdd2;
+}
+
+// SCAN correlation (VSCANc -> Vmetaggac, scan.f:486-697): ec per particle,
+// vc[0..1] d(rho ec)/d rho_up,dn, vcdd[0..1] d(rho ec)/d|grad rho_up,dn|,
+// amu d(rho ec)/d tau (the same for both spins).
+void scan_c(double ru, double rd, double dru, double drd, double drt, double tauu, double taud, double& ec,
+            double vc[2], double vcdd[2], double& amu) {
+  const double PI = 3.141592653589793238, PISQ = PI * PI, TH = 1.0 / 3.0, TH2 = 2.0 * TH, TH5 = 1.0 + TH2;
+  const double C1 = 0.640, C2 = 1.500, D1 = 0.700;
+  if (dru == 0.0) dru = 1.0e-100;
+  if (drd == 0.0) drd = 1.0e-100;
+  const double rt = ru + rd;
+  const double yc = (drt * drt - dru * dru - drd * drd) / 2.0;
+  const double tauw = 1.0 / 8.0 * (drt * drt / rt);
+  const double tau = tauu + taud;
+  const double zeta = std::min(std::max((ru - rd) / rt, -0.99999999999990), 0.99999999999990);
+  const double dsz = (std::pow(1.0 + zeta, TH5) + std::pow(1.0 - zeta, TH5)) / 2.0;
+  const double tau0 = 0.30 * std::pow(3.0 * PISQ, TH2) * std::pow(rt, TH5) * dsz;
+  const double alpha = (tau - tauw) / tau0;
+  const double dz1 = 2.0 * rd / (rt * rt), dz2 = -2.0 * ru / (rt * rt);
+  const double ddsz = TH5 * (std::pow(1.0 + zeta, TH2) - std::pow(1.0 - zeta, TH2)) / 2.0;
+  const double dtau0_1 = TH5 * tau0 / rt + tau0 * (ddsz * dz1) / dsz;
+  const double dtau0_2 = TH5 * tau0 / rt + tau0 * (ddsz * dz2) / dsz;
+  const double dtauw = -tauw / rt;
+  const double da1 = (-dtauw - alpha * dtau0_1) / tau0, da2 = (-dtauw - alpha * dtau0_2) / tau0;
+  const double dtauw_dd1 = 1.0 / 4.0 / rt * (dru + yc / dru);
+  const double dtauw_dd2 = 1.0 / 4.0 / rt * (drd + yc / drd);
+  const double dadd1 = -dtauw_dd1 / tau0, dadd2 = -dtauw_dd2 / tau0;
+  const double dat = 1.0 / tau0;
+  double f = 0.0, df = 0.0;
+  if (alpha < 1.0) {
+    f = std::exp(C1 * alpha / (alpha - 1.0));
+    df = -C1 * f / ((alpha - 1.0) * (alpha - 1.0));
+  } else if (alpha > 1.0) {
+    f = -D1 * std::exp(-C2 / (alpha - 1.0));
+    df = C2 * f / ((alpha - 1.0) * (alpha - 1.0));
+  }
+  double e0[5], e1[5];
+  scan_c0(ru, rd, dru, drd, drt, e0);
+  scan_c1(ru, rd, dru, drd, drt, e1);
+  const double dE = e0[0] - e1[0];
+  const double epp = e1[0] + f * dE;
+  const double d1 = e1[1] + dE * df * da1 + f * (e0[1] - e1[1]);
+  const double d2 = e1[2] + dE * df * da2 + f * (e0[2] - e1[2]);
+  const double dd1 = e1[3] + dE * df * dadd1 + f * (e0[3] - e1[3]);
+  const double dd2 = e1[4] + dE * df * dadd2 + f * (e0[4] - e1[4]);
+  const double dt = dE * df * dat;
+  vc[0] = epp + rt * d1;
+  vc[1] = epp + rt * d2;
+  vcdd[0] = rt * dd1;
+  vcdd[1] = rt * dd2;
+  amu = rt * dt;
+  ec = epp;
+}
+
 // SUBVLXC (subvlxc_libxc.F90:23-508, built-in functionals) for one point,
 // NSPN=2 layout: rht[ispn][10] with rht[0] the total and rht[1] the spin-down
-// density channels.  Adds to vxc[0..1] and the energy accumulators.
-void subvlxc_point(const Problem& P, double rht[2][10], double wgt, double* vxc, double* ex4) {
+// density channels.  Adds to vxc[0..1] and the energy accumulators.  SCAN
+// (IDFTYP 11) also takes the spin kinetic energy densities tau[0..1] and adds
+// the spin-up Hamiltonian ingredients MIXINS(1..4) (call_mgga.f90) to mixin.
+void subvlxc_point(const Problem& P, double rht[2][10], double wgt, double* vxc, double* ex4,
+                   const double* tau = nullptr, double* mixin = nullptr) {
   const int nspn = 2;
   const bool isgga = P.igga[0] >= 1 || P.igga[1] >= 1;
   const int ngrad = isgga ? 10 : 1;
@@ -1726,7 +2010,18 @@ void subvlxc_point(const Problem& P, double rht[2][10], double wgt, double* vxc,
           else U = 0.0;
         }
         double ex = 0, dex = 0, vx = 0;
-        if (P.idftyp[0] <= 6) pw91ex(dkf, S, U, V, ex, dex, vx);
+        if (P.idftyp[0] >= 11) {
+          // call_mgga_ex (call_mgga.f90:8-95) with NSPN=2; DEX is zero
+          const double dgrad = 2.0 * std::sqrt(dg2[s + 1]);
+          double vxdd, amux;
+          scan_x_unp(D, dgrad, 2.0 * tau[s], ex, vx, vxdd, amux);
+          double div = dgrad;
+          if (std::fabs(div) < 1.0e-100) div = 1.0e-100;
+          if (s == 0 && mixin) {
+            for (int d = 0; d < 3; ++d) mixin[d] = 2.0 * vxdd * (rht[0][1 + d] - rht[1][1 + d]) / div;
+            mixin[3] = amux * 0.5;
+          }
+        } else if (P.idftyp[0] <= 6) pw91ex(dkf, S, U, V, ex, dex, vx);
         else if (P.idftyp[0] == 7) pbeex(1, D, S, U, V, ex, dex, vx);
         else if (P.idftyp[0] == 8) pbeex(2, D, S, U, V, ex, dex, vx);
         else if (P.idftyp[0] == 9) pbeex(3, D, S, U, V, ex, dex, vx);
@@ -1765,7 +2060,19 @@ void subvlxc_point(const Problem& P, double rht[2][10], double wgt, double* vxc,
     else UU = 0.0;
   }
   double ec = 0, vcup = 0, vcdn = 0, dec = 0, dvcup = 0, dvcdn = 0;
-  if (P.idftyp[1] <= 5) {
+  if (P.idftyp[1] >= 11) {
+    // call_mgga_cor (call_mgga.f90:100-232), gradient branch, NSPN=2
+    double vc[2], vcdd[2], amu;
+    scan_c(dup, ddn, std::sqrt(dg2[1]), std::sqrt(dg2[2]), std::sqrt(dg2[0]), tau[0], tau[1], ec, vc, vcdd, amu);
+    vcup = vc[0];
+    vcdn = vc[1];
+    if (mixin) {
+      double div1 = dg2[1];
+      if (std::fabs(div1) < 1.0e-100) div1 = 1.0e-100;
+      for (int d = 0; d < 3; ++d) mixin[d] = mixin[d] + vcdd[0] * (rht[0][1 + d] - rht[1][1 + d]) / std::sqrt(div1);
+      mixin[3] = mixin[3] + amu * 0.5;
+    }
+  } else if (P.idftyp[1] <= 5) {
     return;  // LDACOR variants are outside the supported set (rejected at setup)
   } else if (P.idftyp[1] == 6) {
     PW91Gas gas;
@@ -1786,7 +2093,8 @@ void subvlxc_point(const Problem& P, double rht[2][10], double wgt, double* vxc,
 // GETVLXC serial branch (getvlxc.F:125-164) with NSPN=2 and the SIC spin-2
 // density zero.  rhog: RHOG(nmsh,10) of the FO; vxc(2*nmsh); ergs[4] =
 // ERGXL, ERGXN, ERGCL, ERGCN.
-void getvlxc_sic(const Problem& P, const double* rhog, double* vxc, double* ergs) {
+void getvlxc_sic(const Problem& P, const double* rhog, double* vxc, double* ergs, const double* tau = nullptr,
+                 double* mixin = nullptr) {
   const int nmsh = P.nmsh;
   const int ng = P.gga() ? 10 : 1;
   for (int i = 0; i < 4; ++i) ergs[i] = 0.0;
@@ -1801,7 +2109,16 @@ void getvlxc_sic(const Problem& P, const double* rhog, double* vxc, double* ergs
         rht[1][k] = 0.0 + 0.5 * 0.0;
       }
       double v[2] = {0.0, 0.0};
-      subvlxc_point(P, rht, P.wmsh[ip], v, ex4);
+      if (P.mgga()) {
+        // GETTAU_PAR with the SIC FO in spin up (unravel2.f:242-246 zeroes the others)
+        const double t2[2] = {tau[ip], 0.0};
+        double z[4] = {0.0, 0.0, 0.0, 0.0};
+        subvlxc_point(P, rht, P.wmsh[ip], v, ex4, t2, z);
+        if (mixin)
+          for (int d = 0; d < 4; ++d) mixin[(size_t)ip * 4 + d] = z[d];
+      } else {
+        subvlxc_point(P, rht, P.wmsh[ip], v, ex4);
+      }
       vxc[ip] = v[0];
       vxc[ip + nmsh] = v[1];
     }
@@ -1914,12 +2231,32 @@ void fo_coefficients(const Problem& P, int s, std::vector<double>& cfo) {
     }
 }
 
+// GETTAU_PAR (gettau_par.f90:1-226) for one FO: tau = |grad phi|^2 / 2 from
+// the FO coefficients with the |c| <= 1e-10 skip.
+void fo_tau(const Problem& P, const double* cfo, std::vector<double>& tau) {
+  const int nmsh = P.nmsh;
+  tau.assign(nmsh, 0.0);
+  std::vector<double> g;
+  for (int l0 = 0; l0 < nmsh; l0 += MPBLOCKXC) {
+    const int mpts = std::min(MPBLOCKXC, nmsh - l0);
+    orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 1, 4, cfo, P.nbasis, 1, 0, g);
+    for (int i = 0; i < mpts; ++i)
+      tau[l0 + i] = tau[l0 + i] + 0.5 * (g[(size_t)1 * mpts + i] * g[(size_t)1 * mpts + i] +
+                                         g[(size_t)2 * mpts + i] * g[(size_t)2 * mpts + i] +
+                                         g[(size_t)3 * mpts + i] * g[(size_t)3 * mpts + i]);
+  }
+}
+
 // APOTNL_SIC (apotnl_sic.F:31-668) for one FO.
 int apotnl_sic(const Problem& P, int s, int k, const double* cfo, double* results, double* cfrm,
-               double* pot, double* coul_out, double* rhog_out, bool exact) {
+               double* pot, double* coul_out, double* rhog_out, bool exact, double* mixin_out = nullptr) {
   const int nmsh = P.nmsh;
   std::vector<double> coulomb(nmsh), rhog((size_t)10 * nmsh);
   coupot_sic(P, cfo, exact, coulomb.data(), rhog.data(), nullptr);
+  if (P.xc_exact_density && !exact) {
+    std::vector<double> scratch(nmsh);
+    coupot_sic(P, cfo, true, scratch.data(), rhog.data(), nullptr);
+  }
   double addit = 0.0;
   for (int i = 0; i < nmsh; ++i) addit += std::fabs(coulomb[i]);
   if (addit < 0.001) return fail("APOTNL_SIC: COUPOT IS ZERO", 6);
@@ -1945,7 +2282,14 @@ int apotnl_sic(const Problem& P, int s, int k, const double* cfo, double* result
   }
   std::vector<double> vxc(2 * (size_t)nmsh);
   double ergs[4];
-  getvlxc_sic(P, rhog.data(), vxc.data(), ergs);
+  if (P.mgga()) {
+    std::vector<double> tau, mix((size_t)4 * nmsh);
+    fo_tau(P, cfo, tau);
+    getvlxc_sic(P, rhog.data(), vxc.data(), ergs, tau.data(), mix.data());
+    if (mixin_out) std::memcpy(mixin_out, mix.data(), sizeof(double) * 4 * nmsh);
+  } else {
+    getvlxc_sic(P, rhog.data(), vxc.data(), ergs);
+  }
   double xch1 = 0, xch2 = 0, xcou = 0, xexx = 0, xdel = 0;
   const double p43 = (double)(4.0f / 3.0f);
   for (int i = 0; i < nmsh; ++i) pot[i] = vxc[i] + coulomb[i];
@@ -1983,13 +2327,46 @@ int apotnl_sic(const Problem& P, int s, int k, const double* cfo, double* result
   return 0;
 }
 
-// SICLAGM / SICLMSLV (frmorb_mpi.F:2-572), LDA/GGA branch (NGRAD=1).
+// SICLAGM / SICLMSLV (frmorb_mpi.F:2-572).  LDA/GGA: NGRAD=1 and the local
+// potential only.  Meta-GGA (frmorb_mpi.F:440-509): NGRAD=4 and, with the FOs'
+// Hamiltonian ingredients zm [nf][nmsh][4], the gradient terms
+// grad phi_j . (phi_l w Z) + phi_j w (grad phi_l . Z) + Z4 w grad phi_j . grad phi_l.
 void siclagm(const Problem& P, int s, const double* pots /*[nf][nmsh]*/, const double* cfo,
-             double* sic, int ld) {
+             double* sic, int ld, const double* zm = nullptr) {
   const int nf = P.nfrm[s], nmsh = P.nmsh, nb = P.nbasis;
   for (int l = 0; l < nf; ++l)
     for (int j = 0; j < nf; ++j) sic[(size_t)l * ld + j] = 0.0;
   std::vector<double> pts, phi;
+  if (P.mgga()) {
+    for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
+      const int mpts = std::min(MPBLOCK, nmsh - l0);
+      orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 1, 4, cfo, nb, nf, 1, phi);
+      auto G = [&](int f, int ig, int i) { return phi[((size_t)f * 4 + ig) * mpts + i]; };
+      for (int ll = 0; ll < nf; ++ll) {
+        std::vector<double> pl((size_t)8 * mpts);
+        for (int i = 0; i < mpts; ++i) {
+          const double w = P.wmsh[l0 + i];
+          const double* z = &zm[((size_t)ll * nmsh + l0 + i) * 4];
+          pl[i] = G(ll, 0, i) * (pots[(size_t)ll * nmsh + l0 + i] * w);
+          for (int c = 0; c < 3; ++c) pl[(size_t)(1 + c) * mpts + i] = G(ll, 0, i) * w * z[c];
+          pl[(size_t)4 * mpts + i] = w * (G(ll, 1, i) * z[0] + G(ll, 2, i) * z[1] + G(ll, 3, i) * z[2]);
+          for (int c = 0; c < 3; ++c) pl[(size_t)(5 + c) * mpts + i] = G(ll, 1 + c, i) * w * z[3];
+        }
+        auto dot = [&](int jf, int ig, int t) {
+          double a = 0.0;
+          for (int i = 0; i < mpts; ++i) a += G(jf, ig, i) * pl[(size_t)t * mpts + i];
+          return a;
+        };
+        for (int jf = 0; jf < nf; ++jf) {
+          double add = dot(jf, 0, 0);
+          add = add + dot(jf, 1, 1) + dot(jf, 2, 2) + dot(jf, 3, 3) + dot(jf, 0, 4);
+          add = add + dot(jf, 1, 5) + dot(jf, 2, 6) + dot(jf, 3, 7);
+          sic[(size_t)ll * ld + jf] = sic[(size_t)ll * ld + jf] - add;
+        }
+      }
+    }
+    return;
+  }
   for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
     const int mpts = std::min(MPBLOCK, nmsh - l0);
     orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 0, 1, cfo, nb, nf, 1, phi);
@@ -2098,9 +2475,10 @@ orc_problem* orc_create(int natoms, const int* atom_type, const double* rat, int
     fail("orc_create: bad sizes");
     return nullptr;
   }
-  if (!(idftyp_x >= 6 && idftyp_x <= 9) || !(idftyp_c == 6 || idftyp_c == 7) || igga_x < 0 || igga_x > 1 ||
-      igga_c < 0 || igga_c > 1) {
-    fail("orc_create: functional outside the supported set (PW91/PBE exchange, PW91/PBE correlation)");
+  const bool scan = igga_x == 3 && idftyp_x == 11 && igga_c == 3 && idftyp_c == 11;
+  if (!scan && (!(idftyp_x >= 6 && idftyp_x <= 9) || !(idftyp_c == 6 || idftyp_c == 7) || igga_x < 0 ||
+                igga_x > 1 || igga_c < 0 || igga_c > 1)) {
+    fail("orc_create: functional outside the supported set (PW91/PBE exchange, PW91/PBE correlation, SCAN)");
     return nullptr;
   }
   auto* o = new orc_problem;
@@ -2244,12 +2622,38 @@ int orc_pair_stats(orc_problem* p, int spin, int iorb, long long* stats) {
 }
 
 int orc_getvlxc_sic(orc_problem* p, const double* rhog, double* vxc, double* ergs) {
+  if (p->P.mgga()) return fail("GETVLXC: a meta-GGA needs tau (orc_getvlxc_mgga)");
   getvlxc_sic(p->P, rhog, vxc, ergs);
   return 0;
 }
 
+int orc_getvlxc_mgga(orc_problem* p, const double* rhog, const double* tau, double* vxc, double* mixin,
+                     double* ergs) {
+  if (!p->P.mgga()) return fail("GETVLXC: tau and MIXIN belong to meta-GGA functionals");
+  getvlxc_sic(p->P, rhog, vxc, ergs, tau, mixin);
+  return 0;
+}
+
+int orc_set_xc_exact_density(orc_problem* p, int on) {
+  p->P.xc_exact_density = on != 0;
+  return 0;
+}
+
+int orc_fo_tau(orc_problem* p, int spin, int iorb, double* tau) {
+  Problem& P = p->P;
+  if (!P.have_tmat) {
+    int rc = compute_tmat(P);
+    if (rc) return rc;
+  }
+  std::vector<double> c, t;
+  fo_coefficients(P, spin - 1, c);
+  fo_tau(P, &c[(size_t)(iorb - 1) * P.nbasis], t);
+  std::memcpy(tau, t.data(), sizeof(double) * P.nmsh);
+  return 0;
+}
+
 int orc_apotnl_sic(orc_problem* p, int spin, int iorb, double* results, double* cfrm, double* pot,
-                   double* coulomb, double* rhog) {
+                   double* coulomb, double* rhog, double* mixin) {
   Problem& P = p->P;
   if (!P.have_tmat) {
     int rc = compute_tmat(P);
@@ -2258,10 +2662,10 @@ int orc_apotnl_sic(orc_problem* p, int spin, int iorb, double* results, double* 
   std::vector<double> c;
   fo_coefficients(P, spin - 1, c);
   return apotnl_sic(P, spin - 1, iorb - 1, &c[(size_t)(iorb - 1) * P.nbasis], results, cfrm, pot, coulomb, rhog,
-                    false);
+                    false, P.mgga() ? mixin : nullptr);
 }
 
-int orc_siclagm(orc_problem* p, int spin, const double* pots, double* sic, int ld) {
+int orc_siclagm(orc_problem* p, int spin, const double* pots, const double* zm, double* sic, int ld) {
   Problem& P = p->P;
   if (!P.have_tmat) {
     int rc = compute_tmat(P);
@@ -2269,7 +2673,8 @@ int orc_siclagm(orc_problem* p, int spin, const double* pots, double* sic, int l
   }
   std::vector<double> c;
   fo_coefficients(P, spin - 1, c);
-  siclagm(P, spin - 1, pots, c.data(), sic, ld);
+  if (P.mgga() && !zm) return fail("SICLAGM: a meta-GGA needs the FOs' MIXIN arrays");
+  siclagm(P, spin - 1, pots, c.data(), sic, ld, zm);
   return 0;
 }
 
@@ -2296,6 +2701,7 @@ int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* 
     int nf = P.nfrm[s];
     int nrun = (fo_limit > 0) ? std::min(fo_limit, nf) : nf;
     std::vector<double> pots((size_t)nf * P.nmsh, 0.0);
+    std::vector<double> zm(P.mgga() ? (size_t)nf * P.nmsh * 4 : 0, 0.0);
     std::vector<int> rcs(nf, 0);
     {
       std::atomic<int> next(0);
@@ -2305,7 +2711,7 @@ int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* 
           if (k >= nrun) break;
           double res[13], cf[3];
           rcs[k] = apotnl_sic(P, s, k, &c[(size_t)k * P.nbasis], res, cf, &pots[(size_t)k * P.nmsh], nullptr,
-                              nullptr, false);
+                              nullptr, false, P.mgga() ? &zm[(size_t)k * P.nmsh * 4] : nullptr);
           for (int i = 0; i < 13; ++i) results[((size_t)s * ld + k) * 13 + i] = res[i];
           for (int i = 0; i < 3; ++i) cfrm[((size_t)s * ld + k) * 3 + i] = cf[i];
         }
@@ -2319,7 +2725,7 @@ int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* 
     for (int k = 0; k < nrun; ++k)
       if (rcs[k]) return rcs[k];
     if (fo_limit > 0 && nrun < nf) continue;  // sampled timing run: no SIC matrix / forces
-    siclagm(P, s, pots.data(), c.data(), &sic[(size_t)s * ld * ld], ld);
+    siclagm(P, s, pots.data(), c.data(), &sic[(size_t)s * ld * ld], ld, P.mgga() ? zm.data() : nullptr);
     rc = frmorb2_force(P, s, &sic[(size_t)s * ld * ld], ld, &debdax[(size_t)s * ld * 3]);
     if (rc) return rc;
     for (int k = 0; k < nf; ++k) zsic += results[((size_t)s * ld + k) * 13 + 8];
@@ -2344,6 +2750,19 @@ int orc_xc_point(int igga_x, int idftyp_x, int igga_c, int idftyp_c, const doubl
   for (int i = 0; i < 4; ++i) e4[i] = 0.0;
   subvlxc_point(P, rht, w, v2, e4);
   return 0;
+}
+
+void orc_scan_x(double rho, double drho, double tau, double* out) {
+  scan_x_unp(rho, drho, tau, out[0], out[1], out[2], out[3]);
+}
+void orc_scan_c(double ru, double rd, double dru, double drd, double drt, double tauu, double taud, double* out) {
+  double vc[2], vcdd[2];
+  scan_c(ru, rd, dru, drd, drt, tauu, taud, out[0], vc, vcdd, out[5]);
+  out[1] = vc[0];
+  out[2] = vc[1];
+  out[3] = vcdd[0];
+  out[4] = vcdd[1];
+  out[6] = 0.0;
 }
 
 void orc_boys(int maxfmt, double x, double* s) { boys(maxfmt, x, std::exp(-x), s); }

@@ -57,11 +57,23 @@ int orc_coupot_sic(orc_problem* p, int spin, int iorb, int exact,
                    double* coulomb, double* rhog, long long* stats);
 /* getvlxc.F:8 serial branch with subvlxc_libxc.F90 (NSPN forced to 2 as in apotnl_sic.F:419) */
 int orc_getvlxc_sic(orc_problem* p, const double* rhog, double* vxc, double* ergs);
+/* SCAN: tau of the FO per point, MIXIN(4, nmsh) spin-up Hamiltonian ingredients */
+int orc_getvlxc_mgga(orc_problem* p, const double* rhog, const double* tau, double* vxc, double* mixin,
+                     double* ergs);
+int orc_fo_tau(orc_problem* p, int spin, int iorb, double* tau);
+/* Test knob: XC on the untruncated (every point near) pair density while the
+   Coulomb potential keeps the near/far split (0 = the reference's behaviour). */
+int orc_set_xc_exact_density(orc_problem* p, int on);
+/* SCAN point functions (scan.f): x: out[4] = ex, vx, vxdd, amux;
+   c: out[7] = ec, vc_up, vc_dn, vcdd_up, vcdd_dn, amu, (unused) */
+void orc_scan_x(double rho, double drho, double tau, double* out);
+void orc_scan_c(double ru, double rd, double dru, double drd, double drt, double tauu, double taud, double* out);
 /* apotnl_sic.F:31: RESULTS(13), CFRM(3), POT(nmsh) = V_xc + V_H (the ZPOT record) */
 int orc_apotnl_sic(orc_problem* p, int spin, int iorb, double* results, double* cfrm,
-                   double* pot, double* coulomb, double* rhog);
+                   double* pot, double* coulomb, double* rhog, double* mixin);
 /* frmorb_mpi.F:2/184 SICLAGM: SIC(ld, ld) from POT(nmsh, nfrm) */
-int orc_siclagm(orc_problem* p, int spin, const double* pots, double* sic, int ld);
+/* zm: [nf][nmsh][4] Hamiltonian ingredients of the FOs (meta-GGA only, else NULL) */
+int orc_siclagm(orc_problem* p, int spin, const double* pots, const double* zm, double* sic, int ld);
 /* frmorb2.F:586-717: DEBDAX(3, ld) from SIC(ld, ld) */
 int orc_frmorb2_force(orc_problem* p, int spin, const double* sic, int ld, double* debdax);
 

@@ -45,8 +45,15 @@ def lib():
         L.orc_fo_coefficients.argtypes = [C.c_void_p, C.c_int, _dp]
         L.orc_coupot_sic.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, _dp, _lp]
         L.orc_getvlxc_sic.argtypes = [C.c_void_p, _dp, _dp, _dp]
-        L.orc_apotnl_sic.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
-        L.orc_siclagm.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int]
+        L.orc_apotnl_sic.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_siclagm.argtypes = [C.c_void_p, C.c_int, _dp, C.c_void_p, _dp, C.c_int]
+        L.orc_getvlxc_mgga.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.orc_fo_tau.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+        L.orc_set_xc_exact_density.argtypes = [C.c_void_p, C.c_int]
+        L.orc_scan_x.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
+        L.orc_scan_x.restype = None
+        L.orc_scan_c.argtypes = [C.c_double] * 7 + [_dp]
+        L.orc_scan_c.restype = None
         L.orc_frmorb2_force.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp]
         L.orc_sic_cycle.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_int]
         L.orc_pair_stats.argtypes = [C.c_void_p, C.c_int, C.c_int, _lp]
@@ -146,19 +153,45 @@ class Oracle:
         return vxc.reshape(2, n), ergs
 
     def apotnl_sic(self, spin, iorb):
+        """One FO; for a meta-GGA also 'mixin' (nmsh, 4): MIXIN(1:4) of the spin-up half."""
         n = self.sysm.nmsh
         res = np.zeros(13)
         cf = np.zeros(3)
         pot = np.zeros(n)
         coul = np.zeros(n)
         rhog = np.zeros(10 * n)
-        _check(lib().orc_apotnl_sic(self.h, spin, iorb, res, cf, pot, coul, rhog))
-        return dict(results=res, cfrm=cf, pot=pot, coulomb=coul, rhog=rhog.reshape(10, n))
+        mix = np.zeros(4 * n)
+        _check(lib().orc_apotnl_sic(self.h, spin, iorb, res, cf, pot, coul, rhog, mix))
+        return dict(results=res, cfrm=cf, pot=pot, coulomb=coul, rhog=rhog.reshape(10, n),
+                    mixin=mix.reshape(n, 4))
 
-    def siclagm(self, spin, pots):
+    def siclagm(self, spin, pots, mixins=None):
+        """pots (nf, nmsh); mixins (nf, nmsh, 4) for a meta-GGA."""
         sic = np.zeros(self.ld * self.ld)
-        _check(lib().orc_siclagm(self.h, spin, np.ascontiguousarray(pots, dtype=np.float64), sic, self.ld))
+        zm = None if mixins is None else np.ascontiguousarray(mixins, dtype=np.float64)
+        _check(lib().orc_siclagm(self.h, spin, np.ascontiguousarray(pots, dtype=np.float64),
+                                 zm.ctypes.data_as(C.c_void_p) if zm is not None else None, sic, self.ld))
         return sic.reshape(self.ld, self.ld)   # [l][j] = SIC(j,l)
+
+    def getvlxc_mgga(self, rhog, tau):
+        """Meta-GGA GETVLXC: density channels (10, n), tau (n) -> vxc (2, n), mixin (n, 4), ergs (4)."""
+        n = self.sysm.nmsh
+        vxc = np.zeros(2 * n)
+        mix = np.zeros(4 * n)
+        ergs = np.zeros(4)
+        _check(lib().orc_getvlxc_mgga(self.h, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
+                                      np.ascontiguousarray(tau, dtype=np.float64), vxc, mix, ergs))
+        return vxc.reshape(2, n), mix.reshape(n, 4), ergs
+
+    def set_xc_exact_density(self, on):
+        """XC on the untruncated pair density (the GPU's phi^2), Coulomb unchanged."""
+        _check(lib().orc_set_xc_exact_density(self.h, int(bool(on))))
+
+    def fo_tau(self, spin, iorb):
+        """tau = |grad phi_k|^2 / 2 of one FO at the mesh points (GETTAU_PAR)."""
+        tau = np.zeros(self.sysm.nmsh)
+        _check(lib().orc_fo_tau(self.h, spin, iorb, tau))
+        return tau
 
     def frmorb2_force(self, spin, sic):
         deb = np.zeros(3 * self.ld)
@@ -209,3 +242,17 @@ def lebedev19():
     w = np.zeros(146)
     lib().orc_lebedev19(a, w)
     return a.reshape(146, 3), w
+
+
+def scan_x(rho, drho, tau):
+    """SCAN exchange (VSCANxUNP): ex per particle, d(rho ex)/d rho, d/d|grad rho|, d/d tau."""
+    out = np.zeros(4)
+    lib().orc_scan_x(rho, drho, tau, out)
+    return out
+
+
+def scan_c(ru, rd, dru, drd, drt, tauu, taud):
+    """SCAN correlation (VSCANc): ec, vc_up, vc_dn, vcdd_up, vcdd_dn, amu (d/d tau)."""
+    out = np.zeros(7)
+    lib().orc_scan_c(ru, rd, dru, drd, drt, tauu, taud, out)
+    return out[:6]

@@ -15,6 +15,7 @@
 #include "device_math.cuh"
 #include "kernels.cuh"
 #include "xc_functionals.cuh"
+#include "xc_scan.cuh"
 
 namespace flosic {
 
@@ -622,7 +623,14 @@ __device__ __forceinline__ void block_reduce_parts(double v[NPART], double* out)
   }
 }
 
-__global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, int nspn, XCParams xp,
+// Per (point, FO k): the FO density channels from phi (1, 4 or 10 channels:
+// value, gradient, second derivatives), the XC potential, the SIC potential
+// V = V_xc + V_H, Y = w V phi for the SIC matrix and the energy partials.  For
+// SCAN (mgga) also tau = |grad phi|^2/2 and the Hamiltonian ingredients Z of
+// call_mgga.f90, which enter the SIC matrix through four Y channels
+// (frmorb_mpi.F:440-509):
+//   Y0 = w V phi + w grad phi . Z,   Yc = w Z_c phi + w Z_4 d_c phi  (c = x, y, z).
+__global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, int mgga, int nspn, XCParams xp,
                                                    const double* __restrict__ phi, int ldp,
                                                    double* __restrict__ vh, double* __restrict__ vpot,
                                                    double* __restrict__ y, double* __restrict__ part, int nblk) {
@@ -637,6 +645,39 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, 
     double r[10];
     const double f0 = phi[(size_t)k * ldp + p];
     r[0] = f0 * f0;
+    if (mgga) {
+      double f[4];
+      f[0] = f0;
+#pragma unroll
+      for (int ch = 1; ch < 4; ++ch) f[ch] = phi[((size_t)ch * nfo + k) * ldp + p];
+#pragma unroll
+      for (int d = 1; d <= 3; ++d) r[d] = 2 * f[0] * f[d];
+      const double tau = 0.5 * (f[1] * f[1] + f[2] * f[2] + f[3] * f[3]);
+      const size_t kp = (size_t)k * M.n + p;
+      const size_t cs = (size_t)nfo * M.n;  // Y channel stride
+      const double coul = vh[kp] * fnspn / 2.0;
+      vh[kp] = coul;
+      double vup, vdn, e4[4] = {0, 0, 0, 0}, z[4];
+      xc_point_sic_scan(r, tau, w, vup, vdn, e4, z);
+      const double pot = vup + coul;
+      vpot[kp] = pot;
+      y[kp] = w * pot * f0 + w * (f[1] * z[0] + f[2] * z[1] + f[3] * z[2]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) y[(c + 1) * cs + kp] = w * z[c] * f0 + w * z[3] * f[1 + c];
+      const double vx = pot - coul;
+      pv[0] += w * r[0];
+      pv[1] += w * r[0] * coul;
+      pv[2] += w * pow(fabs(r[0]), p43);
+      pv[3] -= w * r[0] * vx;
+      pv[4] += e4[0];
+      pv[5] += e4[1];
+      pv[6] += e4[2];
+      pv[7] += e4[3];
+      pv[8] += M.x[p] * r[0] * w;
+      pv[9] += M.y[p] * r[0] * w;
+      pv[10] += M.z[p] * r[0] * w;
+      continue;
+    }
     if (gga) {
       double f[10];
       f[0] = f0;
@@ -674,15 +715,15 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, 
   block_reduce_parts(pv, part + ((size_t)k * nblk + blockIdx.x) * NPART);
 }
 
-void launch_xc(const MeshDev& M, int nfo, int gga, int nspn, const int* xc, const double* phi, int ldp, double* vh,
-               double* vpot, double* y, double* part, int nblk, cudaStream_t st) {
+void launch_xc(const MeshDev& M, int nfo, int gga, int mgga, int nspn, const int* xc, const double* phi, int ldp,
+               double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st) {
   XCParams xp;
   xp.igga[0] = xc[0];
   xp.idftyp[0] = xc[1];
   xp.igga[1] = xc[2];
   xp.idftyp[1] = xc[3];
   dim3 grid(nblk, nfo);
-  k_xc<<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
+  k_xc<<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, mgga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
 }
 
 // Compensated (Neumaier) sums of the block partials, in block order.
@@ -704,13 +745,21 @@ void launch_reduce_parts(int nfo, int nblk, const double* part, double* sums, cu
   k_reduce_parts<<<nfo, 32, 0, st>>>(nfo, nblk, part, sums);
 }
 
-__global__ void k_density(int npts, int nfo, int k, int gga, const double* __restrict__ phi, int ldp,
+// FO density channels RHOG(ldr, nch) from the phi channels: nch = 1 (LDA),
+// 4 (meta-GGA: value and gradient; the second-derivative channels of the
+// 10-channel layout are written as zero) or 10 (GGA).
+__global__ void k_density(int npts, int nfo, int k, int nch, const double* __restrict__ phi, int ldp,
                           double* __restrict__ rhog, int ldr) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npts) return;
   const double f0 = phi[(size_t)k * ldp + p];
   rhog[p] = f0 * f0;
-  if (!gga) return;
+  if (nch == 1) return;
+  if (nch == 4) {
+    for (int d = 1; d <= 3; ++d) rhog[(size_t)d * ldr + p] = 2 * f0 * phi[((size_t)d * nfo + k) * ldp + p];
+    for (int d = 4; d < 10; ++d) rhog[(size_t)d * ldr + p] = 0.0;
+    return;
+  }
   double f[10];
   f[0] = f0;
   for (int ch = 1; ch < 10; ++ch) f[ch] = phi[((size_t)ch * nfo + k) * ldp + p];
@@ -721,9 +770,52 @@ __global__ void k_density(int npts, int nfo, int k, int gga, const double* __res
   rhog[(size_t)9 * ldr + p] = 2 * (f[2] * f[3] + f[9] * f[0]);
 }
 
-void launch_density(int npts, int nfo, int k, int gga, const double* phi, int ldp, double* rhog, int ldr,
+void launch_density(int npts, int nfo, int k, int nch, const double* phi, int ldp, double* rhog, int ldr,
                     cudaStream_t st) {
-  k_density<<<(npts + 255) / 256, 256, 0, st>>>(npts, nfo, k, gga, phi, ldp, rhog, ldr);
+  k_density<<<(npts + 255) / 256, 256, 0, st>>>(npts, nfo, k, nch, phi, ldp, rhog, ldr);
+}
+
+// tau = |grad phi_k|^2 / 2 of FO k (GETTAU_PAR for the SIC FO).
+__global__ void k_fo_tau(int npts, int nfo, int k, const double* __restrict__ phi, int ldp, double* __restrict__ tau) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  double t = 0.0;
+  for (int d = 1; d <= 3; ++d) {
+    const double g = phi[((size_t)d * nfo + k) * ldp + p];
+    t += g * g;
+  }
+  tau[p] = 0.5 * t;
+}
+
+void launch_fo_tau(int npts, int nfo, int k, const double* phi, int ldp, double* tau, cudaStream_t st) {
+  k_fo_tau<<<(npts + 255) / 256, 256, 0, st>>>(npts, nfo, k, phi, ldp, tau);
+}
+
+// Meta-GGA GETVLXC on given density channels RHOG(ldr, 4+) and tau: VXC(2n),
+// MIXIN(4, n) of the spin-up half, energy partials.
+__global__ void __launch_bounds__(XC_THREADS) k_xc_mgga_rhog(MeshDev M, const double* __restrict__ rhog, int ldr,
+                                                             const double* __restrict__ tau,
+                                                             double* __restrict__ vxc, double* __restrict__ mixin,
+                                                             double* __restrict__ part, int nblk) {
+  double pv[NPART];
+#pragma unroll
+  for (int j = 0; j < NPART; ++j) pv[j] = 0.0;
+  for (int p = blockIdx.x * XC_THREADS + threadIdx.x; p < M.n; p += nblk * XC_THREADS) {
+    double r[4];
+    for (int d = 0; d < 4; ++d) r[d] = rhog[(size_t)d * ldr + p];
+    double vup, vdn, e4[4] = {0, 0, 0, 0}, z[4];
+    xc_point_sic_scan(r, tau[p], M.w[p], vup, vdn, e4, z);
+    vxc[p] = vup;
+    vxc[M.n + p] = vdn;
+    for (int d = 0; d < 4; ++d) mixin[(size_t)4 * p + d] = z[d];
+    for (int j = 0; j < 4; ++j) pv[4 + j] += e4[j];
+  }
+  block_reduce_parts(pv, part + (size_t)blockIdx.x * NPART);
+}
+
+void launch_xc_mgga_rhog(const MeshDev& M, const double* rhog, int ldr, const double* tau, double* vxc,
+                         double* mixin, double* part, int nblk, cudaStream_t st) {
+  k_xc_mgga_rhog<<<nblk, XC_THREADS, 0, st>>>(M, rhog, ldr, tau, vxc, mixin, part, nblk);
 }
 
 __global__ void __launch_bounds__(XC_THREADS) k_xc_rhog(MeshDev M, int gga, XCParams xp,

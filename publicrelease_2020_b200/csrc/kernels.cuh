@@ -90,13 +90,16 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
 // writes the SIC potential V = Vxc + VH*nspn/2 and Y = w V phi, and per-block
 // energy partial sums part[(k*nblk + blk)*NPART + j].
 constexpr int NPART = 11;
-void launch_xc(const MeshDev& M, int nfo, int gga, int nspn, const int* xc, const double* phi, int ldp,
+void launch_xc(const MeshDev& M, int nfo, int gga, int mgga, int nspn, const int* xc, const double* phi, int ldp,
                double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st);
 void launch_reduce_parts(int nfo, int nblk, const double* part, double* sums, cudaStream_t st);
 
 // FO density channels of one FO: rhog[ch*ldr + p] (10 channels for GGA).
-void launch_density(int npts, int nfo, int k, int gga, const double* phi, int ldp, double* rhog, int ldr,
+void launch_density(int npts, int nfo, int k, int nch, const double* phi, int ldp, double* rhog, int ldr,
                     cudaStream_t st);
+void launch_fo_tau(int npts, int nfo, int k, const double* phi, int ldp, double* tau, cudaStream_t st);
+void launch_xc_mgga_rhog(const MeshDev& M, const double* rhog, int ldr, const double* tau, double* vxc,
+                         double* mixin, double* part, int nblk, cudaStream_t st);
 
 // Vxc of given density channels (GETVLXC entry point): vxc[2*n], parts as above (1 FO).
 void launch_xc_rhog(const MeshDev& M, int gga, const int* xc, const double* rhog, int ldr, double* vxc,

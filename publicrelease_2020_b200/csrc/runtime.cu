@@ -290,6 +290,11 @@ struct flosic_ctx {
   bool have_geom = false, have_orb = false;
   // geometry
   int natoms = 0, ntypes = 0, nbasis = 0, nprim = 0, nmsh = 0, nspn = 1, gga = 0;
+  int mgga = 0;  // SCAN: FO values and gradients only, tau and the meta-GGA SIC-matrix terms
+  // FO value channels kept on the mesh: value (LDA), + gradient (meta-GGA),
+  // + second derivatives (GGA, whose potential uses the Laplacian terms)
+  int nch() const { return mgga ? 4 : (gga ? 10 : 1); }
+  int nderv() const { return mgga ? 1 : (gga ? 2 : 0); }
   int xc[4] = {0, 6, 0, 6};
   std::vector<TypeInfo> types;
   std::vector<int> atype, aoff, apoff;
@@ -684,8 +689,8 @@ void fo_setup(flosic_ctx* c, int s) {
 void fo_values(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
   const int nf = S.nf, nb = c->nbasis, P = c->nmsh;
-  const int nch = c->gga ? 10 : 1;
-  const int nderv = c->gga ? 2 : 0;
+  const int nch = c->nch();
+  const int nderv = c->nderv();
   S.phi.ensure((size_t)nch * nf * P);
   const size_t budget = (size_t)3 << 30;  // bytes of basis scratch
   int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nch * nb)));
@@ -777,7 +782,7 @@ void spin_potentials(flosic_ctx* c, int s) {
   CUDA_CHECK(cudaEventRecord(c->ev[4], st));
   const int nf = S.nf, P = c->nmsh;
   S.vpot.ensure((size_t)nf * P);
-  S.y.ensure((size_t)nf * P);
+  S.y.ensure((size_t)(c->mgga ? 4 : 1) * nf * P);
   S.vh.ensure((size_t)nf * P);
   const int nblk = std::min(1024, (P + 255) / 256);
   c->d_part.ensure((size_t)nf * nblk * NPART);
@@ -785,8 +790,8 @@ void spin_potentials(flosic_ctx* c, int s) {
   // XC reads the raw Coulomb potential; keep a scaled copy out of place
   c->d_tmp.ensure((size_t)nf * P);
   CUDA_CHECK(cudaMemcpyAsync(c->d_tmp.p, S.vh.p, sizeof(double) * nf * P, cudaMemcpyDeviceToDevice, st));
-  launch_xc(c->mesh_dev(), nf, c->gga, c->nspn, c->xc, S.phi.p, P, c->d_tmp.p, S.vpot.p, S.y.p, c->d_part.p, nblk,
-            st);
+  launch_xc(c->mesh_dev(), nf, c->gga, c->mgga, c->nspn, c->xc, S.phi.p, P, c->d_tmp.p, S.vpot.p, S.y.p,
+            c->d_part.p, nblk, st);
   launch_reduce_parts(nf, nblk, c->d_part.p, c->d_sums.p, st);
   c->launches += 2;
   std::vector<double> sums((size_t)nf * NPART), far(nf);
@@ -834,7 +839,8 @@ void spin_potentials(flosic_ctx* c, int s) {
   S.pot_valid = true;
 }
 
-// SICLAGM (frmorb_mpi.F:456-517): SIC(j,l) = -sum_p phi_j w V_l phi_l
+// SICLAGM (frmorb_mpi.F:456-517): SIC(j,l) = -sum_p phi_j w V_l phi_l; for a
+// meta-GGA -sum_c sum_p d_c phi_j Y_c,l over the four channels of Y (k_xc).
 void spin_sic(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
   if (S.sic_valid) return;
@@ -843,10 +849,13 @@ void spin_sic(flosic_ctx* c, int s) {
   cudaStream_t st = c->st;
   CUDA_CHECK(cudaEventRecord(c->ev[0], st));
   c->d_sic.ensure((size_t)nf * nf);
-  const double mone = -1.0, zero = 0.0;
-  BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nf, nf, P, &mone, S.phi.p, P, S.y.p, P, &zero,
-                         c->d_sic.p, nf));
-  c->launches++;
+  const double mone = -1.0, zero = 0.0, one = 1.0;
+  const int nyc = c->mgga ? 4 : 1;
+  for (int ch = 0; ch < nyc; ++ch) {
+    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nf, nf, P, &mone, S.phi.p + (size_t)ch * nf * P, P,
+                           S.y.p + (size_t)ch * nf * P, P, ch == 0 ? &zero : &one, c->d_sic.p, nf));
+    c->launches++;
+  }
   S.sic.resize((size_t)nf * nf);
   CUDA_CHECK(cudaMemcpyAsync(S.sic.data(), c->d_sic.p, sizeof(double) * nf * nf, cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaEventRecord(c->ev[1], st));
@@ -1084,10 +1093,14 @@ int flosic_sic_set_geometry(flosic_ctx* c, int natoms, const int32_t* atom_type,
     if (nspn != 1 && nspn != 2) fail(FLOSIC_ERR_ARG, "nspn must be 1 or 2");
     if (!atom_type || !rat || !n_bare || !bfalp || !n_con || !bfcon || !rmsh || !wmsh || !igga || !idftyp)
       fail(FLOSIC_ERR_ARG, "null array argument");
-    for (int i = 0; i < 2; ++i)
-      if (igga[i] < 0 || igga[i] > 1) fail(FLOSIC_ERR_ARG, "IGGA must be 0 (LDA) or 1 (GGA)");
-    if (idftyp[0] < 6 || idftyp[0] > 9) fail(FLOSIC_ERR_ARG, "exchange IDFTYP must be PW91, PBE, REVPBE or RPBE");
-    if (idftyp[1] != 6 && idftyp[1] != 7) fail(FLOSIC_ERR_ARG, "correlation IDFTYP must be PW91 or PBE");
+    const bool scan = igga[0] == 3 && igga[1] == 3 && idftyp[0] == 11 && idftyp[1] == 11;
+    if (!scan) {
+      for (int i = 0; i < 2; ++i)
+        if (igga[i] < 0 || igga[i] > 1)
+          fail(FLOSIC_ERR_ARG, "IGGA must be 0 (LDA) or 1 (GGA), or 3 with IDFTYP 11 for both (SCAN)");
+      if (idftyp[0] < 6 || idftyp[0] > 9) fail(FLOSIC_ERR_ARG, "exchange IDFTYP must be PW91, PBE, REVPBE or RPBE");
+      if (idftyp[1] != 6 && idftyp[1] != 7) fail(FLOSIC_ERR_ARG, "correlation IDFTYP must be PW91 or PBE");
+    }
     invalidate(c);
     c->have_geom = c->have_orb = false;
     c->natoms = natoms;
@@ -1099,6 +1112,7 @@ int flosic_sic_set_geometry(flosic_ctx* c, int natoms, const int32_t* atom_type,
     c->xc[2] = igga[1];
     c->xc[3] = idftyp[1];
     c->gga = (igga[0] > 0 || igga[1] > 0) ? 1 : 0;
+    c->mgga = scan ? 1 : 0;
     c->types.assign(ntypes, TypeInfo());
     for (int t = 0; t < ntypes; ++t) {
       TypeInfo& T = c->types[t];
@@ -1344,8 +1358,8 @@ int flosic_sic_coupot_sic(flosic_ctx* c, int kxxs, int kxxo, double* coulomb, do
     std::vector<double> v(P), r((size_t)10 * P, 0.0);
     CUDA_CHECK(cudaMemcpyAsync(v.data(), S.vh.p + (size_t)k * P, sizeof(double) * P, cudaMemcpyDeviceToHost, c->st));
     c->d_tmp.ensure((size_t)10 * P);
-    launch_density(P, S.nf, k, c->gga, S.phi.p, P, c->d_tmp.p, P, c->st);
-    const int nch = c->gga ? 10 : 1;
+    launch_density(P, S.nf, k, c->nch(), S.phi.p, P, c->d_tmp.p, P, c->st);
+    const int nch = c->gga ? 10 : 1;  // the meta-GGA layout has 10 channels, 4..9 zero
     CUDA_CHECK(cudaMemcpyAsync(r.data(), c->d_tmp.p, sizeof(double) * nch * P, cudaMemcpyDeviceToHost, c->st));
     CUDA_CHECK(cudaStreamSynchronize(c->st));
     for (int i = 0; i < P; ++i) {
@@ -1360,6 +1374,7 @@ int flosic_sic_coupot_sic(flosic_ctx* c, int kxxs, int kxxo, double* coulomb, do
 int flosic_sic_getvlxc(flosic_ctx* c, int ndim, const double* rhog, double* vxc, double* ergs) {
   return guarded([&] {
     require(c, false);
+    if (c->mgga) fail(FLOSIC_ERR_ARG, "GETVLXC: a meta-GGA needs tau; use flosic_sic_getvlxc_mgga");
     if (ndim != c->nmsh) fail(FLOSIC_ERR_ARG, "NDIM must equal the mesh size");
     if (!rhog || !vxc || !ergs) fail(FLOSIC_ERR_ARG, "null array argument");
     const int P = c->nmsh;
@@ -1388,6 +1403,49 @@ int flosic_sic_getvlxc(flosic_ctx* c, int ndim, const double* rhog, double* vxc,
   });
 }
 
+int flosic_sic_getvlxc_mgga(flosic_ctx* c, int ndim, const double* rhog, const double* tau, double* vxc,
+                            double* mixin, double* ergs) {
+  return guarded([&] {
+    require(c, false);
+    if (!c->mgga) fail(FLOSIC_ERR_ARG, "GETVLXC: tau and MIXIN belong to meta-GGA functionals");
+    if (ndim != c->nmsh) fail(FLOSIC_ERR_ARG, "NDIM must equal the mesh size");
+    if (!rhog || !tau || !vxc || !mixin || !ergs) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int P = c->nmsh;
+    std::vector<double> r((size_t)5 * P);  // 4 density channels, then tau
+    for (int i = 0; i < P; ++i) {
+      for (int ch = 0; ch < 4; ++ch) r[(size_t)ch * P + i] = rhog[(size_t)ch * ndim + c->perm[i]];
+      r[(size_t)4 * P + i] = tau[c->perm[i]];
+    }
+    DevBuf<double> dr, dv, dm;
+    dr.upload(r.data(), r.size(), c->st);
+    dv.ensure(2 * (size_t)P);
+    dm.ensure(4 * (size_t)P);
+    const int nblk = std::min(1024, (P + 255) / 256);
+    c->d_part.ensure((size_t)nblk * NPART);
+    c->d_sums.ensure(NPART);
+    launch_xc_mgga_rhog(c->mesh_dev(), dr.p, P, dr.p + (size_t)4 * P, dv.p, dm.p, c->d_part.p, nblk, c->st);
+    launch_reduce_parts(1, nblk, c->d_part.p, c->d_sums.p, c->st);
+    std::vector<double> v(2 * (size_t)P), m(4 * (size_t)P), sums(NPART);
+    CUDA_CHECK(cudaMemcpyAsync(v.data(), dv.p, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaMemcpyAsync(m.data(), dm.p, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaMemcpyAsync(sums.data(), c->d_sums.p, sizeof(double) * NPART, cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    dr.release();
+    dv.release();
+    dm.release();
+    for (int i = 0; i < P; ++i) {
+      const int o = c->perm[i];
+      vxc[o] = v[i];
+      vxc[ndim + o] = v[P + i];
+      for (int d = 0; d < 4; ++d) {
+        mixin[(size_t)4 * o + d] = m[(size_t)4 * i + d];
+        mixin[(size_t)4 * (ndim + o) + d] = 0.0;  // spin-down half: no SIC density there
+      }
+    }
+    for (int j = 0; j < 4; ++j) ergs[j] = sums[4 + j];
+  });
+}
+
 int flosic_sic_set_precision(flosic_ctx* c, int mode) {
   return guarded([&] {
     if (!c) fail(FLOSIC_ERR_ARG, "null context");
@@ -1406,6 +1464,7 @@ int flosic_sic_getvlxc_device(flosic_ctx* c, int npts, const double* d_rhog, int
                               double* d_vxc, double* ergs) {
   return guarded([&] {
     require(c, false);
+    if (c->mgga) fail(FLOSIC_ERR_ARG, "GETVLXC: a meta-GGA needs tau; use flosic_sic_getvlxc_mgga");
     if (npts < 1) fail(FLOSIC_ERR_ARG, "NPTS must be positive");
     if (ldr < npts) fail(FLOSIC_ERR_ARG, "LDR smaller than NPTS");
     if (!d_rhog || !d_wmsh || !d_vxc || !ergs) fail(FLOSIC_ERR_ARG, "null array argument");

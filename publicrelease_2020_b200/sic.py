@@ -34,7 +34,7 @@ EXPORTS = [
     "flosic_sic_set_orbitals", "flosic_sic_gorbdrv", "flosic_sic_frmorb2_fmat", "flosic_sic_frmiorb",
     "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
-    "flosic_sic_set_precision",
+    "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -66,6 +66,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_frmiorb.argtypes = [_vp, _dp, _dp, C.c_int]
     L.flosic_sic_coupot_sic.argtypes = [_vp, C.c_int, C.c_int, _dp, _dp]
     L.flosic_sic_getvlxc.argtypes = [_vp, C.c_int, _dp, _dp, _dp]
+    L.flosic_sic_getvlxc_mgga.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
     L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
     L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
@@ -163,6 +164,16 @@ class FlosicSIC:
         self._check(self.L.flosic_sic_getvlxc(self.h, n, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
                                               vxc, ergs))
         return vxc.reshape(2, n), ergs
+
+    def getvlxc_mgga(self, rhog, tau):
+        """Meta-GGA GETVLXC: RHOG (10, n), TAU (n) -> VXC (2, n), MIXIN (2n, 4), ergs (4)."""
+        n = self.sysm.nmsh
+        vxc = np.zeros(2 * n)
+        mix = np.zeros(8 * n)
+        ergs = np.zeros(4)
+        self._check(self.L.flosic_sic_getvlxc_mgga(self.h, n, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
+                                                   np.ascontiguousarray(tau, dtype=np.float64), vxc, mix, ergs))
+        return vxc.reshape(2, n), mix.reshape(2 * n, 4), ergs
 
     def set_precision(self, mode):
         """"fp64" (the drop-in, default) or "mixed"."""

@@ -40,6 +40,7 @@ FUNCTIONALS = {
     "LDA-PW91*LDA-PW91": (0, 6, 0, 6),
     "GGA-PBE*GGA-PBE": (1, 7, 1, 7),
     "GGA-PW91*GGA-PW91": (1, 6, 1, 6),
+    "MGGA-SCAN*MGGA-SCAN": (3, 11, 3, 11),
 }
 
 
@@ -287,8 +288,9 @@ def atom_centred_mesh(rat, nrad=40, rscale=None, seed=0):
 # ---------------------------------------------------------------------------
 # systems
 # ---------------------------------------------------------------------------
-def water(seed=0, nrad=40):
-    """C1: water, NRLMOL-shaped basis, 5+5 FODs, LDA-PW91*LDA-PW91, NSPN=2."""
+def water(seed=0, nrad=40, functional="LDA-PW91*LDA-PW91"):
+    """C1: water, NRLMOL-shaped basis, 5+5 FODs, NSPN=2; LDA-PW91*LDA-PW91 unless
+    another functional is named."""
     rng = np.random.default_rng(seed)
     b = BOHR_PER_ANG
     rat = np.array([[0.0, 0.0, 0.0], [0.757 * b, 0.0, 0.587 * b], [-0.757 * b, 0.0, 0.587 * b]])
@@ -300,7 +302,7 @@ def water(seed=0, nrad=40):
     n_bare, bfalp, n_con, bfcon = _pack_types(types)
     rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[0.7, 0.5, 0.5], seed=seed + 1)
     sysm = System("water", rat, np.array([0, 1, 1], dtype=np.int32), n_bare, bfalp, n_con, bfcon,
-                  rmsh, wmsh, 2, "LDA-PW91*LDA-PW91")
+                  rmsh, wmsh, 2, functional)
     nocc = 5
     C = orthonormal_orbitals(sysm, 2 * nocc, rng)
     sysm.psi = np.ascontiguousarray(np.concatenate([C[:nocc], C[nocc:]], axis=0))

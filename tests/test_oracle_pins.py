@@ -128,10 +128,12 @@ def test_lda_potential_is_energy_derivative(xc):
         assert abs(v[0] - (ep - em) / (2 * h)) < 1e-7 * max(1.0, abs(v[0]))
 
 
-def test_force_equals_chain_rule_of_lowdin_rotation():
+@pytest.mark.parametrize("functional", ["LDA-PW91*LDA-PW91", "MGGA-SCAN*MGGA-SCAN"])
+def test_force_equals_chain_rule_of_lowdin_rotation(functional):
     """The FOD force of frmorb2.F equals the derivative of E_SIC through the
-    Lowdin-orthonormalised rotation U = S^-1/2 T at fixed potentials."""
-    s = W.water(seed=0, nrad=20)
+    Lowdin-orthonormalised rotation U = S^-1/2 T at fixed potentials (with the
+    meta-GGA terms of the SIC matrix for SCAN)."""
+    s = W.water(seed=0, nrad=20, functional=functional)
     o = O.Oracle(s)
     r = o.sic_cycle(nthreads=4)
     FM = o.fmat()
@@ -181,3 +183,104 @@ def test_pair_plan_counts_small_synthetic():
     o = O.Oracle(s)
     st = o.pair_stats(1, 1)
     assert st["pairs"] > 0 and st["batches"] > 0 and st["weird"] <= st["pairs"]
+
+
+# ---------------------------------------------------------------------------
+# SCAN meta-GGA (scan.f restated in the oracle).  Pins: the uniform-gas limit
+# (exchange = LDA exchange, correlation = PW92 LSD), the one-electron limit
+# (correlation vanishes for a fully polarised single-orbital density), the
+# hydrogen-atom exchange energy SCAN is built to reproduce (-5/16 Ha), and
+# every derivative the functional returns against central differences of its
+# own energy density.
+AX = -0.7385587663820224058842300326808360
+
+
+def _pw92_lsd(rs, zeta):
+    """PW92 correlation energy per particle (Perdew & Wang 1992, eq. 8-10)."""
+    def g(a, a1, b1, b2, b3, b4):
+        q1 = 2 * a * (b1 * rs ** 0.5 + b2 * rs + b3 * rs ** 1.5 + b4 * rs ** 2)
+        return -2 * a * (1 + a1 * rs) * np.log(1 + 1 / q1)
+    eu = g(0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294)
+    ep = g(0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517)
+    am = -g(0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671)
+    f = ((1 + zeta) ** (4 / 3) + (1 - zeta) ** (4 / 3) - 2) / (2 ** (4 / 3) - 2)
+    fzz = 8 / (9 * (2 ** (4 / 3) - 2))
+    return eu + am * f / fzz * (1 - zeta ** 4) + (ep - eu) * f * zeta ** 4
+
+
+@pytest.mark.parametrize("rho", [1e-3, 0.1, 10.0])
+def test_scan_exchange_uniform_gas_is_lda(rho):
+    pi = 3.1415927  # the literal of scan.f's exchange
+    tau_unif = 0.3 * (3 * pi * pi) ** (2 / 3) * rho ** (5 / 3)
+    ex = O.scan_x(rho, 1e-12, tau_unif)[0]
+    assert abs(ex - AX * rho ** (1 / 3)) <= 1e-12 * abs(ex)
+
+
+@pytest.mark.parametrize("rho,zeta", [(0.05, 0.0), (1.0, 0.0), (0.2, 0.6)])
+def test_scan_correlation_uniform_gas_is_pw92(rho, zeta):
+    ru, rd = rho * (1 + zeta) / 2, rho * (1 - zeta) / 2
+    ds = ((1 + zeta) ** (5 / 3) + (1 - zeta) ** (5 / 3)) / 2
+    tau0 = 0.3 * (3 * math.pi ** 2) ** (2 / 3) * rho ** (5 / 3) * ds
+    g = 1e-9  # |grad rho| ~ 0: t -> 0, tau = tau_W + tau0 gives alpha = 1
+    ec = O.scan_c(ru, rd, g / 2, g / 2, g, tau0 / 2 + g * g / (16 * rho), tau0 / 2 + g * g / (16 * rho))[0]
+    rs = (3 / (4 * math.pi * rho)) ** (1 / 3)
+    assert abs(ec - _pw92_lsd(rs, zeta)) <= 1e-9 * abs(ec)
+
+
+def test_scan_correlation_vanishes_for_one_orbital():
+    for ru, dru in ((0.3, 0.2), (2.0, 5.0), (1e-3, 1e-3)):
+        tauw = dru * dru / (8 * ru)  # alpha = 0: tau = tau_W
+        ec = O.scan_c(ru, 0.0, dru, 0.0, dru, tauw, 0.0)[0]
+        assert abs(ec) < 1e-10 * abs(_pw92_lsd((3 / (4 * math.pi * ru)) ** (1 / 3), 1.0))
+
+
+def test_scan_exchange_of_hydrogen_atom():
+    r = np.linspace(1e-6, 40.0, 20001)
+    rho = np.exp(-2 * r) / np.pi
+    # spin scaling E_x[rho, 0] = E_x^unp[2 rho] / 2; tau = tau_W = rho / 2 per spin
+    ex = np.array([O.scan_x(2 * q, 4 * q, q)[0] for q in rho])
+    w = np.full_like(r, r[1] - r[0])
+    w[0] *= 0.5
+    w[-1] *= 0.5
+    e = np.sum(rho * ex * 4 * np.pi * r * r * w)
+    assert abs(e - (-5 / 16)) < 5e-6
+
+
+@pytest.mark.parametrize("alpha", [0.0, 0.4, 1.7])
+def test_scan_exchange_derivatives(alpha):
+    rho, drho = 0.37, 0.29
+    pi = 3.1415927
+    tau = alpha * 0.3 * (3 * pi * pi) ** (2 / 3) * rho ** (5 / 3) + drho * drho / (8 * rho)
+    _, vx, vxdd, amu = O.scan_x(rho, drho, tau)
+    e = lambda a, b, c: a * O.scan_x(a, b, c)[0]
+    h = 1e-6
+    assert abs(vx - (e(rho + h, drho, tau) - e(rho - h, drho, tau)) / (2 * h)) < 1e-7
+    assert abs(vxdd - (e(rho, drho + h, tau) - e(rho, drho - h, tau)) / (2 * h)) < 1e-7
+    assert abs(amu - (e(rho, drho, tau + h) - e(rho, drho, tau - h)) / (2 * h)) < 1e-7
+
+
+@pytest.mark.parametrize("alpha", [0.3, 1.6])
+def test_scan_correlation_derivatives(alpha):
+    """vc = d(rho ec)/d rho_s at fixed gradients and tau; vcdd = d/d|grad rho_s|
+    along grad rho_s, with |grad rho| following; amu = d/d tau."""
+    gu, gd = np.array([0.21, -0.05, 0.13]), np.array([0.02, 0.11, -0.04])
+
+    def e(ru, rd, gu, gd, tauu, taud):
+        dru, drd, drt = np.linalg.norm(gu), np.linalg.norm(gd), np.linalg.norm(gu + gd)
+        return (ru + rd) * O.scan_c(ru, rd, dru, drd, drt, tauu, taud)[0]
+
+    ru, rd = 0.31, 0.12
+    rt, zeta = ru + rd, (ru - rd) / (ru + rd)
+    ds = ((1 + zeta) ** (5 / 3) + (1 - zeta) ** (5 / 3)) / 2
+    tau0 = 0.3 * (3 * math.pi ** 2) ** (2 / 3) * rt ** (5 / 3) * ds
+    tt = alpha * tau0 + np.dot(gu + gd, gu + gd) / (8 * rt)
+    tauu, taud = 0.6 * tt, 0.4 * tt
+    out = O.scan_c(ru, rd, np.linalg.norm(gu), np.linalg.norm(gd), np.linalg.norm(gu + gd), tauu, taud)
+    _, vcu, vcd, vddu, vddd, amu = out
+    h = 1e-6
+    assert abs(vcu - (e(ru + h, rd, gu, gd, tauu, taud) - e(ru - h, rd, gu, gd, tauu, taud)) / (2 * h)) < 1e-7
+    assert abs(vcd - (e(ru, rd + h, gu, gd, tauu, taud) - e(ru, rd - h, gu, gd, tauu, taud)) / (2 * h)) < 1e-7
+    nu, nd = gu / np.linalg.norm(gu), gd / np.linalg.norm(gd)
+    assert abs(vddu - (e(ru, rd, gu + h * nu, gd, tauu, taud) - e(ru, rd, gu - h * nu, gd, tauu, taud)) / (2 * h)) < 1e-7
+    assert abs(vddd - (e(ru, rd, gu, gd + h * nd, tauu, taud) - e(ru, rd, gu, gd - h * nd, tauu, taud)) / (2 * h)) < 1e-7
+    assert abs(amu - (e(ru, rd, gu, gd, tauu + h, taud) - e(ru, rd, gu, gd, tauu - h, taud)) / (2 * h)) < 1e-7

@@ -8,9 +8,12 @@ the SIC matrix and the FOD forces, through the C ABI (flosic_sic_cycle).
 Workload (N=1): the synthetic kernel shape -- 40 atoms in a 12 A cube, 512
 contracted s/p/d functions (3 primitives each, exponents log-uniform in
 [0.05, 1e4]), 1,000,000 mesh points, 128 FOs, PBE -- generated from a seed
-(there is no dataset); the FP64 path.  Multi-GPU (torchrun): every rank runs
-its own SCF cycle on its own GPU (replicas, no data-path collective);
-value = max-over-ranks time / N.
+(there is no dataset).  Multi-GPU (torchrun, NCCL): the same system's mesh
+points are split into N shards, one per rank (flosic_sic_set_shard); a step
+is one cycle with the one exchange of the path, an in-place NCCL all-reduce of
+the packed partial sums (SIC matrix, APOTNL_SIC mesh sums) on the GPU, then
+the combine on every rank -- strong scaling; value = max-over-ranks time of
+one cycle.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -179,7 +182,7 @@ def run_reference(args, rank, world):
     cfg["parallelism"] = "host threads"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "strong",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": cfg,
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
                          "sample": f"oracle (reference algorithm restated in C++) on {sample['points']} of "
@@ -199,9 +202,19 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
     sysm, cfg = workload(args.workload)
     ctx = S.FlosicSIC(local_rank)
+    if world > 1:
+        ctx.set_shard(rank, world)
     ctx.set_geometry(sysm)
     ctx.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
     ld = ctx.ld
+    if world > 1:
+        from publicrelease_2020_b200.shard import sharded_cycle
+
+        def step(out):
+            return sharded_cycle(ctx, device=f"cuda:{local_rank}")
+    else:
+        def step(out):
+            return ctx.cycle(out)
 
     def new_out():
         return dict(results=np.zeros(2 * ld * 13), sic=np.zeros(2 * ld * ld), debdax=np.zeros(2 * ld * 3),
@@ -216,7 +229,7 @@ def run_ours(args, rank, world, local_rank):
         ctx.set_precision(mode)
         out = new_out()
         for _ in range(args.warmup):
-            ctx.cycle(out)
+            step(out)
         acc = dict(coul_ms=0.0, near=0, far=0, terms=0, launches=0, stage=np.zeros(7))
         barrier()
         torch.cuda.synchronize()
@@ -224,7 +237,7 @@ def run_ours(args, rank, world, local_rank):
         with clk_sampler as clk:
             e0.record()
             for _ in range(args.steps):
-                r = ctx.cycle(out)
+                r = step(out)
                 st = ctx.stats()
                 acc["coul_ms"] += st["stage_ms"][3]
                 acc["near"] += st["near_evals"]
@@ -269,7 +282,7 @@ def run_ours(args, rank, world, local_rank):
     f0.record()
     for _ in range(args.steps):
         ctx.set_orbitals(psi, sysm.nwfs, sysm.fods)
-        ctx.cycle(out)
+        step(out)
     f1.record()
     torch.cuda.synchronize()
     barrier()
@@ -289,21 +302,24 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     per_step_s = t_ms / 1e3 / args.steps
-    value = per_step_s / world
+    value = per_step_s
     coul_s = st_acc["coul_ms"] / 1e3 / args.steps
-    flops = (st_acc["near"] * COULOMB_FLOPS_NEAR + st_acc["terms"] * COULOMB_FLOPS_TERM) / args.steps
+    # the work counters are the whole system's (summed over the shards); the
+    # roofline is per GPU: this rank's Coulomb stage against its share
+    flops = (st_acc["near"] * COULOMB_FLOPS_NEAR + st_acc["terms"] * COULOMB_FLOPS_TERM) / args.steps / world
     peak = fp64_peak_tflops(torch)
     achieved = flops / coul_s / 1e12 if coul_s > 0 else 0.0
     ntiles = (cfg["nmsh"] + 127) // 128
     traffic = COULOMB_DRAM_BYTES_PER_TILE * ntiles if args.workload in ("c2", "c2half", "c2tiny") else None
-    cfg.update(parallelism=f"replicas x{world}" if world > 1 else "single GPU", l2="working set >> L2 (126 MB)",
+    cfg.update(parallelism=(f"mesh shards x{world}, NCCL all-reduce of the partial sums" if world > 1
+                            else "single GPU"), l2="working set >> L2 (126 MB)",
                npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision=headline)
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if headline == "fp64" else "f32+f64",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64" if headline == "fp64" else "f32+f64",
         "data": "synthetic (seeded)", "config": cfg,
-        "e2e": {"value": e2e_ms / 1e3 / args.steps / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": e2e_ms / 1e3 / args.steps, "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(st_acc["launches"]),
         "roofline": {"bound": "tensor", "kernel": "k_coulomb_shared + k_coulomb_perfo", "achieved": achieved, "peak": peak,
@@ -322,7 +338,7 @@ def run_ours(args, rank, world, local_rank):
     if len(runs) > 1:
         line["precision"] = {
             "headline": headline,
-            "s_per_cycle": {m: times[m] / 1e3 / args.steps / world for m in runs},
+            "s_per_cycle": {m: times[m] / 1e3 / args.steps for m in runs},
             "stage_ms": {m: {k: round(float(v) / args.steps, 3) for k, v in
                              zip(["fo", "orbitals", "coul_setup", "coul_eval", "xc", "sicmat", "forces"],
                                  runs[m][1]["stage"])} for m in runs},

@@ -155,6 +155,34 @@ int flosic_sic_frmorb2_force(flosic_ctx* ctx, int lspn, const double* sic, int l
 int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, double* debdax,
                      double* cfrm, double* esic);
 
+/* Mesh sharding across GPUs (one context per GPU and rank).  The reference
+   spreads the same work over MPI workers and sums their mesh contributions:
+   MPI_REDUCE of COULOMB/RHOG in pampoiss.F:105-120 and of the SIC matrix in
+   pamlmsic.F:103.  Here each context evaluates the mesh points of its shard
+   (an even split of the 128-point tiles of the sorted mesh); the set-up that
+   does not depend on the points (FO construction, pair coefficients, POISSON1
+   call set-up incl. its far-point counts over the whole mesh) is repeated on
+   every rank, so the only exchange is one sum of a small packed buffer:
+     flosic_sic_set_shard(ctx, shard, nshards)   0 <= shard < nshards; call
+                                                  before or after set_geometry
+     flosic_sic_partial_size(ctx, &n)            doubles in the packed buffer
+     flosic_sic_cycle_partial(ctx, d_buf)        writes this shard's partial
+                                                  sums to DEVICE memory d_buf[n]
+     (caller: sum d_buf over the ranks in place, e.g. ncclAllReduce / MPI)
+     flosic_sic_cycle_combine(ctx, d_buf, ...)   RESULTS, SIC, DEBDAX, CFRM and
+                                                  E_SIC as flosic_sic_cycle
+   Layout of the buffer, per spin: SIC(nfrm,nfrm), the mesh sums (XCH1, XCOU,
+   XEXX, XDEL, ERGXL, ERGXN, ERGCL, ERGCN, CFRM(3)) per FO, the scaled Coulomb
+   potential at the farthest mesh point per FO (zero on the other shards); then
+   the near/far/term work counters.  A sharded context refuses the entry points
+   whose outputs cover the whole mesh (COUPOT_SIC, APOTNL_SIC, SICLAGM,
+   flosic_sic_cycle) with FLOSIC_ERR_STATE. */
+int flosic_sic_set_shard(flosic_ctx* ctx, int shard, int nshards);
+int flosic_sic_partial_size(flosic_ctx* ctx, int64_t* ndoubles);
+int flosic_sic_cycle_partial(flosic_ctx* ctx, double* d_partial);
+int flosic_sic_cycle_combine(flosic_ctx* ctx, const double* d_partial, int ld, double* results, double* sic,
+                             double* debdax, double* cfrm, double* esic);
+
 /* Timing/introspection (no reference counterpart): number of kernels launched by
    the last flosic_sic_cycle, per-stage device milliseconds of the last cycle
    (ms[0]=FO construction, [1]=orbital/density, [2]=Coulomb setup, [3]=Coulomb

@@ -2094,7 +2094,7 @@ void subvlxc_point(const Problem& P, double rht[2][10], double wgt, double* vxc,
 // density zero.  rhog: RHOG(nmsh,10) of the FO; vxc(2*nmsh); ergs[4] =
 // ERGXL, ERGXN, ERGCL, ERGCN.
 void getvlxc_sic(const Problem& P, const double* rhog, double* vxc, double* ergs, const double* tau = nullptr,
-                 double* mixin = nullptr) {
+                 double* mixin = nullptr, int sb = 0, int se = INT32_MAX) {
   const int nmsh = P.nmsh;
   const int ng = P.gga() ? 10 : 1;
   for (int i = 0; i < 4; ++i) ergs[i] = 0.0;
@@ -2109,15 +2109,17 @@ void getvlxc_sic(const Problem& P, const double* rhog, double* vxc, double* ergs
         rht[1][k] = 0.0 + 0.5 * 0.0;
       }
       double v[2] = {0.0, 0.0};
+      double dump[4] = {0.0, 0.0, 0.0, 0.0};
+      double* e4 = (ip >= sb && ip < se) ? ex4 : dump;  // energy sums of the point range only
       if (P.mgga()) {
         // GETTAU_PAR with the SIC FO in spin up (unravel2.f:242-246 zeroes the others)
         const double t2[2] = {tau[ip], 0.0};
         double z[4] = {0.0, 0.0, 0.0, 0.0};
-        subvlxc_point(P, rht, P.wmsh[ip], v, ex4, t2, z);
+        subvlxc_point(P, rht, P.wmsh[ip], v, e4, t2, z);
         if (mixin)
           for (int d = 0; d < 4; ++d) mixin[(size_t)ip * 4 + d] = z[d];
       } else {
-        subvlxc_point(P, rht, P.wmsh[ip], v, ex4);
+        subvlxc_point(P, rht, P.wmsh[ip], v, e4);
       }
       vxc[ip] = v[0];
       vxc[ip + nmsh] = v[1];
@@ -2332,13 +2334,14 @@ int apotnl_sic(const Problem& P, int s, int k, const double* cfo, double* result
 // Hamiltonian ingredients zm [nf][nmsh][4], the gradient terms
 // grad phi_j . (phi_l w Z) + phi_j w (grad phi_l . Z) + Z4 w grad phi_j . grad phi_l.
 void siclagm(const Problem& P, int s, const double* pots /*[nf][nmsh]*/, const double* cfo,
-             double* sic, int ld, const double* zm = nullptr) {
-  const int nf = P.nfrm[s], nmsh = P.nmsh, nb = P.nbasis;
+             double* sic, int ld, const double* zm = nullptr, int pb = 0, int pe = INT32_MAX) {
+  const int nf = P.nfrm[s], nmsh = std::min(P.nmsh, pe), nb = P.nbasis;
   for (int l = 0; l < nf; ++l)
     for (int j = 0; j < nf; ++j) sic[(size_t)l * ld + j] = 0.0;
   std::vector<double> pts, phi;
+  const int nall = P.nmsh;  // row stride of pots and zm
   if (P.mgga()) {
-    for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
+    for (int l0 = pb; l0 < nmsh; l0 += MPBLOCK) {
       const int mpts = std::min(MPBLOCK, nmsh - l0);
       orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 1, 4, cfo, nb, nf, 1, phi);
       auto G = [&](int f, int ig, int i) { return phi[((size_t)f * 4 + ig) * mpts + i]; };
@@ -2346,8 +2349,8 @@ void siclagm(const Problem& P, int s, const double* pots /*[nf][nmsh]*/, const d
         std::vector<double> pl((size_t)8 * mpts);
         for (int i = 0; i < mpts; ++i) {
           const double w = P.wmsh[l0 + i];
-          const double* z = &zm[((size_t)ll * nmsh + l0 + i) * 4];
-          pl[i] = G(ll, 0, i) * (pots[(size_t)ll * nmsh + l0 + i] * w);
+          const double* z = &zm[((size_t)ll * nall + l0 + i) * 4];
+          pl[i] = G(ll, 0, i) * (pots[(size_t)ll * nall + l0 + i] * w);
           for (int c = 0; c < 3; ++c) pl[(size_t)(1 + c) * mpts + i] = G(ll, 0, i) * w * z[c];
           pl[(size_t)4 * mpts + i] = w * (G(ll, 1, i) * z[0] + G(ll, 2, i) * z[1] + G(ll, 3, i) * z[2]);
           for (int c = 0; c < 3; ++c) pl[(size_t)(5 + c) * mpts + i] = G(ll, 1 + c, i) * w * z[3];
@@ -2367,13 +2370,13 @@ void siclagm(const Problem& P, int s, const double* pots /*[nf][nmsh]*/, const d
     }
     return;
   }
-  for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
+  for (int l0 = pb; l0 < nmsh; l0 += MPBLOCK) {
     const int mpts = std::min(MPBLOCK, nmsh - l0);
     orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 0, 1, cfo, nb, nf, 1, phi);
     for (int ll = 0; ll < nf; ++ll) {
       std::vector<double> pl(mpts);
       for (int i = 0; i < mpts; ++i)
-        pl[i] = phi[(size_t)ll * mpts + i] * (pots[(size_t)ll * nmsh + l0 + i] * P.wmsh[l0 + i]);
+        pl[i] = phi[(size_t)ll * mpts + i] * (pots[(size_t)ll * nall + l0 + i] * P.wmsh[l0 + i]);
       for (int jf = 0; jf < nf; ++jf) {
         double add = 0.0;
         for (int i = 0; i < mpts; ++i) add += phi[(size_t)jf * mpts + i] * pl[i];
@@ -2631,6 +2634,146 @@ int orc_getvlxc_mgga(orc_problem* p, const double* rhog, const double* tau, doub
                      double* ergs) {
   if (!p->P.mgga()) return fail("GETVLXC: tau and MIXIN belong to meta-GGA functionals");
   getvlxc_sic(p->P, rhog, vxc, ergs, tau, mixin);
+  return 0;
+}
+
+// Mesh-shard decomposition of one SIC cycle, packed like the library's
+// flosic_sic_cycle_partial: per spin SIC(nf,nf) at [l*nf + j], the mesh sums
+// (XCH1, XCOU, XEXX, XDEL, ERGXL, ERGXN, ERGCL, ERGCN, CFRM x3) per FO, the
+// scaled Coulomb potential at the farthest mesh point per FO (zero off the
+// range); then three work counters (zero here).  The sums of APOTNL_SIC
+// (apotnl_sic.F:381-408, 564-623) and SICLMSLV run over mesh points [b, e) only.
+constexpr int ORC_NPART = 11;
+static size_t orc_partial_doubles(const Problem& P) {
+  size_t n = 3;
+  for (int s = 0; s < P.nspn; ++s) n += (size_t)P.nfrm[s] * P.nfrm[s] + (size_t)P.nfrm[s] * (ORC_NPART + 1);
+  return n;
+}
+
+static void farthest_point(const Problem& P, int& ifar, double& rmx) {
+  ifar = 0;
+  rmx = 0.0;
+  for (int i = 0; i < P.nmsh; ++i) {
+    const double* r = &P.rmsh[3 * (size_t)i];
+    const double rad = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (rad > rmx) {
+      rmx = rad;
+      ifar = i;
+    }
+  }
+}
+
+int orc_partial_size(orc_problem* p, long long* n) {
+  *n = (long long)orc_partial_doubles(p->P);
+  return 0;
+}
+
+int orc_cycle_partial(orc_problem* p, int b, int e, double* out) {
+  Problem& P = p->P;
+  if (b < 0 || e > P.nmsh || b > e) return fail("orc_cycle_partial: bad point range");
+  int rc = compute_fmat(P);
+  if (rc) return rc;
+  rc = compute_tmat(P);
+  if (rc) return rc;
+  const int nmsh = P.nmsh;
+  int ifar;
+  double rmx;
+  farthest_point(P, ifar, rmx);
+  size_t o = 0;
+  std::fill(out, out + orc_partial_doubles(P), 0.0);
+  for (int s = 0; s < P.nspn; ++s) {
+    const int nf = P.nfrm[s];
+    if (nf == 0) continue;
+    std::vector<double> c;
+    fo_coefficients(P, s, c);
+    std::vector<double> pots((size_t)nf * nmsh), zm(P.mgga() ? (size_t)nf * nmsh * 4 : 0);
+    double* parts = out + o + (size_t)nf * nf;
+    double* asy = parts + (size_t)nf * ORC_NPART;
+    for (int k = 0; k < nf; ++k) {
+      const double* cf = &c[(size_t)k * P.nbasis];
+      std::vector<double> coulomb(nmsh), rhog((size_t)10 * nmsh), vxc(2 * (size_t)nmsh);
+      coupot_sic(P, cf, false, coulomb.data(), rhog.data(), nullptr);
+      if (P.xc_exact_density) {
+        std::vector<double> scratch(nmsh);
+        coupot_sic(P, cf, true, scratch.data(), rhog.data(), nullptr);
+      }
+      const double fnspn = (double)(float)P.nspn;
+      for (int i = 0; i < nmsh; ++i) coulomb[i] = coulomb[i] * fnspn / 2.0;
+      double ergs[4];
+      if (P.mgga()) {
+        std::vector<double> tau;
+        fo_tau(P, cf, tau);
+        getvlxc_sic(P, rhog.data(), vxc.data(), ergs, tau.data(), &zm[(size_t)k * nmsh * 4], b, e);
+      } else {
+        getvlxc_sic(P, rhog.data(), vxc.data(), ergs, nullptr, nullptr, b, e);
+      }
+      double* q = &parts[(size_t)k * ORC_NPART];
+      const double p43 = (double)(4.0f / 3.0f);
+      for (int i = 0; i < nmsh; ++i) pots[(size_t)k * nmsh + i] = vxc[i] + coulomb[i];
+      for (int i = b; i < e; ++i) {
+        const double w = P.wmsh[i], r = rhog[i];
+        const double vx = pots[(size_t)k * nmsh + i] - coulomb[i];
+        q[0] = q[0] + w * r;
+        q[1] = q[1] + w * r * coulomb[i];
+        q[2] = q[2] + w * std::pow(std::fabs(r), p43);
+        q[3] = q[3] - w * r * vx;
+        for (int d = 0; d < 3; ++d) q[8 + d] = q[8 + d] + P.rmsh[3 * (size_t)i + d] * r * w;
+      }
+      for (int j = 0; j < 4; ++j) q[4 + j] = ergs[j];
+      asy[k] = (ifar >= b && ifar < e) ? coulomb[ifar] : 0.0;
+    }
+    siclagm(P, s, pots.data(), c.data(), out + o, nf, P.mgga() ? zm.data() : nullptr, b, e);
+    o += (size_t)nf * nf + (size_t)nf * (ORC_NPART + 1);
+  }
+  return 0;
+}
+
+int orc_cycle_combine(orc_problem* p, const double* in, int ld, double* results, double* sic, double* debdax,
+                      double* cfrm, double* esic) {
+  Problem& P = p->P;
+  int ifar;
+  double rmx;
+  farthest_point(P, ifar, rmx);
+  size_t o = 0;
+  double zsic = 0.0;
+  for (int s = 0; s < P.nspn; ++s) {
+    const int nf = P.nfrm[s];
+    if (nf == 0) continue;
+    const double* lam = in + o;
+    const double* parts = lam + (size_t)nf * nf;
+    const double* asy = parts + (size_t)nf * ORC_NPART;
+    for (int k = 0; k < nf; ++k) {
+      const double* q = &parts[(size_t)k * ORC_NPART];
+      double* r = &results[((size_t)s * ld + k) * 13];
+      const double xch1 = q[0], xcou = q[1];
+      const double excsic = q[4] + q[5] + q[6] + q[7];
+      const double xdel = q[3] - xcou;
+      const double xeng = -excsic - xcou / 2.0;
+      const double pi = 4.0 * std::atan(1.0);
+      r[0] = k + 1;
+      r[1] = xch1;
+      r[2] = 0.0;
+      r[3] = asy[k] * rmx;
+      r[4] = q[2] * 0.75 * std::pow(6 / pi, (double)(1.0f / 3.0f));
+      r[5] = -xcou / 2.0;
+      r[6] = xdel;
+      r[7] = xeng;
+      r[8] = xeng * (2.0 / P.nspn);
+      r[9] = q[4];
+      r[10] = q[6];
+      r[11] = q[5];
+      r[12] = q[7];
+      for (int d = 0; d < 3; ++d) cfrm[((size_t)s * ld + k) * 3 + d] = q[8 + d];
+      zsic += r[8];
+    }
+    double* ps = sic + (size_t)s * ld * ld;
+    for (int l = 0; l < nf; ++l)
+      for (int j = 0; j < nf; ++j) ps[(size_t)l * ld + j] = lam[(size_t)l * nf + j];
+    int rc = frmorb2_force(P, s, ps, ld, debdax + (size_t)s * ld * 3);
+    if (rc) return rc;
+    o += (size_t)nf * nf + (size_t)nf * (ORC_NPART + 1);
+  }
+  *esic = zsic;
   return 0;
 }
 

@@ -64,6 +64,12 @@ int orc_fo_tau(orc_problem* p, int spin, int iorb, double* tau);
 /* Test knob: XC on the untruncated (every point near) pair density while the
    Coulomb potential keeps the near/far split (0 = the reference's behaviour). */
 int orc_set_xc_exact_density(orc_problem* p, int on);
+/* Mesh-shard decomposition of one cycle (same packing as flosic_sic_cycle_partial):
+   partial sums over mesh points [b, e), and the cycle's outputs from their sum. */
+int orc_partial_size(orc_problem* p, long long* n);
+int orc_cycle_partial(orc_problem* p, int b, int e, double* out);
+int orc_cycle_combine(orc_problem* p, const double* in, int ld, double* results, double* sic, double* debdax,
+                      double* cfrm, double* esic);
 /* SCAN point functions (scan.f): x: out[4] = ex, vx, vxdd, amux;
    c: out[7] = ec, vc_up, vc_dn, vcdd_up, vcdd_dn, amu, (unused) */
 void orc_scan_x(double rho, double drho, double tau, double* out);

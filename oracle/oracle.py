@@ -50,6 +50,9 @@ def lib():
         L.orc_getvlxc_mgga.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.orc_fo_tau.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.orc_set_xc_exact_density.argtypes = [C.c_void_p, C.c_int]
+        L.orc_partial_size.argtypes = [C.c_void_p, _lp]
+        L.orc_cycle_partial.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.orc_cycle_combine.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
         L.orc_scan_x.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
         L.orc_scan_x.restype = None
         L.orc_scan_c.argtypes = [C.c_double] * 7 + [_dp]
@@ -256,3 +259,31 @@ def scan_c(ru, rd, dru, drd, drt, tauu, taud):
     out = np.zeros(7)
     lib().orc_scan_c(ru, rd, dru, drd, drt, tauu, taud, out)
     return out[:6]
+
+
+class OracleShard:
+    """The oracle as one shard of a mesh-sharded cycle: mesh points [b, e) of
+    the system, the same partial/combine protocol (and packing) as the CUDA
+    library's flosic_sic_cycle_partial / _combine, on host buffers."""
+
+    def __init__(self, orc, b, e):
+        self.orc, self.b, self.e = orc, int(b), int(e)
+
+    def partial_size(self):
+        n = np.zeros(1, dtype=np.int64)
+        _check(lib().orc_partial_size(self.orc.h, n))
+        return int(n[0])
+
+    def cycle_partial(self, address):
+        _check(lib().orc_cycle_partial(self.orc.h, self.b, self.e, C.c_void_p(int(address))))
+
+    def cycle_combine(self, address):
+        ld = self.orc.ld
+        res = np.zeros(2 * ld * 13)
+        sic = np.zeros(2 * ld * ld)
+        deb = np.zeros(2 * ld * 3)
+        cfrm = np.zeros(2 * ld * 3)
+        esic = np.zeros(1)
+        _check(lib().orc_cycle_combine(self.orc.h, C.c_void_p(int(address)), ld, res, sic, deb, cfrm, esic))
+        return dict(results=res.reshape(2, ld, 13), sic=sic.reshape(2, ld, ld), debdax=deb.reshape(2, ld, 3),
+                    cfrm=cfrm.reshape(2, ld, 3), esic=float(esic[0]))

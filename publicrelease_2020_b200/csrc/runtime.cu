@@ -261,6 +261,8 @@ struct SpinCache {
   std::vector<double> lam;     // Lowdin eigenvalues
   std::vector<double> filo;    // Lowdin eigenvectors [k*nf + a]: component k of eigenvector a
   std::vector<double> results; // [k*13 + i]
+  std::vector<double> parts;   // [k*NPART + j] mesh sums of this context's shard
+  std::vector<double> asy;     // [k] scaled Coulomb potential at the farthest point (0 off this shard)
   std::vector<double> cfrm;    // [k*3 + d]
   std::vector<double> sic;     // [l*nf + j] = SIC(j,l)
   bool sic_valid = false;
@@ -303,6 +305,11 @@ struct flosic_ctx {
   int ntiles = 0;
   int ifar_sorted = 0;         // farthest point from the origin (apotnl_sic.F:410-418)
   double rmx = 0.0;
+  // Mesh shard this context evaluates: tiles [eval_t0, eval_t0 + eval_nt) of
+  // the sorted mesh = sorted points [eval_p0, eval_p0 + eval_n).  One shard
+  // (the default) is the whole mesh.
+  int shard = 0, nshards = 1;
+  int eval_t0 = 0, eval_nt = 0, eval_p0 = 0, eval_n = 0;
   std::vector<PairGeo> pairs;
   std::vector<CallInfo> calls;
   // device geometry
@@ -364,6 +371,20 @@ struct flosic_ctx {
     M.w = d_w.p;
     M.tile_lo = d_tlo.p;
     M.tile_hi = d_thi.p;
+    return M;
+  }
+  // The shard's tiles as a mesh of their own (tile-aligned, so every per-tile
+  // kernel runs on it unchanged).
+  MeshDev eval_mesh() const {
+    MeshDev M = mesh_dev();
+    M.n = eval_n;
+    M.ntiles = eval_nt;
+    M.x += eval_p0;
+    M.y += eval_p0;
+    M.z += eval_p0;
+    M.w += eval_p0;
+    M.tile_lo += 3 * (size_t)eval_t0;
+    M.tile_hi += 3 * (size_t)eval_t0;
     return M;
   }
 };
@@ -569,6 +590,16 @@ void invalidate(flosic_ctx* c) {
   }
 }
 
+// Tiles of shard `shard` of `nshards`: an even split of the sorted tiles.
+void set_eval_range(flosic_ctx* c) {
+  const long long nt = c->ntiles;
+  const int t0 = (int)(nt * c->shard / c->nshards), t1 = (int)(nt * (c->shard + 1) / c->nshards);
+  c->eval_t0 = t0;
+  c->eval_nt = t1 - t0;
+  c->eval_p0 = t0 * TILE;
+  c->eval_n = std::min(t1 * TILE, c->nmsh) - c->eval_p0;
+}
+
 // ---------------------------------------------------------------------------
 // FO construction (FRMORB2(0,0) and FRMIORB(1,1)) for one spin
 // ---------------------------------------------------------------------------
@@ -688,7 +719,7 @@ void fo_setup(flosic_ctx* c, int s) {
 // FO values (+ derivatives for GGA) on the mesh: phi[(ch*nf + k)*P + p]
 void fo_values(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
-  const int nf = S.nf, nb = c->nbasis, P = c->nmsh;
+  const int nf = S.nf, nb = c->nbasis, P = c->eval_n;
   const int nch = c->nch();
   const int nderv = c->nderv();
   S.phi.ensure((size_t)nch * nf * P);
@@ -699,7 +730,8 @@ void fo_values(flosic_ctx* c, int s) {
   const double one = 1.0, zero = 0.0;
   for (int p0 = 0; p0 < P; p0 += chunk) {
     const int np = std::min(chunk, P - p0);
-    launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + p0, c->d_y.p + p0, c->d_z.p + p0, c->d_basis.p, np,
+    const size_t q0 = (size_t)c->eval_p0 + p0;
+    launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
                         c->st);
     c->launches++;
     for (int ch = 0; ch < nch; ++ch) {
@@ -713,7 +745,7 @@ void fo_values(flosic_ctx* c, int s) {
 
 void coulomb(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
-  const int nf = S.nf, P = c->nmsh;
+  const int nf = S.nf, P = c->eval_n;
   const int npairs = (int)c->pairs.size(), ncalls = (int)c->calls.size();
   cudaStream_t st = c->st;
   c->d_u.ensure((size_t)nf * c->nprim * 10);
@@ -747,7 +779,7 @@ void coulomb(flosic_ctx* c, int s) {
   }
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p, c->d_coef_hl.p, c->d_momv_hl.p, c->d_tc_err.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                     c->d_mom.p, c->mesh_dev(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, mixed, scr,
+                     c->d_mom.p, c->eval_mesh(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, mixed, scr,
                      c->d_cnt.p, st);
   c->launches += c->per_fo_coulomb ? 4 : 5;
   unsigned long long cnt[3];
@@ -768,6 +800,9 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+void results_from_parts(const flosic_ctx* c, int nf, const double* parts, const double* asy,
+                        std::vector<double>& results, std::vector<double>& cfrm);
+
 // Everything of APOTNL_SIC for all FOs of spin s (apotnl_sic.F:232-623).
 void spin_potentials(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
@@ -780,7 +815,7 @@ void spin_potentials(flosic_ctx* c, int s) {
   CUDA_CHECK(cudaEventRecord(c->ev[7], st));
   coulomb(c, s);
   CUDA_CHECK(cudaEventRecord(c->ev[4], st));
-  const int nf = S.nf, P = c->nmsh;
+  const int nf = S.nf, P = c->eval_n;
   S.vpot.ensure((size_t)nf * P);
   S.y.ensure((size_t)(c->mgga ? 4 : 1) * nf * P);
   S.vh.ensure((size_t)nf * P);
@@ -790,14 +825,19 @@ void spin_potentials(flosic_ctx* c, int s) {
   // XC reads the raw Coulomb potential; keep a scaled copy out of place
   c->d_tmp.ensure((size_t)nf * P);
   CUDA_CHECK(cudaMemcpyAsync(c->d_tmp.p, S.vh.p, sizeof(double) * nf * P, cudaMemcpyDeviceToDevice, st));
-  launch_xc(c->mesh_dev(), nf, c->gga, c->mgga, c->nspn, c->xc, S.phi.p, P, c->d_tmp.p, S.vpot.p, S.y.p,
+  launch_xc(c->eval_mesh(), nf, c->gga, c->mgga, c->nspn, c->xc, S.phi.p, P, c->d_tmp.p, S.vpot.p, S.y.p,
             c->d_part.p, nblk, st);
   launch_reduce_parts(nf, nblk, c->d_part.p, c->d_sums.p, st);
   c->launches += 2;
-  std::vector<double> sums((size_t)nf * NPART), far(nf);
+  std::vector<double>& sums = S.parts;
+  sums.assign((size_t)nf * NPART, 0.0);
+  S.asy.assign(nf, 0.0);
   CUDA_CHECK(cudaMemcpyAsync(sums.data(), c->d_sums.p, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, st));
-  CUDA_CHECK(cudaMemcpy2DAsync(far.data(), sizeof(double), c->d_tmp.p + c->ifar_sorted, sizeof(double) * P,
-                               sizeof(double), nf, cudaMemcpyDeviceToHost, st));
+  // the farthest point's scaled Coulomb potential, from the shard that holds it
+  const int ifar = c->ifar_sorted - c->eval_p0;
+  if (ifar >= 0 && ifar < P)
+    CUDA_CHECK(cudaMemcpy2DAsync(S.asy.data(), sizeof(double), c->d_tmp.p + ifar, sizeof(double) * P,
+                                 sizeof(double), nf, cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaEventRecord(c->ev[5], st));
   CUDA_CHECK(cudaStreamSynchronize(st));
   c->stage_ms[0] += elapsed(c->ev[0], c->ev[1]);
@@ -805,11 +845,21 @@ void spin_potentials(flosic_ctx* c, int s) {
   c->stage_ms[2] += elapsed(c->ev[7], c->ev[3]);
   c->stage_ms[3] += elapsed(c->ev[3], c->ev[4]);
   c->stage_ms[4] += elapsed(c->ev[4], c->ev[5]);
-  S.results.assign((size_t)nf * 13, 0.0);
-  S.cfrm.assign((size_t)nf * 3, 0.0);
+  results_from_parts(c, nf, sums.data(), S.asy.data(), S.results, S.cfrm);
+  S.pot_valid = true;
+}
+
+// RESULTS(1:13) and CFRM of nf FOs (apotnl_sic.F:564-623) from the mesh sums
+// parts[k*NPART + j] (j: XCH1, XCOU, XEXX, XDEL, ERGXL, ERGXN, ERGCL, ERGCN,
+// CFRM x3) and the farthest point's scaled Coulomb potential asy[k] -- of one
+// context, or summed over the mesh shards.
+void results_from_parts(const flosic_ctx* c, int nf, const double* parts, const double* asy,
+                        std::vector<double>& results, std::vector<double>& cfrm) {
+  results.assign((size_t)nf * 13, 0.0);
+  cfrm.assign((size_t)nf * 3, 0.0);
   for (int k = 0; k < nf; ++k) {
-    const double* q = &sums[(size_t)k * NPART];
-    double* r = &S.results[(size_t)k * 13];
+    const double* q = &parts[(size_t)k * NPART];
+    double* r = &results[(size_t)k * 13];
     const double xch1 = q[0], xcou = q[1];
     double xexx = q[2];
     double xdel = q[3];
@@ -822,7 +872,7 @@ void spin_potentials(flosic_ctx* c, int s) {
     r[0] = k + 1;
     r[1] = xch1;
     r[2] = 0.0;
-    r[3] = far[k] * c->rmx;
+    r[3] = asy[k] * c->rmx;
     r[4] = xexx;
     r[5] = -xcou / 2.0;
     r[6] = xdel;
@@ -832,11 +882,8 @@ void spin_potentials(flosic_ctx* c, int s) {
     r[10] = ergcl;
     r[11] = ergxn;
     r[12] = ergcn;
-    for (int d = 0; d < 3; ++d) S.cfrm[(size_t)k * 3 + d] = q[8 + d];
-    double addit = 0.0;
-    (void)addit;
+    for (int d = 0; d < 3; ++d) cfrm[(size_t)k * 3 + d] = q[8 + d];
   }
-  S.pot_valid = true;
 }
 
 // SICLAGM (frmorb_mpi.F:456-517): SIC(j,l) = -sum_p phi_j w V_l phi_l; for a
@@ -845,7 +892,7 @@ void spin_sic(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
   if (S.sic_valid) return;
   spin_potentials(c, s);
-  const int nf = S.nf, P = c->nmsh;
+  const int nf = S.nf, P = c->eval_n;
   cudaStream_t st = c->st;
   CUDA_CHECK(cudaEventRecord(c->ev[0], st));
   c->d_sic.ensure((size_t)nf * nf);
@@ -976,6 +1023,12 @@ void require(flosic_ctx* c, bool orb) {
   if (!c->have_geom) fail(FLOSIC_ERR_STATE, "flosic_sic_set_geometry has not been called");
   if (orb && !c->have_orb) fail(FLOSIC_ERR_STATE, "flosic_sic_set_orbitals has not been called");
   CUDA_CHECK(cudaSetDevice(c->device));
+}
+
+// Entry points whose outputs cover the whole mesh need an unsharded context.
+void require_whole_mesh(flosic_ctx* c) {
+  if (c->nshards != 1)
+    fail(FLOSIC_ERR_STATE, "this context evaluates one mesh shard: use flosic_sic_cycle_partial / _combine");
 }
 
 // ---------------------------------------------------------------------------
@@ -1193,6 +1246,9 @@ int flosic_sic_set_geometry(flosic_ctx* c, int natoms, const int32_t* atom_type,
     c->d_prim_atom.upload(prim_atom.data(), prim_atom.size(), st);
     c->d_prim_ib.upload(prim_ib.data(), prim_ib.size(), st);
     sort_mesh(c, rmsh, wmsh);
+    if (c->nshards > c->ntiles)
+      fail(FLOSIC_ERR_ARG, "more mesh shards (" + std::to_string(c->nshards) + ") than mesh tiles of 128 points");
+    set_eval_range(c);
     build_pair_plan(c);
     c->d_pairs.upload(c->pairs.data(), c->pairs.size(), st);
     c->d_calls.upload(c->calls.data(), c->calls.size(), st);
@@ -1349,6 +1405,7 @@ int flosic_sic_frmiorb(flosic_ctx* c, double* tmat, double* eval, int ld) {
 int flosic_sic_coupot_sic(flosic_ctx* c, int kxxs, int kxxo, double* coulomb, double* rhog) {
   return guarded([&] {
     require(c, true);
+    require_whole_mesh(c);
     if (kxxs < 1 || kxxs > c->nspn) fail(FLOSIC_ERR_ARG, "KXXS out of range");
     const int s = kxxs - 1;
     if (kxxo < 1 || kxxo > c->nfrm[s]) fail(FLOSIC_ERR_ARG, "KXXO out of range");
@@ -1492,6 +1549,7 @@ int flosic_sic_apotnl_sic(flosic_ctx* c, double* totqnum, int lspx, int iorbx, d
                           double* pot) {
   return guarded([&] {
     require(c, true);
+    require_whole_mesh(c);
     if (lspx < 1 || lspx > c->nspn) fail(FLOSIC_ERR_ARG, "LSPX out of range");
     const int s = lspx - 1;
     if (iorbx == 0) fail(FLOSIC_ERR_ARG, "APOTNL_SIC is trying to run DFT calculation");
@@ -1517,6 +1575,7 @@ int flosic_sic_apotnl_sic(flosic_ctx* c, double* totqnum, int lspx, int iorbx, d
 int flosic_sic_siclagm(flosic_ctx* c, int lspn, double* sic, int ld) {
   return guarded([&] {
     require(c, true);
+    require_whole_mesh(c);
     if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
     const int s = lspn - 1;
     if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
@@ -1546,6 +1605,7 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
                      double* esic) {
   return guarded([&] {
     require(c, true);
+    require_whole_mesh(c);
     if (!results || !sic || !debdax || !cfrm || !esic) fail(FLOSIC_ERR_ARG, "null array argument");
     for (int s = 0; s < c->nspn; ++s)
       if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
@@ -1569,6 +1629,109 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
         for (int j = 0; j < nf; ++j) ps[(size_t)l * ld + j] = S.sic[(size_t)l * nf + j];
       spin_force(c, s, ps, ld, debdax + (size_t)s * ld * 3);
     }
+    *esic = zsic;
+  });
+}
+
+int flosic_sic_set_shard(flosic_ctx* c, int shard, int nshards) {
+  return guarded([&] {
+    if (!c) fail(FLOSIC_ERR_ARG, "null context");
+    if (nshards < 1 || shard < 0 || shard >= nshards) fail(FLOSIC_ERR_ARG, "shard must lie in [0, nshards)");
+    if (c->have_geom && nshards > c->ntiles)
+      fail(FLOSIC_ERR_ARG, "more mesh shards (" + std::to_string(nshards) + ") than mesh tiles of 128 points");
+    c->shard = shard;
+    c->nshards = nshards;
+    if (c->have_geom) set_eval_range(c);
+    invalidate(c);
+  });
+}
+
+// Packed partial sums of one shard: per spin SIC(nf,nf) | parts(NPART,nf) |
+// asy(nf), then the three work counters.
+static size_t partial_doubles(const flosic_ctx* c) {
+  size_t n = 3;
+  for (int s = 0; s < c->nspn; ++s) {
+    const size_t nf = (size_t)c->nfrm[s];
+    n += nf * nf + nf * NPART + nf;
+  }
+  return n;
+}
+
+int flosic_sic_partial_size(flosic_ctx* c, int64_t* ndoubles) {
+  return guarded([&] {
+    require(c, true);
+    if (!ndoubles) fail(FLOSIC_ERR_ARG, "null argument");
+    *ndoubles = (int64_t)partial_doubles(c);
+  });
+}
+
+int flosic_sic_cycle_partial(flosic_ctx* c, double* d_partial) {
+  return guarded([&] {
+    require(c, true);
+    if (!d_partial) fail(FLOSIC_ERR_ARG, "null partial buffer");
+    c->launches = 0;
+    c->work_near = c->work_far = c->work_terms = 0;
+    for (double& m : c->stage_ms) m = 0.0;
+    invalidate(c);
+    std::vector<double> h(partial_doubles(c), 0.0);
+    size_t o = 0;
+    for (int s = 0; s < c->nspn; ++s) {
+      const int nf = c->nfrm[s];
+      if (nf == 0) continue;
+      spin_sic(c, s);
+      const SpinCache& S = c->spin[s];
+      std::copy(S.sic.begin(), S.sic.end(), h.begin() + o);
+      o += (size_t)nf * nf;
+      std::copy(S.parts.begin(), S.parts.end(), h.begin() + o);
+      o += (size_t)nf * NPART;
+      std::copy(S.asy.begin(), S.asy.end(), h.begin() + o);
+      o += nf;
+    }
+    h[o] = (double)c->work_near;
+    h[o + 1] = (double)c->work_far;
+    h[o + 2] = (double)c->work_terms;
+    CUDA_CHECK(cudaMemcpyAsync(d_partial, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int flosic_sic_cycle_combine(flosic_ctx* c, const double* d_partial, int ld, double* results, double* sic,
+                             double* debdax, double* cfrm, double* esic) {
+  return guarded([&] {
+    require(c, true);
+    if (!d_partial || !results || !sic || !debdax || !cfrm || !esic) fail(FLOSIC_ERR_ARG, "null array argument");
+    for (int s = 0; s < c->nspn; ++s)
+      if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+    for (int s = 0; s < c->nspn; ++s)
+      if (c->nfrm[s] > 0 && !c->spin[s].fo_valid)
+        fail(FLOSIC_ERR_STATE, "flosic_sic_cycle_partial has not run on this context");
+    std::vector<double> h(partial_doubles(c));
+    CUDA_CHECK(cudaMemcpyAsync(h.data(), d_partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    size_t o = 0;
+    double zsic = 0.0;
+    for (int s = 0; s < c->nspn; ++s) {
+      const int nf = c->nfrm[s];
+      if (nf == 0) continue;
+      const double* lam = &h[o];
+      const double* parts = &h[o + (size_t)nf * nf];
+      const double* asy = &h[o + (size_t)nf * nf + (size_t)nf * NPART];
+      o += (size_t)nf * nf + (size_t)nf * NPART + nf;
+      std::vector<double> res, cf;
+      results_from_parts(c, nf, parts, asy, res, cf);
+      for (int k = 0; k < nf; ++k) {
+        for (int i = 0; i < 13; ++i) results[((size_t)s * ld + k) * 13 + i] = res[(size_t)k * 13 + i];
+        for (int d = 0; d < 3; ++d) cfrm[((size_t)s * ld + k) * 3 + d] = cf[(size_t)k * 3 + d];
+        zsic += res[(size_t)k * 13 + 8];
+      }
+      double* ps = sic + (size_t)s * ld * ld;
+      for (int l = 0; l < nf; ++l)
+        for (int j = 0; j < nf; ++j) ps[(size_t)l * ld + j] = lam[(size_t)l * nf + j];
+      spin_force(c, s, ps, ld, debdax + (size_t)s * ld * 3);
+    }
+    c->work_near = (unsigned long long)h[o];
+    c->work_far = (unsigned long long)h[o + 1];
+    c->work_terms = (unsigned long long)h[o + 2];
     *esic = zsic;
   });
 }

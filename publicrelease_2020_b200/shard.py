@@ -1,0 +1,37 @@
+"""Mesh-sharded SIC cycle: one process (rank) per GPU, each context evaluating
+one shard of the mesh points, and one in-place sum of the packed partial sums
+over the ranks -- the exchange step the reference performs with MPI_REDUCE of
+the mesh contributions (pampoiss.F:105-120) and of the SIC matrix
+(pamlmsic.F:103).
+
+The sum runs on the GPU buffer with an NCCL process group (over NVLink /
+NVSwitch on one node); with a gloo group the buffer goes through host memory.
+Any object with partial_size(), cycle_partial(address) and
+cycle_combine(address) can be driven: the CUDA library (sic.FlosicSIC) and,
+in the CPU tests, the FP64 CPU restatement of the same decomposition."""
+from __future__ import annotations
+
+
+def sharded_cycle(ctx, group=None, device=None):
+    """One SIC cycle over the ranks of `group` (torch.distributed default group
+    if None).  Every rank calls it with its own shard's context; every rank
+    returns the full cycle's outputs (RESULTS, SIC, DEBDAX, CFRM, E_SIC)."""
+    import torch
+    import torch.distributed as dist
+
+    n = ctx.partial_size()
+    backend = dist.get_backend(group)
+    on_gpu = device is not None and torch.device(device).type == "cuda"
+    buf = torch.zeros(n, dtype=torch.float64, device=device if on_gpu else "cpu")
+    ctx.cycle_partial(buf.data_ptr())
+    if on_gpu and backend == "nccl":
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+        torch.cuda.synchronize(buf.device)   # the library reads the sum on its own stream
+    elif on_gpu:
+        host = buf.cpu()
+        dist.all_reduce(host, op=dist.ReduceOp.SUM, group=group)
+        buf.copy_(host)
+        torch.cuda.synchronize(buf.device)
+    else:
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+    return ctx.cycle_combine(buf.data_ptr())

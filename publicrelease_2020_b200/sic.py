@@ -34,7 +34,8 @@ EXPORTS = [
     "flosic_sic_set_orbitals", "flosic_sic_gorbdrv", "flosic_sic_frmorb2_fmat", "flosic_sic_frmiorb",
     "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
-    "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga",
+    "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
+    "flosic_sic_cycle_partial", "flosic_sic_cycle_combine",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -74,6 +75,10 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_frmorb2_force.argtypes = [_vp, C.c_int, _dp, C.c_int, _dp]
     L.flosic_sic_cycle.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64, _i64]
+    L.flosic_sic_set_shard.argtypes = [_vp, C.c_int, C.c_int]
+    L.flosic_sic_partial_size.argtypes = [_vp, _i64]
+    L.flosic_sic_cycle_partial.argtypes = [_vp, C.c_void_p]
+    L.flosic_sic_cycle_combine.argtypes = [_vp, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
     _lib = L
     return L
 
@@ -218,6 +223,30 @@ class FlosicSIC:
                     debdax=out["debdax"].reshape(2, ld, 3), cfrm=out["cfrm"].reshape(2, ld, 3),
                     esic=float(out["esic"][0]))
 
+    def set_shard(self, shard, nshards):
+        """Evaluate only mesh shard `shard` of `nshards` (flosic_sic_set_shard)."""
+        self._check(self.L.flosic_sic_set_shard(self.h, int(shard), int(nshards)))
+
+    def partial_size(self):
+        n = np.zeros(1, dtype=np.int64)
+        self._check(self.L.flosic_sic_partial_size(self.h, n))
+        return int(n[0])
+
+    def cycle_partial(self, d_partial):
+        """This shard's packed partial sums into device memory at address d_partial."""
+        self._check(self.L.flosic_sic_cycle_partial(self.h, C.c_void_p(int(d_partial))))
+
+    def cycle_combine(self, d_partial):
+        """The cycle's outputs from the summed partials at device address d_partial."""
+        ld = self.ld
+        out = dict(results=np.zeros(2 * ld * 13), sic=np.zeros(2 * ld * ld), debdax=np.zeros(2 * ld * 3),
+                   cfrm=np.zeros(2 * ld * 3), esic=np.zeros(1))
+        self._check(self.L.flosic_sic_cycle_combine(self.h, C.c_void_p(int(d_partial)), ld, out["results"],
+                                                    out["sic"], out["debdax"], out["cfrm"], out["esic"]))
+        return dict(results=out["results"].reshape(2, ld, 13), sic=out["sic"].reshape(2, ld, ld),
+                    debdax=out["debdax"].reshape(2, ld, 3), cfrm=out["cfrm"].reshape(2, ld, 3),
+                    esic=float(out["esic"][0]))
+
     def stats(self):
         la = np.zeros(1, dtype=np.int64)
         ms = np.zeros(7)
@@ -229,9 +258,12 @@ class FlosicSIC:
                     near_evals=int(work[0]), far_evals=int(work[1]), far_terms=int(work[2]))
 
 
-def open_system(sysm, device=0):
-    """Context with geometry and orbitals of a workloads.System loaded."""
+def open_system(sysm, device=0, shard=None):
+    """Context with geometry and orbitals of a workloads.System loaded;
+    shard = (index, count) makes it evaluate one mesh shard."""
     ctx = FlosicSIC(device)
+    if shard is not None:
+        ctx.set_shard(*shard)
     ctx.set_geometry(sysm)
     ctx.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
     return ctx

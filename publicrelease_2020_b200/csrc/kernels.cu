@@ -630,7 +630,10 @@ __device__ __forceinline__ void block_reduce_parts(double v[NPART], double* out)
 // call_mgga.f90, which enter the SIC matrix through four Y channels
 // (frmorb_mpi.F:440-509):
 //   Y0 = w V phi + w grad phi . Z,   Yc = w Z_c phi + w Z_4 d_c phi  (c = x, y, z).
-__global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, int mgga, int nspn, XCParams xp,
+// MGGA selects the SCAN instance, so that the LDA/GGA instance keeps its own
+// (smaller) register allocation.
+template <bool MGGA>
+__global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, int nspn, XCParams xp,
                                                    const double* __restrict__ phi, int ldp,
                                                    double* __restrict__ vh, double* __restrict__ vpot,
                                                    double* __restrict__ y, double* __restrict__ part, int nblk) {
@@ -645,7 +648,7 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, 
     double r[10];
     const double f0 = phi[(size_t)k * ldp + p];
     r[0] = f0 * f0;
-    if (mgga) {
+    if constexpr (MGGA) {
       double f[4];
       f[0] = f0;
 #pragma unroll
@@ -723,7 +726,8 @@ void launch_xc(const MeshDev& M, int nfo, int gga, int mgga, int nspn, const int
   xp.igga[1] = xc[2];
   xp.idftyp[1] = xc[3];
   dim3 grid(nblk, nfo);
-  k_xc<<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, mgga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
+  if (mgga) k_xc<true><<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
+  else k_xc<false><<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
 }
 
 // Compensated (Neumaier) sums of the block partials, in block order.

@@ -155,6 +155,15 @@ int flosic_sic_frmorb2_force(flosic_ctx* ctx, int lspn, const double* sic, int l
 int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, double* debdax,
                      double* cfrm, double* esic);
 
+/* Adjoint of the SIC energy with respect to the FO coefficients (no single
+   reference counterpart: the basis-space form of the SIC-matrix quadrature of
+   SICLMSLV, frmorb_mpi.F:184-572).  G(ldg, nfrm) = dE_SIC/dC_FO for the FOs of
+   spin lspn at the current potentials: -(4/NSPN) sum_p w chi_mu V_k phi_k (and,
+   for SCAN, the gradient terms), so that C_FO^T G = (4/NSPN) SIC.  The FOD
+   forces and basis-centre terms follow from G by the chain rule through the
+   FO construction. */
+int flosic_sic_adjoint(flosic_ctx* ctx, int lspn, double* g, int ldg);
+
 /* Mesh sharding across GPUs (one context per GPU and rank).  The reference
    spreads the same work over MPI workers and sums their mesh contributions:
    MPI_REDUCE of COULOMB/RHOG in pampoiss.F:105-120 and of the SIC matrix in

@@ -1633,6 +1633,50 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
   });
 }
 
+int flosic_sic_adjoint(flosic_ctx* c, int lspn, double* g, int ldg) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
+    if (!g) fail(FLOSIC_ERR_ARG, "null array argument");
+    if (ldg < c->nbasis) fail(FLOSIC_ERR_ARG, "ldg smaller than the number of basis functions");
+    const int s = lspn - 1;
+    spin_potentials(c, s);
+    SpinCache& S = c->spin[s];
+    const int nf = S.nf, nb = c->nbasis, P = c->eval_n;
+    // dE_SIC/dC[mu][k] = -(4/NSPN) sum_c sum_p chi_c,mu(p) Y_c,k(p): E_SIC = (2/NSPN) sum_k XENG_k and
+    // dXENG_k/dphi_k(p) = -2 w V_k phi_k (+ the meta-GGA gradient terms, carried by Y_1..3)
+    const int nyc = c->mgga ? 4 : 1;
+    const int nderv = c->mgga ? 1 : 0;
+    const size_t budget = (size_t)3 << 30;
+    int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nyc * nb)));
+    chunk = std::max(TILE, chunk / TILE * TILE);
+    c->d_basis.ensure((size_t)nyc * nb * chunk);
+    DevBuf<double> dg;
+    dg.ensure((size_t)nb * nf);
+    const double alpha = -4.0 / c->nspn, zero = 0.0, one = 1.0;
+    bool first = true;
+    for (int p0 = 0; p0 < P; p0 += chunk) {
+      const int np = std::min(chunk, P - p0);
+      const size_t q0 = (size_t)c->eval_p0 + p0;
+      launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
+                          c->st);
+      for (int ch = 0; ch < nyc; ++ch) {
+        BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &alpha,
+                               c->d_basis.p + (size_t)ch * nb * np, np, S.y.p + (size_t)ch * nf * P + p0, P,
+                               first ? &zero : &one, dg.p, nb));
+        first = false;
+      }
+    }
+    std::vector<double> h((size_t)nb * nf);
+    CUDA_CHECK(cudaMemcpyAsync(h.data(), dg.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    dg.release();
+    for (int k = 0; k < nf; ++k)
+      for (int mu = 0; mu < nb; ++mu) g[(size_t)k * ldg + mu] = h[(size_t)k * nb + mu];
+  });
+}
+
 int flosic_sic_set_shard(flosic_ctx* c, int shard, int nshards) {
   return guarded([&] {
     if (!c) fail(FLOSIC_ERR_ARG, "null context");

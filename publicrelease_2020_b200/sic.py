@@ -35,7 +35,7 @@ EXPORTS = [
     "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
-    "flosic_sic_cycle_partial", "flosic_sic_cycle_combine",
+    "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -76,6 +76,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_cycle.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64, _i64]
     L.flosic_sic_set_shard.argtypes = [_vp, C.c_int, C.c_int]
+    L.flosic_sic_adjoint.argtypes = [_vp, C.c_int, _dp, C.c_int]
     L.flosic_sic_partial_size.argtypes = [_vp, _i64]
     L.flosic_sic_cycle_partial.argtypes = [_vp, C.c_void_p]
     L.flosic_sic_cycle_combine.argtypes = [_vp, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -222,6 +223,13 @@ class FlosicSIC:
         return dict(results=out["results"].reshape(2, ld, 13), sic=out["sic"].reshape(2, ld, ld),
                     debdax=out["debdax"].reshape(2, ld, 3), cfrm=out["cfrm"].reshape(2, ld, 3),
                     esic=float(out["esic"][0]))
+
+    def adjoint(self, lspn):
+        """G = dE_SIC/dC_FO (nbasis, nfrm) of spin lspn (flosic_sic_adjoint)."""
+        nb = self.sysm.nbasis
+        g = np.zeros(nb * self.nfrm[lspn - 1])
+        self._check(self.L.flosic_sic_adjoint(self.h, lspn, g, nb))
+        return g.reshape(self.nfrm[lspn - 1], nb).T
 
     def set_shard(self, shard, nshards):
         """Evaluate only mesh shard `shard` of `nshards` (flosic_sic_set_shard)."""

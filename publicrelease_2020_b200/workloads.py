@@ -411,3 +411,128 @@ def small_synthetic(seed=5, natoms=3, nbasis=24, nmsh=6000, nfo=4, functional="G
     """Seconds-sized synthetic system for parity tests."""
     return synthetic(natoms=natoms, nbasis=nbasis, nmsh=nmsh, nfo=nfo, box_ang=4.0, seed=seed,
                      functional=functional, nspn=nspn, min_sep=1.8)
+
+
+def _fods_conditioned(sysm, fods, rng, sigma=0.05, min_eig=1e-4, tries=50):
+    """Perturb structured FOD guesses by N(0, sigma) until the Fermi-orbital
+    overlap T T^T (frmiorb.f:426-438) of every spin is safely non-singular."""
+    out = []
+    for s, base in enumerate(fods):
+        C = sysm.psi[s * sysm.nwfs[0]: s * sysm.nwfs[0] + sysm.nwfs[s]]
+        f = base + rng.normal(0, sigma, base.shape)
+        for _ in range(tries):
+            psi = basis_values(sysm, f) @ C.T
+            rho = np.einsum("ij,ij->i", psi, psi)
+            T = psi / np.sqrt(rho)[:, None]
+            if np.linalg.eigvalsh(T @ T.T).min() > min_eig:
+                break
+            f = base + rng.normal(0, sigma, base.shape)
+        out.append(f)
+    return out
+
+
+def benzene(seed=3, nrad=40, functional="LDA-PW91*LDA-PW91"):
+    """C3: benzene, planar D6h (C-C 1.39 A, C-H 1.09 A), NRLMOL-shaped basis
+    (C 5s4p3d = 35 functions, H 4s3p1d = 19; 324 in all), 21+21 FODs at core,
+    C-H and C-C bond and pi positions, perturbed by N(0, 0.05 bohr); NSPN=2."""
+    rng = np.random.default_rng(seed)
+    b = BOHR_PER_ANG
+    ang = np.arange(6) * np.pi / 3
+    ring = np.stack([np.cos(ang), np.sin(ang), np.zeros(6)], axis=1)
+    rc, rh = 1.39 * b, (1.39 + 1.09) * b
+    rat = np.concatenate([rc * ring, rh * ring])
+    types = []
+    alp, con = _nrlmol_like_type(14, (5, 4, 3), 0.08, 2.2e4, rng)
+    types.append((alp, con, (5, 4, 3)))
+    alp, con = _nrlmol_like_type(6, (4, 3, 1), 0.08, 80.0, rng)
+    types.append((alp, con, (4, 3, 1)))
+    n_bare, bfalp, n_con, bfcon = _pack_types(types)
+    rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[0.7] * 6 + [0.5] * 6, seed=seed + 1)
+    sysm = System("benzene", rat, np.array([0] * 6 + [1] * 6, dtype=np.int32), n_bare, bfalp, n_con, bfcon,
+                  rmsh, wmsh, 2, functional)
+    nocc = 21
+    C = orthonormal_orbitals(sysm, 2 * nocc, rng)
+    sysm.psi = np.ascontiguousarray(np.concatenate([C[:nocc], C[nocc:]], axis=0))
+    sysm.nwfs = (nocc, nocc)
+    cc = 0.5 * (rat[:6] + np.roll(rat[:6], -1, axis=0))        # C-C bond midpoints
+    ch = rat[:6] + 0.5 * (rat[6:] - rat[:6])                    # C-H bond points
+    z = np.array([0.0, 0.0, 0.9])
+    up = np.concatenate([rat[:6], ch, cc, cc[0::2] + z])        # pi FODs above the plane
+    dn = np.concatenate([rat[:6], ch, cc, cc[1::2] - z])        # and below, on the other bonds
+    sysm.fods = _fods_conditioned(sysm, [up, dn], rng)
+    return sysm
+
+
+def _truncated_icosahedron():
+    """The 60 vertices (edge length 2) of the truncated icosahedron: even
+    permutations of (0, +-1, +-3p), (+-1, +-(2+p), +-2p), (+-p, +-2, +-(2p+1)),
+    p the golden ratio."""
+    p = (1 + 5 ** 0.5) / 2
+    base = [(0.0, 1.0, 3 * p), (1.0, 2 + p, 2 * p), (p, 2.0, 2 * p + 1)]
+    pts = set()
+    for x, y, z in base:
+        for sx in (1, -1):
+            for sy in (1, -1):
+                for sz in (1, -1):
+                    v = (sx * x, sy * y, sz * z)
+                    for k in range(3):  # cyclic (even) permutations
+                        pts.add(tuple(round(c, 12) for c in (v[k], v[(k + 1) % 3], v[(k + 2) % 3])))
+    return np.array(sorted(pts))
+
+
+def c60(seed=4, nrad=40, functional="MGGA-SCAN*MGGA-SCAN", rscale=0.7):
+    """C5: C60 (truncated icosahedron, radius 3.55 A), carbon 3s2p1d basis (15
+    functions, 900 in all), 180+180 FODs: 60 cores, one per single (5-6) bond,
+    two per double (6-6) bond, perturbed by N(0, 0.05 bohr); SCAN; NSPN=2.
+    nrad sets the radial shells of the atom-centred mesh (60 x nrad x 146
+    points before the cut-off)."""
+    rng = np.random.default_rng(seed)
+    v = _truncated_icosahedron()
+    rat = v / np.linalg.norm(v[0]) * 3.55 * BOHR_PER_ANG
+    d = np.linalg.norm(rat[:, None] - rat[None], axis=2)
+    bond = d[0][d[0] > 1e-6].min()
+    edges = [(i, j) for i in range(60) for j in range(i + 1, 60) if abs(d[i, j] - bond) < 0.05 * bond]
+    # 6-6 (double) bonds: edges whose two atoms share no pentagon, found as the
+    # edges not on any 5-cycle
+    nb = {i: [j for j in range(60) if j != i and abs(d[i, j] - bond) < 0.05 * bond] for i in range(60)}
+    pent = set()
+    for i in range(60):
+        for j in nb[i]:
+            for k in nb[j]:
+                if k == i:
+                    continue
+                for l in nb[k]:
+                    if l in (i, j):
+                        continue
+                    for m in nb[l]:
+                        if m in (i, j, k) or i not in nb[m]:
+                            continue
+                        for e in ((i, j), (j, k), (k, l), (l, m), (m, i)):
+                            pent.add(tuple(sorted(e)))
+    single = [e for e in edges if e in pent]
+    double = [e for e in edges if e not in pent]
+    assert len(edges) == 90 and len(single) == 60 and len(double) == 30
+    types = []
+    alp, con = _nrlmol_like_type(9, (3, 2, 1), 0.1, 5.0e3, rng)
+    types.append((alp, con, (3, 2, 1)))
+    n_bare, bfalp, n_con, bfcon = _pack_types(types)
+    rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[rscale] * 60, seed=seed + 1)
+    sysm = System("c60", rat, np.zeros(60, dtype=np.int32), n_bare, bfalp, n_con, bfcon, rmsh, wmsh, 2,
+                  functional)
+    nocc = 180
+    C = orthonormal_orbitals(sysm, 2 * nocc, rng)
+    sysm.psi = np.ascontiguousarray(np.concatenate([C[:nocc], C[nocc:]], axis=0))
+    sysm.nwfs = (nocc, nocc)
+    mid_s = np.array([0.5 * (rat[i] + rat[j]) for i, j in single])
+    out = []
+    for sgn in (1.0, -1.0):
+        dbl = []
+        for i, j in double:
+            m = 0.5 * (rat[i] + rat[j])
+            rad = m / np.linalg.norm(m)
+            tan = np.cross(rat[j] - rat[i], rad)
+            tan /= np.linalg.norm(tan)
+            dbl += [m + 0.6 * rad * sgn, m + 0.6 * tan * sgn]
+        out.append(np.concatenate([rat, mid_s, np.array(dbl)]))
+    sysm.fods = _fods_conditioned(sysm, out, rng)
+    return sysm

@@ -536,3 +536,68 @@ def c60(seed=4, nrad=40, functional="MGGA-SCAN*MGGA-SCAN", rscale=0.7):
         out.append(np.concatenate([rat, mid_s, np.array(dbl)]))
     sysm.fods = _fods_conditioned(sysm, out, rng)
     return sysm
+
+
+def alkane(ncarbon, ring=False, seed=0, nrad=12, functional="LDA-PW91*LDA-PW91"):
+    """An alkane chain C_nH_(2n+2) or cycloalkane ring C_nH_2n (n >= 3) of
+    tetrahedral carbons (C-C 1.54 A, C-H 1.09 A), carbon 3s2p1d (15 functions)
+    and hydrogen 2s1p (5 functions) bases, an atom-centred mesh of nrad
+    radial shells per atom, random orthonormal occupied orbitals and FODs near
+    the atoms; NSPN=2, one FO per occupied orbital of each spin."""
+    rng = np.random.default_rng(seed)
+    b = BOHR_PER_ANG
+    cc, chd = 1.54 * b, 1.09 * b
+    tet = np.deg2rad(109.47)
+    if ring:
+        if ncarbon < 3:
+            raise ValueError("a ring needs at least three carbons")
+        rad = cc / (2 * np.sin(np.pi / ncarbon))
+        ang = 2 * np.pi * np.arange(ncarbon) / ncarbon
+        carb = np.stack([rad * np.cos(ang), rad * np.sin(ang), 0.3 * b * (-1) ** np.arange(ncarbon)], axis=1)
+    else:
+        carb = np.zeros((ncarbon, 3))
+        for i in range(1, ncarbon):  # planar zigzag
+            carb[i] = carb[i - 1] + cc * np.array([np.sin(tet / 2), (-1) ** i * np.cos(tet / 2), 0.0])
+    hyd = []
+    for i in range(ncarbon):
+        nbr = [j for j in range(ncarbon) if j != i and np.linalg.norm(carb[j] - carb[i]) < 1.1 * cc]
+        nh = 4 - len(nbr)
+        axis = -sum((carb[j] - carb[i]) for j in nbr) if nbr else np.array([0.0, 0.0, 1.0])
+        axis = axis / np.linalg.norm(axis) if np.linalg.norm(axis) > 1e-9 else np.array([0.0, 0.0, 1.0])
+        perp = np.cross(axis, [0.0, 0.0, 1.0] if abs(axis[2]) < 0.9 else [1.0, 0.0, 0.0])
+        perp /= np.linalg.norm(perp)
+        for h in range(nh):
+            phi = 2 * np.pi * h / max(nh, 1) + rng.uniform(0, 0.2)
+            rot = np.cos(phi) * perp + np.sin(phi) * np.cross(axis, perp)
+            d = axis * np.cos(np.pi - tet) + rot * np.sin(np.pi - tet) if nh > 1 else axis
+            hyd.append(carb[i] + chd * d / np.linalg.norm(d))
+    rat = np.concatenate([carb, np.array(hyd)]) if hyd else carb
+    types = []
+    alp, con = _nrlmol_like_type(9, (3, 2, 1), 0.1, 5.0e3, rng)
+    types.append((alp, con, (3, 2, 1)))
+    alp, con = _nrlmol_like_type(5, (2, 1, 0), 0.08, 50.0, rng)
+    types.append((alp, con, (2, 1, 0)))
+    n_bare, bfalp, n_con, bfcon = _pack_types(types)
+    atype = np.array([0] * ncarbon + [1] * len(hyd), dtype=np.int32)
+    rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[0.7] * ncarbon + [0.5] * len(hyd), seed=seed + 1)
+    name = f"c{ncarbon}h{len(hyd)}" + ("-ring" if ring else "")
+    sysm = System(name, rat, atype, n_bare, bfalp, n_con, bfcon, rmsh, wmsh, 2, functional)
+    nocc = (6 * ncarbon + len(hyd)) // 2
+    C = orthonormal_orbitals(sysm, 2 * nocc, rng)
+    sysm.psi = np.ascontiguousarray(np.concatenate([C[:nocc], C[nocc:]], axis=0))
+    sysm.nwfs = (nocc, nocc)
+    sysm.fods = [place_fods(sysm, C[:nocc], rng), place_fods(sysm, C[nocc:], rng)]
+    return sysm
+
+
+def alkane_batch(n=64, seed=100, max_carbons=9, nrad=(8, 40)):
+    """C4: n molecules of uneven size from consecutive seeds -- chains and
+    rings of 1..max_carbons carbons (2..29 atoms), meshes of nrad[0]..nrad[1]
+    radial shells per atom."""
+    out = []
+    for i in range(n):
+        rng = np.random.default_rng(seed + i)
+        ring = bool(rng.integers(0, 2)) and max_carbons >= 3
+        nc = int(rng.integers(3 if ring else 1, max_carbons + 1))
+        out.append(alkane(nc, ring=ring, seed=seed + i, nrad=int(rng.integers(nrad[0], nrad[1] + 1))))
+    return out

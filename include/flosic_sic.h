@@ -107,6 +107,12 @@ int flosic_sic_getvlxc(flosic_ctx* ctx, int ndim, const double* rhog, double* vx
 int flosic_sic_getvlxc_mgga(flosic_ctx* ctx, int ndim, const double* rhog, const double* tau, double* vxc,
                             double* mixin, double* ergs);
 
+/* The MGGA#### record of FO iorbx of spin lspx (getvlxc.F:203-227, written
+   with KXXO = IRBSIC = iorbx + (lspx-1)*NWFS(1)): MIXIN(4, 2*nmsh), the
+   spin-up Hamiltonian ingredients of the FO's own density and tau, spin-down
+   half zero.  SCAN contexts only; the SIC block itself keeps them on the GPU. */
+int flosic_sic_mgga_mixin(flosic_ctx* ctx, int lspx, int iorbx, double* mixin);
+
 /* Precision of the SIC path (no counterpart in the reference).
    FLOSIC_PRECISION_FP64 (default) is the drop-in: every step in FP64.
    FLOSIC_PRECISION_MIXED forms the Coulomb potential's geometric columns

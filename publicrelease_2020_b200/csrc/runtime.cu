@@ -1633,6 +1633,44 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
   });
 }
 
+int flosic_sic_mgga_mixin(flosic_ctx* c, int lspx, int iorbx, double* mixin) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (!c->mgga) fail(FLOSIC_ERR_ARG, "MIXIN belongs to meta-GGA functionals");
+    if (lspx < 1 || lspx > c->nspn) fail(FLOSIC_ERR_ARG, "LSPX out of range");
+    const int s = lspx - 1, k = iorbx - 1;
+    if (k < 0 || k >= c->nfrm[s]) fail(FLOSIC_ERR_ARG, "IORBX out of range");
+    if (!mixin) fail(FLOSIC_ERR_ARG, "null array argument");
+    spin_potentials(c, s);
+    SpinCache& S = c->spin[s];
+    const int P = c->nmsh;
+    // the FO's density channels and tau (as k_xc forms them), then SUBVLXC's SCAN branch
+    DevBuf<double> dr, dv, dm;
+    dr.ensure((size_t)11 * P);
+    dv.ensure(2 * (size_t)P);
+    dm.ensure(4 * (size_t)P);
+    launch_density(P, S.nf, k, 4, S.phi.p, P, dr.p, P, c->st);
+    launch_fo_tau(P, S.nf, k, S.phi.p, P, dr.p + (size_t)10 * P, c->st);
+    const int nblk = std::min(1024, (P + 255) / 256);
+    c->d_part.ensure((size_t)nblk * NPART);
+    launch_xc_mgga_rhog(c->mesh_dev(), dr.p, P, dr.p + (size_t)10 * P, dv.p, dm.p, c->d_part.p, nblk, c->st);
+    std::vector<double> m(4 * (size_t)P);
+    CUDA_CHECK(cudaMemcpyAsync(m.data(), dm.p, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    dr.release();
+    dv.release();
+    dm.release();
+    for (int i = 0; i < P; ++i) {
+      const int o = c->perm[i];
+      for (int d = 0; d < 4; ++d) {
+        mixin[(size_t)4 * o + d] = m[(size_t)4 * i + d];
+        mixin[(size_t)4 * (P + o) + d] = 0.0;
+      }
+    }
+  });
+}
+
 int flosic_sic_adjoint(flosic_ctx* c, int lspn, double* g, int ldg) {
   return guarded([&] {
     require(c, true);

@@ -35,7 +35,7 @@ EXPORTS = [
     "flosic_sic_coupot_sic", "flosic_sic_getvlxc", "flosic_sic_apotnl_sic", "flosic_sic_siclagm",
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
-    "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint",
+    "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -77,6 +77,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64, _i64]
     L.flosic_sic_set_shard.argtypes = [_vp, C.c_int, C.c_int]
     L.flosic_sic_adjoint.argtypes = [_vp, C.c_int, _dp, C.c_int]
+    L.flosic_sic_mgga_mixin.argtypes = [_vp, C.c_int, C.c_int, _dp]
     L.flosic_sic_partial_size.argtypes = [_vp, _i64]
     L.flosic_sic_cycle_partial.argtypes = [_vp, C.c_void_p]
     L.flosic_sic_cycle_combine.argtypes = [_vp, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -223,6 +224,13 @@ class FlosicSIC:
         return dict(results=out["results"].reshape(2, ld, 13), sic=out["sic"].reshape(2, ld, ld),
                     debdax=out["debdax"].reshape(2, ld, 3), cfrm=out["cfrm"].reshape(2, ld, 3),
                     esic=float(out["esic"][0]))
+
+    def mgga_mixin(self, lspx, iorbx):
+        """MIXIN(4, 2*nmsh) of one FO (the MGGA#### record) as an array (2*nmsh, 4)."""
+        n = self.sysm.nmsh
+        m = np.zeros(8 * n)
+        self._check(self.L.flosic_sic_mgga_mixin(self.h, lspx, iorbx, m))
+        return m.reshape(2 * n, 4)
 
     def adjoint(self, lspn):
         """G = dE_SIC/dC_FO (nbasis, nfrm) of spin lspn (flosic_sic_adjoint)."""

@@ -170,6 +170,29 @@ int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, doub
    FO construction. */
 int flosic_sic_adjoint(flosic_ctx* ctx, int lspn, double* g, int ldg);
 
+/* SICLAG_DER / SICLM_DERSLV (siclag_der.F:2-688): the basis-centre (Pulay)
+   terms of the SIC atomic forces,
+     DERSIC(ix, lfn, A) = sum_p w V_l(p) phi_l(p) d_ix phi_l^(A)(p)
+   with phi_l^(A) the part of FO l carried by atom A's basis functions and
+   lfn = l + (s-1)*NFRM(1) over both spins; for SCAN plus the meta-GGA terms of
+   siclag_der.F:576-640 through the Hessian of the basis.  Doubled for NSPN=1
+   (siclag_der.F:153-161).  Fortran DERSIC(3, ldo, natoms): dersic[(A*ldo +
+   lfn)*3 + ix], ldo >= NFRM(1)+NFRM(2).  The caller subtracts the sum over lfn
+   from the atomic force as mfpulay.F:80-95 does.  Whole mesh only. */
+int flosic_sic_siclag_der(flosic_ctx* ctx, double* dersic, int ldo);
+
+/* SICHAM / APATCH / NEWWAY (sicham.F:922-944, sicmat.F:146-318), C1 symmetry:
+   the basis-space SIC Hamiltonian of spin LSPN in the projector form the
+   reference selects (MM=2),
+     H_mu,nu = -1/2 sum_k ( <chi_mu|V_k|phi_k><phi_k|chi_nu>
+                          + <chi_mu|phi_k><phi_k|V_k|chi_nu> ),
+   both brackets by mesh quadrature; for SCAN, V_k acts in the weak form of
+   the SIC matrix (the gradient terms of the FO's Hamiltonian ingredients).
+   ADDED to ham: packed = 0, full symmetric matrix ham[mu*ldh + nu];
+   packed = 1, HSTOR(INDX,2) order (mu = 1..N outer, nu = mu..N inner,
+   N(N+1)/2 entries).  Whole mesh only. */
+int flosic_sic_sicham(flosic_ctx* ctx, int lspn, double* ham, int ldh, int packed);
+
 /* Mesh sharding across GPUs (one context per GPU and rank).  The reference
    spreads the same work over MPI workers and sums their mesh contributions:
    MPI_REDUCE of COULOMB/RHOG in pampoiss.F:105-120 and of the SIC matrix in

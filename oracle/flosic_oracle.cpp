@@ -307,12 +307,13 @@ bool gorbdrv(const Problem& P, int nderv, int npts, const double* pts /*PTS(NSPE
 // ---------------------------------------------------------------------------
 void orbital_values(const Problem& P, const double* pts3 /*3*npts*/, int npts, int nderv,
                     int ngrad, const double* coef, int ldc, int nwf, int mode,
-                    std::vector<double>& out) {
+                    std::vector<double>& out, int only_atom = -1) {
   out.assign((size_t)nwf * ngrad * npts, 0.0);
   std::vector<double> grad((size_t)NSPEED * 10 * 6 * MAX_CON * 3);
   double pts[3 * NSPEED];
   bool iallctr[3 * MAX_CON];
   for (int a = 0; a < P.natoms; ++a) {
+    if (only_atom >= 0 && a != only_atom) continue;  // one atom's share (SICLAG_DER's site derivatives)
     const int t = P.atype[a];
     const double* R = &P.rat[3 * a];
     for (int j0 = 0; j0 < npts; j0 += NSPEED) {
@@ -2775,6 +2776,148 @@ int orc_cycle_combine(orc_problem* p, const double* in, int ld, double* results,
   }
   *esic = zsic;
   return 0;
+}
+
+// SICLAG_DER / SICLM_DERSLV (siclag_der.F:2-688), C1 symmetry:
+//   DERSIC(ix, lfn, A) = sum_p w V_l phi_l d_ix phi_l^(A)
+// with phi_l^(A) the part of FO l carried by the basis functions of atom A
+// (PSID), lfn = l + s*NFRM(1), plus for a meta-GGA the terms of
+// siclag_der.F:576-640 with the FO's Hamiltonian ingredients Z:
+//   + sum_p w [(grad phi . Z) d_ix phi^(A) + phi sum_c Z_c d_ix d_c phi^(A)
+//              + Z_4 sum_c d_c phi d_ix d_c phi^(A)];
+// doubled for NSPN=1 (siclag_der.F:153-161).  dersic[(A*ldo + lfn)*3 + ix].
+int orc_siclag_der(orc_problem* p, double* dersic, int ldo) {
+  Problem& P = p->P;
+  int rc = compute_fmat(P);
+  if (rc) return rc;
+  rc = compute_tmat(P);
+  if (rc) return rc;
+  const int nmsh = P.nmsh, nb = P.nbasis;
+  const bool mg = P.mgga();
+  std::fill(dersic, dersic + (size_t)P.natoms * ldo * 3, 0.0);
+  // Hessian channel of (d_ix, d_c): value 0, gradient 1-3, xx yy zz 4-6, xy xz yz 7-9
+  const int hch[3][3] = {{4, 7, 8}, {7, 5, 9}, {8, 9, 6}};
+  for (int s = 0; s < P.nspn; ++s) {
+    const int nf = P.nfrm[s];
+    if (nf == 0) continue;
+    std::vector<double> c;
+    fo_coefficients(P, s, c);
+    std::vector<double> pots((size_t)nf * nmsh), zm(mg ? (size_t)nf * nmsh * 4 : 0);
+    for (int k = 0; k < nf; ++k) {
+      double res[13], cf[3];
+      rc = apotnl_sic(P, s, k, &c[(size_t)k * nb], res, cf, &pots[(size_t)k * nmsh], nullptr, nullptr, false,
+                      mg ? &zm[(size_t)k * nmsh * 4] : nullptr);
+      if (rc) return rc;
+    }
+    std::vector<double> phi, pa;
+    for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
+      const int mpts = std::min(MPBLOCK, nmsh - l0);
+      orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 1, 4, c.data(), nb, nf, 1, phi);
+      for (int a = 0; a < P.natoms; ++a) {
+        orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, mg ? 2 : 1, mg ? 10 : 4, c.data(), nb, nf, 1, pa, a);
+        const int ng = mg ? 10 : 4;
+        for (int k = 0; k < nf; ++k) {
+          double* d = &dersic[((size_t)a * ldo + k + (size_t)s * P.nfrm[0]) * 3];
+          auto F = [&](int ig, int i) { return phi[((size_t)k * 4 + ig) * mpts + i]; };
+          auto A = [&](int ig, int i) { return pa[((size_t)k * ng + ig) * mpts + i]; };
+          for (int i = 0; i < mpts; ++i) {
+            const double w = P.wmsh[l0 + i];
+            const double v = pots[(size_t)k * nmsh + l0 + i];
+            double y0 = w * v * F(0, i);
+            double yc[3] = {0.0, 0.0, 0.0};
+            if (mg) {
+              const double* z = &zm[((size_t)k * nmsh + l0 + i) * 4];
+              y0 = y0 + w * (F(1, i) * z[0] + F(2, i) * z[1] + F(3, i) * z[2]);
+              for (int cc = 0; cc < 3; ++cc) yc[cc] = w * z[cc] * F(0, i) + w * z[3] * F(1 + cc, i);
+            }
+            for (int ix = 0; ix < 3; ++ix) {
+              double add = A(1 + ix, i) * y0;
+              if (mg)
+                for (int cc = 0; cc < 3; ++cc) add = add + A(hch[ix][cc], i) * yc[cc];
+              d[ix] = d[ix] + add;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (P.nspn == 1)
+    for (size_t i = 0; i < (size_t)P.natoms * ldo * 3; ++i) dersic[i] = 2.0 * dersic[i];
+  return 0;
+}
+
+// SICHAM / APATCH / NEWWAY (sicham.F:922-944, sicmat.F:146-318) in C1
+// symmetry, MM=2: per FO, BASPHI(mu,1) = sum_p w phi chi_mu and BASPHI(mu,2) =
+// -sum_p w V phi chi_mu (for a meta-GGA the weak form of the FO's Hamiltonian:
+// + w (grad phi . Z) chi_mu + w phi Z . grad chi_mu + w Z4 grad phi . grad chi_mu),
+// HAM(j,i) = BASPHI(i,2) BASPHI(j,1), HSTOR += (HAM + HAM^T)/2.  Adds into
+// ham[mu*ldh + nu].
+int orc_sicham(orc_problem* p, int spin, double* ham, int ldh) {
+  Problem& P = p->P;
+  int rc = compute_fmat(P);
+  if (rc) return rc;
+  rc = compute_tmat(P);
+  if (rc) return rc;
+  const int s = spin - 1, nf = P.nfrm[s], nb = P.nbasis, nmsh = P.nmsh;
+  const bool mg = P.mgga();
+  if (nf == 0) return 0;
+  std::vector<double> c;
+  fo_coefficients(P, s, c);
+  std::vector<double> eye((size_t)nb * nb, 0.0);
+  for (int m = 0; m < nb; ++m) eye[(size_t)m * nb + m] = 1.0;
+  std::vector<double> pots((size_t)nf * nmsh), zm(mg ? (size_t)nf * nmsh * 4 : 0);
+  for (int k = 0; k < nf; ++k) {
+    double res[13], cf[3];
+    rc = apotnl_sic(P, s, k, &c[(size_t)k * nb], res, cf, &pots[(size_t)k * nmsh], nullptr, nullptr, false,
+                    mg ? &zm[(size_t)k * nmsh * 4] : nullptr);
+    if (rc) return rc;
+  }
+  std::vector<double> b1((size_t)nf * nb, 0.0), b2((size_t)nf * nb, 0.0), phi, chi;
+  for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
+    const int mpts = std::min(MPBLOCK, nmsh - l0);
+    orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 1, 4, c.data(), nb, nf, 1, phi);
+    orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, 1, 4, eye.data(), nb, nb, 1, chi);
+    for (int k = 0; k < nf; ++k)
+      for (int m = 0; m < nb; ++m) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int i = 0; i < mpts; ++i) {
+          const double w = P.wmsh[l0 + i];
+          const double f = phi[((size_t)k * 4) * mpts + i];
+          const double x = chi[((size_t)m * 4) * mpts + i];
+          s1 = s1 + w * f * x;
+          double h = w * pots[(size_t)k * nmsh + l0 + i] * f * x;
+          if (mg) {
+            const double* z = &zm[((size_t)k * nmsh + l0 + i) * 4];
+            for (int cc = 0; cc < 3; ++cc) {
+              const double gf = phi[((size_t)k * 4 + 1 + cc) * mpts + i];
+              const double gx = chi[((size_t)m * 4 + 1 + cc) * mpts + i];
+              h = h + w * (gf * z[cc] * x + f * z[cc] * gx + z[3] * gf * gx);
+            }
+          }
+          s2 = s2 - h;
+        }
+        b1[(size_t)k * nb + m] += s1;
+        b2[(size_t)k * nb + m] += s2;
+      }
+  }
+  for (int k = 0; k < nf; ++k)
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j) {
+        // HAM(j,i) = BASPHI(i,2) BASPHI(j,1); symmetrised
+        const double hji = b2[(size_t)k * nb + i] * b1[(size_t)k * nb + j];
+        const double hij = b2[(size_t)k * nb + j] * b1[(size_t)k * nb + i];
+        ham[(size_t)i * ldh + j] += (hji + hij) / 2.0;
+      }
+  return 0;
+}
+
+// APOTNL_SIC of one orbital given by its basis coefficients (no FODs needed):
+// RESULTS(1:13) as apotnl_sic.F:564-623 writes them.
+int orc_fo_energy(orc_problem* p, int spin, const double* cfo, double* results) {
+  Problem& P = p->P;
+  std::vector<double> pot(P.nmsh);
+  double cfrm[3];
+  return apotnl_sic(P, spin - 1, 0, cfo, results, cfrm, pot.data(), nullptr, nullptr, false, nullptr);
 }
 
 int orc_set_xc_exact_density(orc_problem* p, int on) {

@@ -64,6 +64,12 @@ int orc_fo_tau(orc_problem* p, int spin, int iorb, double* tau);
 /* Test knob: XC on the untruncated (every point near) pair density while the
    Coulomb potential keeps the near/far split (0 = the reference's behaviour). */
 int orc_set_xc_exact_density(orc_problem* p, int on);
+/* SICLAG_DER: DERSIC(3, ldo, natoms) as dersic[(A*ldo + lfn)*3 + ix] */
+int orc_siclag_der(orc_problem* p, double* dersic, int ldo);
+/* APOTNL_SIC RESULTS(13) of one orbital given by its basis coefficients */
+int orc_fo_energy(orc_problem* p, int spin, const double* cfo, double* results);
+/* SICHAM's basis-space SIC Hamiltonian of one spin, added to ham[mu*ldh + nu] */
+int orc_sicham(orc_problem* p, int spin, double* ham, int ldh);
 /* Mesh-shard decomposition of one cycle (same packing as flosic_sic_cycle_partial):
    partial sums over mesh points [b, e), and the cycle's outputs from their sum. */
 int orc_partial_size(orc_problem* p, long long* n);

@@ -50,6 +50,9 @@ def lib():
         L.orc_getvlxc_mgga.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.orc_fo_tau.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.orc_set_xc_exact_density.argtypes = [C.c_void_p, C.c_int]
+        L.orc_siclag_der.argtypes = [C.c_void_p, _dp, C.c_int]
+        L.orc_fo_energy.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.orc_sicham.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
         L.orc_partial_size.argtypes = [C.c_void_p, _lp]
         L.orc_cycle_partial.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.orc_cycle_combine.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -185,6 +188,25 @@ class Oracle:
         _check(lib().orc_getvlxc_mgga(self.h, np.ascontiguousarray(rhog, dtype=np.float64).reshape(-1),
                                       np.ascontiguousarray(tau, dtype=np.float64), vxc, mix, ergs))
         return vxc.reshape(2, n), mix.reshape(n, 4), ergs
+
+    def siclag_der(self):
+        """DERSIC (natoms, nfrm(1)+nfrm(2), 3): SICLAG_DER's site derivatives."""
+        ldo = max(1, self.sysm.nfrm[0] + (self.sysm.nfrm[1] if self.sysm.nspn == 2 else 0))
+        out = np.zeros(self.sysm.natoms * ldo * 3)
+        _check(lib().orc_siclag_der(self.h, out, ldo))
+        return out.reshape(self.sysm.natoms, ldo, 3)
+
+    def sicham(self, spin):
+        """SICHAM's basis-space SIC Hamiltonian (nbasis, nbasis) of one spin."""
+        h = np.zeros((self.nbasis, self.nbasis))
+        _check(lib().orc_sicham(self.h, spin, h.reshape(-1), self.nbasis))
+        return h
+
+    def fo_energy(self, spin, cfo):
+        """APOTNL_SIC RESULTS(13) of the orbital with basis coefficients cfo."""
+        res = np.zeros(13)
+        _check(lib().orc_fo_energy(self.h, spin, np.ascontiguousarray(cfo, dtype=np.float64), res))
+        return res
 
     def set_xc_exact_density(self, on):
         """XC on the untruncated pair density (the GPU's phi^2), Coulomb unchanged."""

@@ -1715,6 +1715,139 @@ int flosic_sic_adjoint(flosic_ctx* c, int lspn, double* g, int ldg) {
   });
 }
 
+int flosic_sic_siclag_der(flosic_ctx* c, double* dersic, int ldo) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (!dersic) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int nwft = c->nfrm[0] + (c->nspn == 2 ? c->nfrm[1] : 0);
+    if (ldo < std::max(1, nwft)) fail(FLOSIC_ERR_ARG, "ldo smaller than NFRM(1)+NFRM(2)");
+    const int nb = c->nbasis, P = c->eval_n;
+    std::fill(dersic, dersic + (size_t)c->natoms * ldo * 3, 0.0);
+    // Hessian channel of (d_ix, d_c) in the basis layout: xx yy zz 4-6, xy xz yz 7-9
+    const int hch[3][3] = {{4, 7, 8}, {7, 5, 9}, {8, 9, 6}};
+    const int nderv = c->mgga ? 2 : 1, nbch = c->mgga ? 10 : 4;
+    const size_t budget = (size_t)3 << 30;
+    int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nbch * nb)));
+    chunk = std::max(TILE, chunk / TILE * TILE);
+    for (int s = 0; s < c->nspn; ++s) {
+      const int nf = c->nfrm[s];
+      if (nf == 0) continue;
+      spin_potentials(c, s);
+      SpinCache& S = c->spin[s];
+      c->d_basis.ensure((size_t)nbch * nb * chunk);
+      // H_ix = B_{1+ix}^T Y_0 (+ sum_c B_{h(ix,c)}^T Y_{1+c}), nb x nf each
+      DevBuf<double> dh;
+      dh.ensure((size_t)3 * nb * nf);
+      const double one = 1.0, zero = 0.0;
+      bool first = true;
+      for (int p0 = 0; p0 < P; p0 += chunk) {
+        const int np = std::min(chunk, P - p0);
+        const size_t q0 = (size_t)c->eval_p0 + p0;
+        launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
+                            c->st);
+        c->launches++;
+        for (int ix = 0; ix < 3; ++ix) {
+          const int nterm = c->mgga ? 4 : 1;
+          for (int t = 0; t < nterm; ++t) {
+            const int bch = t == 0 ? 1 + ix : hch[ix][t - 1];
+            BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &one,
+                                   c->d_basis.p + (size_t)bch * nb * np, np, S.y.p + (size_t)t * nf * P + p0, P,
+                                   (first && t == 0) ? &zero : &one, dh.p + (size_t)ix * nb * nf, nb));
+            c->launches++;
+          }
+        }
+        first = false;
+      }
+      std::vector<double> h((size_t)3 * nb * nf), cf((size_t)nb * nf);
+      CUDA_CHECK(cudaMemcpyAsync(h.data(), dh.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+      CUDA_CHECK(cudaMemcpyAsync(cf.data(), S.cfo.p, sizeof(double) * cf.size(), cudaMemcpyDeviceToHost, c->st));
+      CUDA_CHECK(cudaStreamSynchronize(c->st));
+      dh.release();
+      // DERSIC(ix, lfn, A) = sum_{mu on A} C_mu,k H_ix[mu, k]
+      const double fac = c->nspn == 1 ? 2.0 : 1.0;
+      for (int a = 0; a < c->natoms; ++a) {
+        const int m0 = c->aoff[a], m1 = (a + 1 < c->natoms) ? c->aoff[a + 1] : nb;
+        for (int k = 0; k < nf; ++k) {
+          double* d = dersic + ((size_t)a * ldo + k + (size_t)s * c->nfrm[0]) * 3;
+          for (int ix = 0; ix < 3; ++ix) {
+            const double* hk = &h[((size_t)ix * nf + k) * nb];
+            double acc = 0.0;
+            for (int mu = m0; mu < m1; ++mu) acc += cf[(size_t)k * nb + mu] * hk[mu];
+            d[ix] = fac * acc;
+          }
+        }
+      }
+    }
+  });
+}
+
+int flosic_sic_sicham(flosic_ctx* c, int lspn, double* ham, int ldh, int packed) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
+    if (!ham) fail(FLOSIC_ERR_ARG, "null array argument");
+    if (packed != 0 && packed != 1) fail(FLOSIC_ERR_ARG, "packed must be 0 or 1");
+    if (!packed && ldh < c->nbasis) fail(FLOSIC_ERR_ARG, "ldh smaller than the number of basis functions");
+    const int s = lspn - 1, nb = c->nbasis, P = c->eval_n;
+    const int nf = c->nfrm[s];
+    if (nf == 0) return;
+    spin_potentials(c, s);
+    SpinCache& S = c->spin[s];
+    // a = sum_c B_c^T Y_c = <chi|V_k|phi_k> (NEWWAY's BASPHI(.,2) up to its sign),
+    // b = B_0^T (w phi) = <chi|phi_k> (BASPHI(.,1)), both nb x nf
+    const int nyc = c->mgga ? 4 : 1;
+    const int nderv = c->mgga ? 1 : 0;
+    const size_t budget = (size_t)3 << 30;
+    int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nyc * nb)));
+    chunk = std::max(TILE, chunk / TILE * TILE);
+    c->d_basis.ensure((size_t)nyc * nb * chunk);
+    c->d_tmp.ensure((size_t)nf * P);
+    BLAS_CHECK(cublasDdgmm(c->blas, CUBLAS_SIDE_LEFT, P, nf, S.phi.p, P, c->d_w.p + c->eval_p0, 1, c->d_tmp.p, P));
+    DevBuf<double> dab, dh;
+    dab.ensure((size_t)2 * nb * nf);
+    dh.ensure((size_t)nb * nb);
+    double* da = dab.p;
+    double* db = dab.p + (size_t)nb * nf;
+    const double zero = 0.0, one = 1.0, mhalf = -0.5;
+    for (int p0 = 0; p0 < P; p0 += chunk) {
+      const int np = std::min(chunk, P - p0);
+      const size_t q0 = (size_t)c->eval_p0 + p0;
+      launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
+                          c->st);
+      c->launches++;
+      const double* beta = p0 == 0 ? &zero : &one;
+      for (int ch = 0; ch < nyc; ++ch)
+        BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &one,
+                               c->d_basis.p + (size_t)ch * nb * np, np, S.y.p + (size_t)ch * nf * P + p0, P,
+                               ch == 0 ? beta : &one, da, nb));
+      BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &one, c->d_basis.p, np,
+                             c->d_tmp.p + p0, P, beta, db, nb));
+      c->launches += nyc + 1;
+    }
+    // APATCH: HSTOR += (HAM + HAM^T)/2 with HAM(j,i) = BASPHI(i,2) BASPHI(j,1), summed
+    // over the spin's FOs: H = -(a b^T + b a^T)/2
+    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, nf, &mhalf, da, nb, db, nb, &zero, dh.p, nb));
+    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, nf, &mhalf, db, nb, da, nb, &one, dh.p, nb));
+    c->launches += 2;
+    std::vector<double> h((size_t)nb * nb);
+    CUDA_CHECK(cudaMemcpyAsync(h.data(), dh.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    dab.release();
+    dh.release();
+    if (packed) {
+      // HSTOR order of a C1 calculation: IBAS = 1..N outer, JBAS = IBAS..N inner
+      size_t indx = 0;
+      for (int i = 0; i < nb; ++i)
+        for (int j = i; j < nb; ++j) ham[indx++] += h[(size_t)i * nb + j];
+    } else {
+      for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) ham[(size_t)i * ldh + j] += h[(size_t)i * nb + j];
+    }
+  });
+}
+
 int flosic_sic_set_shard(flosic_ctx* c, int shard, int nshards) {
   return guarded([&] {
     if (!c) fail(FLOSIC_ERR_ARG, "null context");

@@ -36,6 +36,7 @@ EXPORTS = [
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
+    "flosic_sic_siclag_der", "flosic_sic_sicham",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -78,6 +79,8 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_set_shard.argtypes = [_vp, C.c_int, C.c_int]
     L.flosic_sic_adjoint.argtypes = [_vp, C.c_int, _dp, C.c_int]
     L.flosic_sic_mgga_mixin.argtypes = [_vp, C.c_int, C.c_int, _dp]
+    L.flosic_sic_siclag_der.argtypes = [_vp, _dp, C.c_int]
+    L.flosic_sic_sicham.argtypes = [_vp, C.c_int, _dp, C.c_int, C.c_int]
     L.flosic_sic_partial_size.argtypes = [_vp, _i64]
     L.flosic_sic_cycle_partial.argtypes = [_vp, C.c_void_p]
     L.flosic_sic_cycle_combine.argtypes = [_vp, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -238,6 +241,26 @@ class FlosicSIC:
         g = np.zeros(nb * self.nfrm[lspn - 1])
         self._check(self.L.flosic_sic_adjoint(self.h, lspn, g, nb))
         return g.reshape(self.nfrm[lspn - 1], nb).T
+
+    def siclag_der(self):
+        """DERSIC (natoms, nfrm(1)+nfrm(2), 3): the basis-centre SIC force terms
+        (flosic_sic_siclag_der, SICLAG_DER in siclag_der.F)."""
+        ldo = max(1, self.nfrm[0] + (self.nfrm[1] if self.sysm.nspn == 2 else 0))
+        out = np.zeros(self.sysm.natoms * ldo * 3)
+        self._check(self.L.flosic_sic_siclag_der(self.h, out, ldo))
+        return out.reshape(self.sysm.natoms, ldo, 3)
+
+    def sicham(self, lspn, ham=None, packed=False):
+        """Add the basis-space SIC Hamiltonian of spin lspn to ham (flosic_sic_sicham,
+        SICHAM's projector form); a new zero matrix (nbasis, nbasis), or the
+        N(N+1)/2 HSTOR-ordered vector when packed, if ham is None."""
+        nb = self.sysm.nbasis
+        if ham is None:
+            ham = np.zeros(nb * (nb + 1) // 2 if packed else (nb, nb))
+        if ham.dtype != np.float64 or not ham.flags.c_contiguous:
+            raise ValueError("ham must be a C-contiguous float64 array")
+        self._check(self.L.flosic_sic_sicham(self.h, int(lspn), ham.reshape(-1), nb, int(bool(packed))))
+        return ham
 
     def set_shard(self, shard, nshards):
         """Evaluate only mesh shard `shard` of `nshards` (flosic_sic_set_shard)."""

@@ -157,6 +157,51 @@ def test_force_equals_chain_rule_of_lowdin_rotation(functional):
         assert np.allclose(r["debdax"][spin][:n], grad, atol=1e-9, rtol=1e-9)
 
 
+@pytest.mark.parametrize("functional,atom,ix", [("LDA-PW91*LDA-PW91", 1, 2), ("MGGA-SCAN*MGGA-SCAN", 2, 0)])
+def test_siclag_der_is_basis_centre_derivative(functional, atom, ix):
+    """SICLAG_DER (siclag_der.F): 2 sum_k DERSIC(ix, k, A) is the derivative of
+    E_SIC with respect to atom A's basis centre at fixed FO coefficients and a
+    fixed mesh (for SCAN through the basis Hessian terms).  Central differences
+    agree to the quadrature error of the analytic Coulomb potential on the mesh,
+    about 1e-3 for the hydrogens of the 40-shell water mesh; the oxygen core
+    functions need a far finer mesh, so they are not used here."""
+    import copy
+    s = W.water(seed=0, nrad=40, functional=functional)
+    o = O.Oracle(s)
+    D = o.siclag_der()
+    assert D.shape == (s.natoms, sum(s.nfrm), 3)
+    h = 1e-4
+    cf = [o.fo_coefficients(sp) for sp in range(1, s.nspn + 1)]
+    e = []
+    for sg in (1.0, -1.0):
+        s2 = copy.deepcopy(s)
+        r = np.array(s2.rat, dtype=float).reshape(-1, 3)
+        r[atom, ix] += sg * h
+        s2.rat = r
+        o2 = O.Oracle(s2)
+        e.append(sum(o2.fo_energy(sp + 1, c)[8] for sp in range(s.nspn) for c in cf[sp]))
+    fd = (e[0] - e[1]) / (2 * h)
+    an = 2 * D[atom, :, ix].sum()
+    assert abs(fd - an) < 3e-3 * abs(an), (fd, an)
+
+
+@pytest.mark.parametrize("functional", ["LDA-PW91*LDA-PW91", "MGGA-SCAN*MGGA-SCAN"])
+def test_sicham_projects_to_symmetrised_sic_matrix(functional):
+    """SICHAM's projector form (sicham.F:922-944, APATCH in sicmat.F): the FOs
+    are orthonormal on the mesh, so C_FO H C_FO^T is the symmetrised SICLAGM
+    matrix (SIC + SIC^T)/2 of the same spin, to rounding."""
+    s = W.water(seed=0, nrad=14, functional=functional)
+    o = O.Oracle(s)
+    r = o.sic_cycle(nthreads=4)
+    for sp in (1, 2):
+        H = o.sicham(sp)
+        assert np.abs(H - H.T).max() == 0.0
+        C = o.fo_coefficients(sp)
+        n = s.nfrm[sp - 1]
+        sic_m = r["sic"][sp - 1][:n, :n]
+        assert np.abs(C @ H @ C.T - 0.5 * (sic_m + sic_m.T)).max() < 1e-12 * np.abs(sic_m).max()
+
+
 def test_fo_orthonormal_and_lowden():
     s = W.water(seed=3, nrad=20)
     o = O.Oracle(s)

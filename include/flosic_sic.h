@@ -193,6 +193,20 @@ int flosic_sic_siclag_der(flosic_ctx* ctx, double* dersic, int ldo);
    N(N+1)/2 entries).  Whole mesh only. */
 int flosic_sic_sicham(flosic_ctx* ctx, int lspn, double* ham, int ldh, int packed);
 
+/* The DFT side of the potential on the same mesh, basis and kernels.
+   DENSOLD (densold.F:5-277): the spin densities of the occupied Kohn-Sham
+   orbitals given to flosic_sic_set_orbitals, RHOG(NMSH, NGRAD, NSPN) with
+   NGRAD = 1 (density) or 10 (density, gradient, second derivatives xx yy zz
+   xy xz yz, as densold.F:24-43 lists them), and PHIG(NMSH, NSPN) = sum_i
+   |grad psi_i|^2 (zero for NGRAD = 1; phig may be NULL).  Orbital
+   coefficients at or below 1e-10 in magnitude are skipped as densold.F does.
+   COUPOT1 (coupot1.F:5-762, the DFTCALL branch of COUPOT_SIC): the Coulomb
+   potential COULOMB(NMSH) of the total density of those orbitals (both spins;
+   the spin-up density doubled for NSPN=1), by the same pair batches, POISSON1
+   near field and multipole far field as the FO potentials.  Whole mesh only. */
+int flosic_sic_densold(flosic_ctx* ctx, int ngrad, double* rhog, double* phig);
+int flosic_sic_coupot1(flosic_ctx* ctx, double* coulomb);
+
 /* Mesh sharding across GPUs (one context per GPU and rank).  The reference
    spreads the same work over MPI workers and sums their mesh contributions:
    MPI_REDUCE of COULOMB/RHOG in pampoiss.F:105-120 and of the SIC matrix in

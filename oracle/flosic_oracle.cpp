@@ -1290,7 +1290,8 @@ struct BatchPlan {
 };
 
 template <class Flush>
-void coupot_pairs(const Problem& P, const double* cfo, int nspn, Flush&& flush, Stats* st) {
+void coupot_pairs(const Problem& P, const double* cfo, int nspn, Flush&& flush, Stats* st,
+                  const double* dmfull = nullptr) {
   const double ZED = 1.0e-30;
   // centres: atoms (C1 symmetry: one site per atom) plus origin if far from atoms
   std::vector<std::array<double, 3>> center;
@@ -1370,11 +1371,14 @@ void coupot_pairs(const Problem& P, const double* cfo, int nspn, Flush&& flush, 
             for (int mui = kShift[li]; mui < kShift[li] + kNcomp[li]; ++mui)
               for (int ib = 0; ib < P.ncon[ti * 3 + li]; ++ib, ++iloc) {
                 int jloc = 0;
-                const double ci = cfo[P.aoff[ia] + iloc];
+                // ADD: the FO's rank-1 block (coupot_sic.F:262-281) or, for the
+                // DFT density, the occupied orbitals' density matrix (coupot1.F:380-395)
+                const double ci = dmfull ? 0.0 : cfo[P.aoff[ia] + iloc];
                 for (int lj = 0; lj <= P.lmax[tj]; ++lj)
                   for (int muj = kShift[lj]; muj < kShift[lj] + kNcomp[lj]; ++muj)
                     for (int jb = 0; jb < P.ncon[tj * 3 + lj]; ++jb, ++jloc) {
-                      const double add = ci * cfo[P.aoff[ja] + jloc];
+                      const double add = dmfull ? dmfull[(size_t)(P.aoff[ia] + iloc) * P.nbasis + P.aoff[ja] + jloc]
+                                                : ci * cfo[P.aoff[ja] + jloc];
                       const double prod = P.bcon(ti, li, ib, ialp) * P.bcon(tj, lj, jb, jalp);
                       pr.dmat[mui][muj] = pr.dmat[mui][muj] + prod * add;
                     }
@@ -2843,6 +2847,82 @@ int orc_siclag_der(orc_problem* p, double* dersic, int ldo) {
   }
   if (P.nspn == 1)
     for (size_t i = 0; i < (size_t)P.natoms * ldo * 3; ++i) dersic[i] = 2.0 * dersic[i];
+  return 0;
+}
+
+// COUPOT1 (coupot1.F:5-762): the Coulomb potential of the occupied orbitals'
+// total density, ADD(i,j,s) = sum_{iwf in s} PSI(i) PSI(j) summed over the
+// spins in POISSON1 (doubled for NSPN=1), with COUPOT_SIC's pair batches.
+int orc_coupot1(orc_problem* p, double* coulomb) {
+  Problem& P = p->P;
+  if (!P.have_orbitals) return fail("COUPOT1: no orbitals");
+  const int nb = P.nbasis, nwf = P.nwfs[0] + P.nwfs[1];
+  std::vector<double> dm((size_t)nb * nb, 0.0);
+  for (int w = 0; w < nwf; ++w)
+    for (int i = 0; i < nb; ++i) {
+      const double a = P.psi[(size_t)w * nb + i];
+      for (int j = 0; j < nb; ++j) dm[(size_t)i * nb + j] += a * P.psi[(size_t)w * nb + j];
+    }
+  std::vector<double> rhog((size_t)10 * P.nmsh);
+  for (int i = 0; i < P.nmsh; ++i) coulomb[i] = 0.0;
+  const bool gga = P.gga();
+  auto flush = [&](const std::vector<PairRec>& b, bool weird) {
+    if (weird) {
+      for (const auto& pr : b) {
+        std::vector<PairRec> one(1, pr);
+        poisson1(P, one, P.nspn, gga, false, coulomb, rhog.data(), nullptr);
+      }
+    } else {
+      poisson1(P, b, P.nspn, gga, false, coulomb, rhog.data(), nullptr);
+    }
+  };
+  coupot_pairs(P, nullptr, P.nspn, flush, nullptr, dm.data());
+  return 0;
+}
+
+// DENSOLD (densold.F:5-277): rhog[(s*ngrad + ch)*nmsh + i], phig[s*nmsh + i]
+// from the orbital values of frmiorb.f's PSIG accumulation (coefficients at or
+// below 1e-10 skipped, as densold.F:160-185).
+int orc_densold(orc_problem* p, int ngrad, double* rhog, double* phig) {
+  Problem& P = p->P;
+  if (!P.have_orbitals) return fail("DENSOLD: no orbitals");
+  if (ngrad != 1 && ngrad != 10) return fail("DENSOLD: NGRAD must be 1 or 10");
+  const int nb = P.nbasis, nmsh = P.nmsh, ns = P.nspn;
+  const int nwf = P.nwfs[0] + P.nwfs[1];
+  std::fill(rhog, rhog + (size_t)ns * ngrad * nmsh, 0.0);
+  if (phig) std::fill(phig, phig + (size_t)ns * nmsh, 0.0);
+  std::vector<double> psig;
+  for (int l0 = 0; l0 < nmsh; l0 += MPBLOCK) {
+    const int mpts = std::min(MPBLOCK, nmsh - l0);
+    orbital_values(P, &P.rmsh[3 * (size_t)l0], mpts, ngrad == 10 ? 2 : 0, ngrad, P.psi.data(), nb, nwf, 0, psig);
+    auto F = [&](int w, int ig, int i) { return psig[((size_t)w * ngrad + ig) * mpts + i]; };
+    for (int s = 0; s < ns; ++s) {
+      const int jbeg = s * P.nwfs[0];
+      double* r = rhog + (size_t)s * ngrad * nmsh + l0;
+      for (int jwf = 0; jwf < P.nwfs[s]; ++jwf) {
+        const int w = jwf + jbeg;
+        for (int i = 0; i < mpts; ++i) r[i] = r[i] + F(w, 0, i) * F(w, 0, i);
+        if (ngrad == 1) continue;
+        for (int ig = 1; ig <= 3; ++ig)
+          for (int i = 0; i < mpts; ++i) {
+            r[(size_t)ig * nmsh + i] = r[(size_t)ig * nmsh + i] + 2 * F(w, 0, i) * F(w, ig, i);
+            if (phig) phig[(size_t)s * nmsh + l0 + i] = phig[(size_t)s * nmsh + l0 + i] + F(w, ig, i) * F(w, ig, i);
+          }
+        for (int ig = 4; ig <= 6; ++ig)
+          for (int i = 0; i < mpts; ++i)
+            r[(size_t)ig * nmsh + i] =
+                r[(size_t)ig * nmsh + i] + 2 * (F(w, ig - 3, i) * F(w, ig - 3, i) + F(w, ig, i) * F(w, 0, i));
+        // (x,y) -> 7, (x,z) -> 8, (y,z) -> 9 as densold.F:232-243 (KGR = IGR+JGR+3)
+        for (int ig = 1; ig <= 2; ++ig)
+          for (int jg = ig + 1; jg <= 3; ++jg) {
+            const int kg = ig + jg + 4;
+            for (int i = 0; i < mpts; ++i)
+              r[(size_t)kg * nmsh + i] =
+                  r[(size_t)kg * nmsh + i] + 2 * (F(w, ig, i) * F(w, jg, i) + F(w, kg, i) * F(w, 0, i));
+          }
+      }
+    }
+  }
   return 0;
 }
 

@@ -70,6 +70,10 @@ int orc_siclag_der(orc_problem* p, double* dersic, int ldo);
 int orc_fo_energy(orc_problem* p, int spin, const double* cfo, double* results);
 /* SICHAM's basis-space SIC Hamiltonian of one spin, added to ham[mu*ldh + nu] */
 int orc_sicham(orc_problem* p, int spin, double* ham, int ldh);
+/* COUPOT1: Coulomb potential of the occupied orbitals' total density */
+int orc_coupot1(orc_problem* p, double* coulomb);
+/* DENSOLD: rhog[(s*ngrad + ch)*nmsh + i], phig[s*nmsh + i] (phig may be NULL) */
+int orc_densold(orc_problem* p, int ngrad, double* rhog, double* phig);
 /* Mesh-shard decomposition of one cycle (same packing as flosic_sic_cycle_partial):
    partial sums over mesh points [b, e), and the cycle's outputs from their sum. */
 int orc_partial_size(orc_problem* p, long long* n);

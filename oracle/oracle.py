@@ -53,6 +53,8 @@ def lib():
         L.orc_siclag_der.argtypes = [C.c_void_p, _dp, C.c_int]
         L.orc_fo_energy.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.orc_sicham.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
+        L.orc_coupot1.argtypes = [C.c_void_p, _dp]
+        L.orc_densold.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.orc_partial_size.argtypes = [C.c_void_p, _lp]
         L.orc_cycle_partial.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.orc_cycle_combine.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -195,6 +197,20 @@ class Oracle:
         out = np.zeros(self.sysm.natoms * ldo * 3)
         _check(lib().orc_siclag_der(self.h, out, ldo))
         return out.reshape(self.sysm.natoms, ldo, 3)
+
+    def coupot1(self):
+        """COUPOT1: Coulomb potential (nmsh) of the KS orbitals' total density."""
+        v = np.zeros(self.sysm.nmsh)
+        _check(lib().orc_coupot1(self.h, v))
+        return v
+
+    def densold(self, ngrad=10):
+        """DENSOLD: (rhog (nspn, ngrad, nmsh), phig (nspn, nmsh))."""
+        n, ns = self.sysm.nmsh, self.sysm.nspn
+        r = np.zeros(ns * ngrad * n)
+        ph = np.zeros(ns * n)
+        _check(lib().orc_densold(self.h, ngrad, r, ph))
+        return r.reshape(ns, ngrad, n), ph.reshape(ns, n)
 
     def sicham(self, spin):
         """SICHAM's basis-space SIC Hamiltonian (nbasis, nbasis) of one spin."""

@@ -261,9 +261,9 @@ __device__ void poly1d_entry(double a0, double b0, double delta, int n, int m, i
 
 __global__ void __launch_bounds__(128) k_pair_coef(const PairGeo* __restrict__ pairs,
                                                    const CallInfo* __restrict__ calls, int nfo, int nprim,
-                                                   const double* __restrict__ u, int nspn,
-                                                   double* __restrict__ coef, int8_t* __restrict__ maxfmt,
-                                                   double* __restrict__ cgp) {
+                                                   const double* __restrict__ u, const double* __restrict__ dm,
+                                                   int nspn, double* __restrict__ coef,
+                                                   int8_t* __restrict__ maxfmt, double* __restrict__ cgp) {
   __shared__ Poly1DNZ P;
   __shared__ double W[4][10][10];
   __shared__ double V[3][3][3][2];
@@ -314,14 +314,22 @@ __global__ void __launch_bounds__(128) k_pair_coef(const PairGeo* __restrict__ p
     }
   }
   __syncthreads();
+  // dm != nullptr: one density, the pair's block of a general density matrix
+  // (COUPOT1's ADD, coupot1.F:380-395); otherwise the rank-1 block u_i u_j^T of FO k
   for (int k = tid; k < nfo; k += blockDim.x) {
     double ui[10], vj[10];
-    const double* pu = u + ((size_t)k * nprim + g.pi) * 10;
-    const double* pv = u + ((size_t)k * nprim + g.pj) * 10;
+    const double* dmb = dm ? dm + (size_t)ip * 100 : nullptr;
+    if (dmb) {
 #pragma unroll
-    for (int m = 0; m < 10; ++m) {
-      ui[m] = pu[m];
-      vj[m] = pv[m];
+      for (int m = 0; m < 10; ++m) ui[m] = vj[m] = 1.0;
+    } else {
+      const double* pu = u + ((size_t)k * nprim + g.pi) * 10;
+      const double* pv = u + ((size_t)k * nprim + g.pj) * 10;
+#pragma unroll
+      for (int m = 0; m < 10; ++m) {
+        ui[m] = pu[m];
+        vj[m] = pv[m];
+      }
     }
     double cf[NCOEF];
 #pragma unroll
@@ -331,7 +339,7 @@ __global__ void __launch_bounds__(128) k_pair_coef(const PairGeo* __restrict__ p
       if (ui[mu] == 0.0) continue;
       const int nx = c_pow[mu][0], ny = c_pow[mu][1], nz = c_pow[mu][2];
       for (int nu = 0; nu < 10; ++nu) {
-        double d = ui[mu] * vj[nu] * g.times;
+        double d = (dmb ? dmb[mu * 10 + nu] : ui[mu] * vj[nu]) * g.times;
         const double r = (nspn == 1) ? d + d : d;
         if (r == 0.0) continue;
         if (slots != 1)
@@ -376,9 +384,32 @@ __global__ void __launch_bounds__(128) k_pair_coef(const PairGeo* __restrict__ p
 }
 
 void launch_pair_coef(int npairs, const PairGeo* pairs, const CallInfo* calls, int nfo, int nprim,
-                      const double* u, int nspn, double* coef, int8_t* maxfmt, double* cgp, cudaStream_t st) {
+                      const double* u, const double* dm, int nspn, double* coef, int8_t* maxfmt, double* cgp,
+                      cudaStream_t st) {
   if (npairs <= 0) return;
-  k_pair_coef<<<npairs, 128, 0, st>>>(pairs, calls, nfo, nprim, u, nspn, coef, maxfmt, cgp);
+  k_pair_coef<<<npairs, 128, 0, st>>>(pairs, calls, nfo, nprim, u, dm, nspn, coef, maxfmt, cgp);
+}
+
+// Pair blocks of the density matrix of norb orbitals (both spins):
+// dm[(ip*10 + mu)*10 + nu] = sum_i u_i(pi)[mu] u_i(pj)[nu] (coupot1.F:380-395
+// summed with the contraction of coupot1.F:405-430 folded into u).
+__global__ void __launch_bounds__(128) k_pair_dm(const PairGeo* __restrict__ pairs, int norb, int nprim,
+                                                 const double* __restrict__ u, double* __restrict__ dm) {
+  const int ip = blockIdx.x;
+  const int t = threadIdx.x;
+  if (t >= 100) return;
+  const PairGeo g = pairs[ip];
+  const int mu = t / 10, nu = t % 10;
+  double acc = 0.0;
+  for (int i = 0; i < norb; ++i)
+    acc += u[((size_t)i * nprim + g.pi) * 10 + mu] * u[((size_t)i * nprim + g.pj) * 10 + nu];
+  dm[(size_t)ip * 100 + t] = acc;
+}
+
+void launch_pair_dm(int npairs, const PairGeo* pairs, int norb, int nprim, const double* u, double* dm,
+                    cudaStream_t st) {
+  if (npairs <= 0) return;
+  k_pair_dm<<<npairs, 128, 0, st>>>(pairs, norb, nprim, u, dm);
 }
 
 // ---------------------------------------------------------------------------
@@ -777,6 +808,51 @@ __global__ void k_density(int npts, int nfo, int k, int nch, const double* __res
 void launch_density(int npts, int nfo, int k, int nch, const double* phi, int ldp, double* rhog, int ldr,
                     cudaStream_t st) {
   k_density<<<(npts + 255) / 256, 256, 0, st>>>(npts, nfo, k, nch, phi, ldp, rhog, ldr);
+}
+
+// DENSOLD (densold.F:190-250): spin densities of the occupied orbitals and,
+// for ngrad = 10, their gradients and second derivatives, plus PHIG = sum
+// |grad psi|^2, from the orbital values psig[(ch*nwf + i)*ldp + p] (ch < ngrad).
+// Orbitals [0, nw0) are spin 1, [nw0, nw0+nw1) spin 2.  rhog[(s*ngrad + ch)*ldr + p],
+// phig[s*ldr + p].
+__global__ void k_densold(int npts, int nw0, int nw1, int nspn, int ngrad, const double* __restrict__ psig, int ldp,
+                          double* __restrict__ rhog, double* __restrict__ phig, int ldr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int nwf = nw0 + nw1;
+  for (int s = 0; s < nspn; ++s) {
+    const int i0 = s == 0 ? 0 : nw0, i1 = s == 0 ? nw0 : nw0 + nw1;
+    double r[10], ph = 0.0;
+#pragma unroll
+    for (int ch = 0; ch < 10; ++ch) r[ch] = 0.0;
+    for (int i = i0; i < i1; ++i) {
+      const double f0 = psig[(size_t)i * ldp + p];
+      r[0] += f0 * f0;
+      if (ngrad == 1) continue;
+      double f[10];
+      f[0] = f0;
+#pragma unroll
+      for (int ch = 1; ch < 10; ++ch) f[ch] = psig[((size_t)ch * nwf + i) * ldp + p];
+#pragma unroll
+      for (int d = 1; d <= 3; ++d) {
+        r[d] += 2 * f[0] * f[d];
+        ph += f[d] * f[d];
+      }
+#pragma unroll
+      for (int d = 4; d <= 6; ++d) r[d] += 2 * (f[d - 3] * f[d - 3] + f[d] * f[0]);
+      r[7] += 2 * (f[1] * f[2] + f[7] * f[0]);
+      r[8] += 2 * (f[1] * f[3] + f[8] * f[0]);
+      r[9] += 2 * (f[2] * f[3] + f[9] * f[0]);
+    }
+    for (int ch = 0; ch < ngrad; ++ch) rhog[((size_t)s * ngrad + ch) * ldr + p] = r[ch];
+    if (phig) phig[(size_t)s * ldr + p] = ph;
+  }
+}
+
+void launch_densold(int npts, int nw0, int nw1, int nspn, int ngrad, const double* psig, int ldp, double* rhog,
+                    double* phig, int ldr, cudaStream_t st) {
+  if (npts <= 0) return;
+  k_densold<<<(npts + 255) / 256, 256, 0, st>>>(npts, nw0, nw1, nspn, ngrad, psig, ldp, rhog, phig, ldr);
 }
 
 // tau = |grad phi_k|^2 / 2 of FO k (GETTAU_PAR for the SIC FO).

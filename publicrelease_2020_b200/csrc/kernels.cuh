@@ -42,9 +42,19 @@ void launch_prim_u(const BasisDev& B, int nfo, const double* cfo, int ldc, doubl
 
 // Per (pair, FO): 46 potential coefficients (rows of COEF_LD doubles, zero
 // padded), Boys variant, centre-of-gravity partials.
+// dm != nullptr (nfo = 1): the pair blocks of one general density matrix
+// instead of the FOs' rank-1 blocks.
 void launch_pair_coef(int npairs, const PairGeo* pairs, const CallInfo* calls, int nfo, int nprim,
-                      const double* u, int nspn, double* coef, int8_t* maxfmt, double* cgp,
+                      const double* u, const double* dm, int nspn, double* coef, int8_t* maxfmt, double* cgp,
                       cudaStream_t st);
+
+// dm[(ip*10 + mu)*10 + nu] = sum_{i<norb} u_i(pi)[mu] u_i(pj)[nu]
+void launch_pair_dm(int npairs, const PairGeo* pairs, int norb, int nprim, const double* u, double* dm,
+                    cudaStream_t st);
+
+// DENSOLD spin densities (+ derivatives for ngrad = 10) and PHIG from orbital values
+void launch_densold(int npts, int nw0, int nw1, int nspn, int ngrad, const double* psig, int ldp, double* rhog,
+                    double* phig, int ldr, cudaStream_t st);
 
 // Per (call, FO): CG, RCUT, NPOT, skip mask and normalised multipole moments
 // momv[(c*nfo + k)*MOM_LD + lm] (skipped terms and padding zero).

@@ -743,28 +743,27 @@ void fo_values(flosic_ctx* c, int s) {
   }
 }
 
-void coulomb(flosic_ctx* c, int s) {
-  SpinCache& S = c->spin[s];
-  const int nf = S.nf, P = c->eval_n;
+// Pair coefficients, POISSON1 call set-up and the Coulomb kernels for nf
+// densities whose primitive projections are in d_u (dm == nullptr: FO k is
+// the rank-1 density of u_k), or for the one density given by its pair
+// blocks dm (nf = 1).  vh[k*P + p] over the evaluated mesh.
+void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
+  const int P = c->eval_n;
   const int npairs = (int)c->pairs.size(), ncalls = (int)c->calls.size();
   cudaStream_t st = c->st;
-  c->d_u.ensure((size_t)nf * c->nprim * 10);
-  launch_prim_u(c->basis_dev(), nf, S.cfo.p, c->nbasis, c->d_u.p, st);
-  c->launches++;
   c->d_coef.ensure((size_t)std::max(npairs, 1) * nf * COEF_LD);
   c->d_maxfmt.ensure((size_t)std::max(npairs, 1) * nf);
   c->d_cgp.ensure((size_t)std::max(npairs, 1) * nf * 4);
   c->d_callfo.ensure((size_t)std::max(ncalls, 1) * nf);
   c->d_mom.ensure((size_t)std::max(ncalls, 1) * nf * MOM_LD);
   CUDA_CHECK(cudaEventRecord(c->ev[2], st));
-  launch_pair_coef(npairs, c->d_pairs.p, c->d_calls.p, nf, c->nprim, c->d_u.p, c->nspn, c->d_coef.p,
+  launch_pair_coef(npairs, c->d_pairs.p, c->d_calls.p, nf, c->nprim, c->d_u.p, dm, c->nspn, c->d_coef.p,
                    c->d_maxfmt.p, c->d_cgp.p, st);
   c->launches++;
   launch_call_setup(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->nspn, c->d_coef.p, c->d_maxfmt.p, c->d_cgp.p,
                     c->mesh_dev(), c->d_boys.p, c->d_callfo.p, c->d_mom.p, st);
   c->launches++;
   CUDA_CHECK(cudaEventRecord(c->ev[3], st));
-  S.vh.ensure((size_t)nf * P);
   c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
   c->d_share.ensure((size_t)std::max(ncalls, 1));
   c->d_lists.ensure((size_t)2 * ncalls + 2);
@@ -779,7 +778,7 @@ void coulomb(flosic_ctx* c, int s) {
   }
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p, c->d_coef_hl.p, c->d_momv_hl.p, c->d_tc_err.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                     c->d_mom.p, c->eval_mesh(), c->d_boys.p, S.vh.p, P, c->per_fo_coulomb, mixed, scr,
+                     c->d_mom.p, c->eval_mesh(), c->d_boys.p, vh, P, c->per_fo_coulomb, mixed, scr,
                      c->d_cnt.p, st);
   c->launches += c->per_fo_coulomb ? 4 : 5;
   unsigned long long cnt[3];
@@ -792,6 +791,17 @@ void coulomb(flosic_ctx* c, int s) {
   c->work_far += cnt[1];
   c->work_terms += cnt[2];
   CUDA_CHECK(cudaGetLastError());
+}
+
+// COUPOT_SIC's Coulomb part for the FOs of spin s.
+void coulomb(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  const int nf = S.nf;
+  c->d_u.ensure((size_t)nf * c->nprim * 10);
+  launch_prim_u(c->basis_dev(), nf, S.cfo.p, c->nbasis, c->d_u.p, c->st);
+  c->launches++;
+  S.vh.ensure((size_t)nf * c->eval_n);
+  coulomb_eval(c, nf, nullptr, S.vh.p);
 }
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
@@ -1845,6 +1855,75 @@ int flosic_sic_sicham(flosic_ctx* c, int lspn, double* ham, int ldh, int packed)
       for (int i = 0; i < nb; ++i)
         for (int j = 0; j < nb; ++j) ham[(size_t)i * ldh + j] += h[(size_t)i * nb + j];
     }
+  });
+}
+
+int flosic_sic_densold(flosic_ctx* c, int ngrad, double* rhog, double* phig) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (ngrad != 1 && ngrad != 10) fail(FLOSIC_ERR_ARG, "NGRAD must be 1 or 10");
+    if (!rhog) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int nb = c->nbasis, P = c->nmsh, ns = c->nspn;
+    const int nw0 = c->nwfs[0], nw1 = ns == 2 ? c->nwfs[1] : 0, nwf = nw0 + nw1;
+    const int nderv = ngrad == 10 ? 2 : 0;
+    const size_t budget = (size_t)3 << 30;
+    int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * ngrad * (nb + nwf))));
+    chunk = std::max(TILE, chunk / TILE * TILE);
+    c->d_basis.ensure((size_t)ngrad * nb * chunk);
+    DevBuf<double> dv, dr, dph;
+    dv.ensure((size_t)ngrad * std::max(nwf, 1) * chunk);
+    dr.ensure((size_t)ns * ngrad * P);
+    if (phig) dph.ensure((size_t)ns * P);
+    const double one = 1.0, zero = 0.0;
+    for (int p0 = 0; p0 < P; p0 += chunk) {
+      const int np = std::min(chunk, P - p0);
+      launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + p0, c->d_y.p + p0, c->d_z.p + p0, c->d_basis.p, np,
+                          c->st);
+      c->launches++;
+      // PSIG (densold.F:160-185): coefficients at or below 1e-10 are skipped, as in d_psi_thr
+      if (nwf > 0)
+        for (int ch = 0; ch < ngrad; ++ch) {
+          BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, np, nwf, nb, &one,
+                                 c->d_basis.p + (size_t)ch * nb * np, np, c->d_psi_thr.p, nb, &zero,
+                                 dv.p + (size_t)ch * nwf * np, np));
+          c->launches++;
+        }
+      launch_densold(np, nw0, nw1, ns, ngrad, dv.p, np, dr.p + p0, phig ? dph.p + p0 : nullptr, P, c->st);
+      c->launches++;
+    }
+    std::vector<double> h((size_t)ns * ngrad * P), hp(phig ? (size_t)ns * P : 0);
+    CUDA_CHECK(cudaMemcpyAsync(h.data(), dr.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    if (phig) CUDA_CHECK(cudaMemcpyAsync(hp.data(), dph.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    for (int i = 0; i < P; ++i) {
+      const int o = c->perm[i];
+      for (int q = 0; q < ns * ngrad; ++q) rhog[(size_t)q * P + o] = h[(size_t)q * P + i];
+      if (phig)
+        for (int q = 0; q < ns; ++q) phig[(size_t)q * P + o] = hp[(size_t)q * P + i];
+    }
+  });
+}
+
+int flosic_sic_coupot1(flosic_ctx* c, double* coulomb) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (!coulomb) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int P = c->nmsh, nwf = c->nwfs[0] + (c->nspn == 2 ? c->nwfs[1] : 0);
+    const int npairs = (int)c->pairs.size();
+    c->d_u.ensure((size_t)std::max(nwf, 1) * c->nprim * 10);
+    if (nwf > 0) launch_prim_u(c->basis_dev(), nwf, c->d_psi.p, c->nbasis, c->d_u.p, c->st);
+    DevBuf<double> ddm, dvh;
+    ddm.ensure((size_t)std::max(npairs, 1) * 100);
+    dvh.ensure((size_t)P);
+    launch_pair_dm(npairs, c->d_pairs.p, nwf, c->nprim, c->d_u.p, ddm.p, c->st);
+    c->launches += 2;
+    coulomb_eval(c, 1, ddm.p, dvh.p);
+    std::vector<double> v(P);
+    CUDA_CHECK(cudaMemcpyAsync(v.data(), dvh.p, sizeof(double) * P, cudaMemcpyDeviceToHost, c->st));
+    CUDA_CHECK(cudaStreamSynchronize(c->st));
+    for (int i = 0; i < P; ++i) coulomb[c->perm[i]] = v[i];
   });
 }
 

@@ -36,7 +36,7 @@ EXPORTS = [
     "flosic_sic_frmorb2_force", "flosic_sic_cycle", "flosic_sic_stats", "flosic_sic_getvlxc_device",
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
-    "flosic_sic_siclag_der", "flosic_sic_sicham",
+    "flosic_sic_siclag_der", "flosic_sic_sicham", "flosic_sic_densold", "flosic_sic_coupot1",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -81,6 +81,8 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_mgga_mixin.argtypes = [_vp, C.c_int, C.c_int, _dp]
     L.flosic_sic_siclag_der.argtypes = [_vp, _dp, C.c_int]
     L.flosic_sic_sicham.argtypes = [_vp, C.c_int, _dp, C.c_int, C.c_int]
+    L.flosic_sic_densold.argtypes = [_vp, C.c_int, _dp, C.c_void_p]
+    L.flosic_sic_coupot1.argtypes = [_vp, _dp]
     L.flosic_sic_partial_size.argtypes = [_vp, _i64]
     L.flosic_sic_cycle_partial.argtypes = [_vp, C.c_void_p]
     L.flosic_sic_cycle_combine.argtypes = [_vp, C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -261,6 +263,20 @@ class FlosicSIC:
             raise ValueError("ham must be a C-contiguous float64 array")
         self._check(self.L.flosic_sic_sicham(self.h, int(lspn), ham.reshape(-1), nb, int(bool(packed))))
         return ham
+
+    def densold(self, ngrad=10):
+        """DENSOLD: (rhog (nspn, ngrad, nmsh), phig (nspn, nmsh)) of the KS orbitals."""
+        n, ns = self.sysm.nmsh, self.sysm.nspn
+        rhog = np.zeros(ns * ngrad * n)
+        phig = np.zeros(ns * n)
+        self._check(self.L.flosic_sic_densold(self.h, int(ngrad), rhog, phig.ctypes.data_as(C.c_void_p)))
+        return rhog.reshape(ns, ngrad, n), phig.reshape(ns, n)
+
+    def coupot1(self):
+        """COUPOT1: Coulomb potential (nmsh) of the KS orbitals' total density."""
+        v = np.zeros(self.sysm.nmsh)
+        self._check(self.L.flosic_sic_coupot1(self.h, v))
+        return v
 
     def set_shard(self, shard, nshards):
         """Evaluate only mesh shard `shard` of `nshards` (flosic_sic_set_shard)."""

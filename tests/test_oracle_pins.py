@@ -59,6 +59,48 @@ def test_coulomb_of_s_gaussian_is_erf_over_r(exact):
         assert st[4] > 0  # some points went through the multipole far field
 
 
+def test_coupot1_and_densold_of_s_gaussian():
+    """DENSOLD and COUPOT1 of one s orbital per spin: rho_s = psi^2 with its
+    gradient, Hessian and PHIG = |grad psi|^2 in closed form; the Coulomb
+    potential of both spins is 2 erf(sqrt(2a) r)/r."""
+    a = 0.8
+    s = one_gaussian_system(a)
+    o = O.Oracle(s)
+    d = s.rmsh - s.rat[0]
+    r = np.linalg.norm(d, axis=1)
+    v = o.coupot1()
+    ref = 2 * erf(np.sqrt(2 * a) * r) / r
+    assert np.max(np.abs(v - ref) / ref) < 1e-10
+    rg, ph = o.densold(10)
+    g = (2 * a / math.pi) ** 0.75 * np.exp(-a * r ** 2)
+    rho = g * g
+    for sp in (0, 1):
+        assert np.abs(rg[sp, 0] - rho).max() < 1e-14
+        assert np.abs(rg[sp, 1:4] - (-4 * a * d * rho[:, None]).T).max() < 1e-14
+        assert np.abs(ph[sp] - (4 * a * a * (d ** 2).sum(1) * rho)).max() < 1e-14
+        for ch, (i, j) in {4: (0, 0), 5: (1, 1), 6: (2, 2), 7: (0, 1), 8: (0, 2), 9: (1, 2)}.items():
+            h = (16 * a * a * d[:, i] * d[:, j] - (4 * a if i == j else 0.0)) * rho
+            assert np.abs(rg[sp, ch] - h).max() < 1e-13
+    r1, _ = o.densold(1)
+    assert np.array_equal(r1[:, 0], rg[:, 0])
+
+
+@pytest.mark.parametrize("case", ["water", "synthetic_nspn1"])
+def test_coupot1_is_sum_of_fo_potentials(case):
+    """The FOs are an orthogonal rotation of the occupied orbitals, so the
+    total density's potential (COUPOT1) is the sum of the FO potentials
+    (COUPOT_SIC) up to the multipole truncation (EPSMULTI 1e-6), whose call
+    set-up depends on the density; DENSOLD integrates to the electron count."""
+    s = W.water(seed=0, nrad=14) if case == "water" else W.small_synthetic(seed=5, nspn=1)
+    o = O.Oracle(s)
+    v = o.coupot1()
+    tot = sum(o.coupot_sic(sp, k + 1)[0] for sp in range(1, s.nspn + 1) for k in range(s.nfrm[sp - 1]))
+    assert np.abs(v - tot).max() < 1e-6 * np.abs(v).max()
+    rg, _ = o.densold(1)
+    for sp in range(s.nspn):
+        assert abs((rg[sp, 0] * s.wmsh).sum() - s.nwfs[sp]) < 1e-8
+
+
 def test_lebedev_and_harmonics_orthonormal():
     ang, w = O.lebedev19()
     assert ang.shape == (146, 3)

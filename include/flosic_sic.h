@@ -167,7 +167,8 @@ int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, doub
    spin lspn at the current potentials: -(4/NSPN) sum_p w chi_mu V_k phi_k (and,
    for SCAN, the gradient terms), so that C_FO^T G = (4/NSPN) SIC.  The FOD
    forces and basis-centre terms follow from G by the chain rule through the
-   FO construction. */
+   FO construction.  On a mesh shard the result is the shard's partial sum,
+   to be summed over the shards (the dE/dC part of the exchange). */
 int flosic_sic_adjoint(flosic_ctx* ctx, int lspn, double* g, int ldg);
 
 /* SICLAG_DER / SICLM_DERSLV (siclag_der.F:2-688): the basis-centre (Pulay)
@@ -178,7 +179,9 @@ int flosic_sic_adjoint(flosic_ctx* ctx, int lspn, double* g, int ldg);
    siclag_der.F:576-640 through the Hessian of the basis.  Doubled for NSPN=1
    (siclag_der.F:153-161).  Fortran DERSIC(3, ldo, natoms): dersic[(A*ldo +
    lfn)*3 + ix], ldo >= NFRM(1)+NFRM(2).  The caller subtracts the sum over lfn
-   from the atomic force as mfpulay.F:80-95 does.  Whole mesh only. */
+   from the atomic force as mfpulay.F:80-95 does.  On a mesh shard
+   (flosic_sic_set_shard) the result is the shard's partial sum over its
+   points; the shards' results add up to the whole mesh's. */
 int flosic_sic_siclag_der(flosic_ctx* ctx, double* dersic, int ldo);
 
 /* SICHAM / APATCH / NEWWAY (sicham.F:922-944, sicmat.F:146-318), C1 symmetry:

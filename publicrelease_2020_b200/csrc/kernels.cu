@@ -435,62 +435,38 @@ __device__ __forceinline__ void box_dist2(const double lo[3], const double hi[3]
 }
 
 constexpr int SETUP_THREADS = 160;
+constexpr int SETUP1_THREADS = 128;
+constexpr int GEO_LD = 48;  // per sphere point: 35 monomials, F_0..2 (s3), F_0..3 (s4), F_0..4 (s5)
 
-__global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __restrict__ calls,
-                                                              const PairGeo* __restrict__ pairs, int nfo,
-                                                              int nspn, const double* __restrict__ coef,
-                                                              const int8_t* __restrict__ maxfmt,
-                                                              const double* __restrict__ cgp, MeshDev M,
-                                                              const double* __restrict__ boys_tab,
-                                                              CallFO* __restrict__ out,
-                                                              double* __restrict__ momv) {
-  extern __shared__ double sm[];  // [NANG][NMOM] products, then NANG potentials
-  double* prod = sm;
-  double* vang = sm + NANG * NMOM;
-  __shared__ double s_cg[3], s_rcut;
-  __shared__ int s_far, s_stop;
-  const int c = blockIdx.x, k = blockIdx.y, tid = threadIdx.x;
-  const CallInfo ci = calls[c];
+// RCUT of a call around its centre of gravity (poisson1.f:522-538).
+__device__ double call_rcut(const CallInfo& ci, const PairGeo* __restrict__ pairs, const double cgr[3]) {
+  double dmax = 0.0;
+  for (int q = 0; q < ci.np; ++q) {
+    const double* C = pairs[ci.p0 + q].C;
+    const double dist = sqrt(sqdist_rn(C[0], C[1], C[2], cgr));
+    if (dist > dmax) dmax = dist;
+  }
+  double rcut = sqrt(30.0 / ci.delta_min) + dmax;
+  const double pirc = 1.0 / (4 * atan(1.0));
+  const double fact = sqrt(pirc / (pirc + LM + 1));
+  const double dist = 2 * dmax / pow(1.0e-6 / fact, 1.0 / (LM + 1));
+  return fmax(rcut, dist);
+}
+
+// Far-point count of a call (all threads of the block), with early exit once
+// NPOT=2 is certain; returns NPOT of the cost model (poisson1.f:548-583) and
+// the count in nfar.
+__device__ int call_far_count(const CallInfo& ci, const MeshDev& M, const double cg[3], double rcut2, int* s_far,
+                              int* s_stop, int& nfar) {
+  const int tid = threadIdx.x, nth = blockDim.x;
   if (tid == 0) {
-    double cg[4] = {0, 0, 0, 0};
-    for (int q = 0; q < ci.np; ++q) {
-      const double* p = cgp + ((size_t)(ci.p0 + q) * nfo + k) * 4;
-      for (int i = 0; i < 4; ++i) cg[i] += p[i];
-    }
-    double cgr[3];
-    if (cg[3] != 0.0 && ci.slots > 1) {
-      for (int d = 0; d < 3; ++d) cgr[d] = cg[d] / cg[3];
-    } else {
-      for (int d = 0; d < 3; ++d) {
-        double s = 0.0;
-        for (int q = 0; q < ci.np; ++q) s = s - (-pairs[ci.p0 + q].C[d]);
-        cgr[d] = (nspn * s) / ci.slots;
-      }
-    }
-    double dmax = 0.0;
-    for (int q = 0; q < ci.np; ++q) {
-      const double* C = pairs[ci.p0 + q].C;
-      const double dist = sqrt(sqdist_rn(C[0], C[1], C[2], cgr));
-      if (dist > dmax) dmax = dist;
-    }
-    double rcut = sqrt(30.0 / ci.delta_min) + dmax;
-    const double pirc = 1.0 / (4 * atan(1.0));
-    const double fact = sqrt(pirc / (pirc + LM + 1));
-    const double dist = 2 * dmax / pow(1.0e-6 / fact, 1.0 / (LM + 1));
-    rcut = fmax(rcut, dist);
-    for (int d = 0; d < 3; ++d) s_cg[d] = cgr[d];
-    s_rcut = rcut;
-    s_far = 0;
-    s_stop = 0;
+    *s_far = 0;
+    *s_stop = 0;
   }
   __syncthreads();
-  const double cg[3] = {s_cg[0], s_cg[1], s_cg[2]};
-  const double rcut = s_rcut;
-  const double rcut2 = __dmul_rn(rcut, rcut);
-  // far-point count with early exit once NPOT=2 is certain
   const double slots = (double)ci.slots;
   const double thr = 1.36 * slots * NANG / (1.36 * slots - 0.99) + 2.0;
-  for (int t0 = 0; t0 < M.ntiles; t0 += SETUP_THREADS) {
+  for (int t0 = 0; t0 < M.ntiles; t0 += nth) {
     const int t = t0 + tid;
     int myfar = 0;
     if (t < M.ntiles) {
@@ -508,20 +484,65 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
           if (sqdist_rn(M.x[p], M.y[p], M.z[p], cg) > rcut2) ++myfar;
       }
     }
-    if (myfar) atomicAdd(&s_far, myfar);
+    if (myfar) atomicAdd(s_far, myfar);
     __syncthreads();
-    if (tid == 0 && (double)s_far > thr) s_stop = 1;
+    if (tid == 0 && (double)*s_far > thr) *s_stop = 1;
     __syncthreads();
-    if (s_stop) break;
+    if (*s_stop) break;
   }
+  nfar = *s_far;
   int npot = 2;
-  const int nfar = s_far;
-  if (!s_stop) {
+  if (!*s_stop) {
     const double cls = (double)(M.n - nfar);
     const double cost1 = 1.36 * (cls + NANG) * slots + 0.99 * (double)nfar;
     const double cost2 = 1.36 * ((double)nfar + cls) * slots;
     if (cost2 < cost1) npot = 1;
   }
+  return npot;
+}
+
+__global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const int* __restrict__ list,
+                                                              const CallInfo* __restrict__ calls,
+                                                              const PairGeo* __restrict__ pairs, int nfo,
+                                                              int nspn, const double* __restrict__ coef,
+                                                              const int8_t* __restrict__ maxfmt,
+                                                              const double* __restrict__ cgp, MeshDev M,
+                                                              const double* __restrict__ boys_tab,
+                                                              CallFO* __restrict__ out,
+                                                              double* __restrict__ momv) {
+  extern __shared__ double sm[];  // [NANG][NMOM] products, then NANG potentials
+  double* prod = sm;
+  double* vang = sm + NANG * NMOM;
+  __shared__ double s_cg[3], s_rcut;
+  __shared__ int s_far, s_stop;
+  const int c = list[blockIdx.x], k = blockIdx.y, tid = threadIdx.x;
+  const CallInfo ci = calls[c];
+  if (tid == 0) {
+    double cg[4] = {0, 0, 0, 0};
+    for (int q = 0; q < ci.np; ++q) {
+      const double* p = cgp + ((size_t)(ci.p0 + q) * nfo + k) * 4;
+      for (int i = 0; i < 4; ++i) cg[i] += p[i];
+    }
+    double cgr[3];
+    if (cg[3] != 0.0 && ci.slots > 1) {
+      for (int d = 0; d < 3; ++d) cgr[d] = cg[d] / cg[3];
+    } else {
+      for (int d = 0; d < 3; ++d) {
+        double s = 0.0;
+        for (int q = 0; q < ci.np; ++q) s = s - (-pairs[ci.p0 + q].C[d]);
+        cgr[d] = (nspn * s) / ci.slots;
+      }
+    }
+    const double rcut = call_rcut(ci, pairs, cgr);
+    for (int d = 0; d < 3; ++d) s_cg[d] = cgr[d];
+    s_rcut = rcut;
+  }
+  __syncthreads();
+  const double cg[3] = {s_cg[0], s_cg[1], s_cg[2]};
+  const double rcut = s_rcut;
+  const double rcut2 = __dmul_rn(rcut, rcut);
+  int nfar = 0;
+  const int npot = call_far_count(ci, M, cg, rcut2, &s_far, &s_stop, nfar);
   CallFO* o = out + (size_t)c * nfo + k;
   if (tid == 0) {
     o->cg[0] = cg[0];
@@ -616,19 +637,158 @@ __global__ void __launch_bounds__(SETUP_THREADS) k_call_setup(const CallInfo* __
   }
 }
 
+// The same set-up for a call of one slot (one pair, NSPN=1), all FOs in one
+// block: CG is the pair centre (poisson1.f:515-520), so CG, RCUT, the far
+// count and NPOT are the same for every FO and are formed once; the sphere
+// points' Boys values, monomials and weighted harmonics are formed once and
+// each thread (FO) contracts them with its coefficients.  Every FO's numbers
+// are bitwise those of k_call_setup: the same expressions, in the same order.
+__global__ void __launch_bounds__(SETUP1_THREADS) k_call_setup_single(
+    const int* __restrict__ list, const CallInfo* __restrict__ calls, const PairGeo* __restrict__ pairs, int nfo,
+    int nspn, const double* __restrict__ coef, const int8_t* __restrict__ maxfmt, MeshDev M,
+    const double* __restrict__ boys_tab, CallFO* __restrict__ out, double* __restrict__ momv) {
+  extern __shared__ double sm[];  // [NANG][GEO_LD] geometry, then [NANG][NMOM] w Y
+  double* geo = sm;
+  double* wy = sm + NANG * GEO_LD;
+  __shared__ double s_cg[3], s_rcut, s_vf[NMOM];
+  __shared__ int s_far, s_stop;
+  const int c = list[blockIdx.x], tid = threadIdx.x;
+  const CallInfo ci = calls[c];
+  if (tid < NMOM) {
+    // normalisation sqrt(NRUN (2l+1)/4pi (l-m)!/(l+m)!) of moment tid, as k_call_setup
+    int l = 0;
+    while ((l + 1) * (l + 1) <= tid) ++l;
+    const int j = tid - l * l;
+    const int m = (j + 1) / 2;
+    const int nrun = (m == 0) ? 1 : 2;
+    double facfc = (2 * l + 1) * (1.0 / (16 * atan(1.0)));
+    for (int mm = 0; mm < m; ++mm) facfc = facfc / ((l - mm > 1 ? l - mm : 1) * (l + mm + 1));
+    s_vf[tid] = sqrt(nrun * facfc);
+  }
+  if (tid == 0) {
+    double cgr[3];
+    for (int d = 0; d < 3; ++d) {
+      double s = 0.0;
+      for (int q = 0; q < ci.np; ++q) s = s - (-pairs[ci.p0 + q].C[d]);
+      cgr[d] = (nspn * s) / ci.slots;
+    }
+    const double rcut = call_rcut(ci, pairs, cgr);
+    for (int d = 0; d < 3; ++d) s_cg[d] = cgr[d];
+    s_rcut = rcut;
+  }
+  __syncthreads();
+  const double cg[3] = {s_cg[0], s_cg[1], s_cg[2]};
+  const double rcut = s_rcut;
+  const double rcut2 = __dmul_rn(rcut, rcut);
+  int nfar = 0;
+  const int npot = call_far_count(ci, M, cg, rcut2, &s_far, &s_stop, nfar);
+  for (int k = tid; k < nfo; k += blockDim.x) {
+    CallFO* o = out + (size_t)c * nfo + k;
+    o->cg[0] = cg[0];
+    o->cg[1] = cg[1];
+    o->cg[2] = cg[2];
+    o->rcut = rcut;
+    o->rcut2 = (npot == 1) ? DBL_MAX : rcut2;
+    o->npot = npot;
+    o->nfar = (npot == 1) ? 0 : nfar;
+    if (npot == 1 || nfar == 0) {
+      double* mv = momv + ((size_t)c * nfo + k) * MOM_LD;
+      for (int m = 0; m < MOM_LD; ++m) mv[m] = 0.0;
+      o->keep = 0ull;
+      o->lmax = 0;
+    }
+  }
+  if (npot == 1 || nfar == 0) return;
+  // the sphere points: Boys values and monomials of the pair, weighted harmonics
+  const PairGeo& g = pairs[ci.p0];
+  for (int i = tid; i < NANG; i += blockDim.x) {
+    const double q[3] = {cg[0] + c_leb_ang[3 * i] * rcut, cg[1] + c_leb_ang[3 * i + 1] * rcut,
+                         cg[2] + c_leb_ang[3 * i + 2] * rcut};
+    const double rx = q[0] - g.C[0], ry = q[1] - g.C[1], rz = q[2] - g.C[2];
+    const double xx = g.delta * (rz * rz + ry * ry + rx * rx);
+    const double chgd = exp(-xx);
+    double* gi = geo + (size_t)i * GEO_LD;
+    double s3[3], s4[4], s5[5], mono[35];
+    boys_all(boys_tab, xx, chgd, s3, s4, s5);
+    monomials(rx, ry, rz, mono);
+    for (int t = 0; t < 35; ++t) gi[t] = mono[t];
+    for (int t = 0; t < 3; ++t) gi[35 + t] = s3[t];
+    for (int t = 0; t < 4; ++t) gi[38 + t] = s4[t];
+    for (int t = 0; t < 5; ++t) gi[42 + t] = s5[t];
+    const double hn = 1.0 / sqrt(rcut * rcut);
+    double Y[NMOM];
+    harmonics6(LM, hn * (c_leb_ang[3 * i] * rcut), hn * (c_leb_ang[3 * i + 1] * rcut),
+               hn * (c_leb_ang[3 * i + 2] * rcut), Y);
+    for (int m = 0; m < NMOM; ++m) wy[(size_t)i * NMOM + m] = __dmul_rn(c_leb_w[i], Y[m]);
+  }
+  __syncthreads();
+  const double h = sqrt(rcut * rcut);
+  const double ri1 = 1.0 / rcut;
+  for (int k = tid; k < nfo; k += blockDim.x) {
+    const size_t pk = (size_t)ci.p0 * nfo + k;
+    const double* cf = coef + pk * COEF_LD;
+    const int fmt = maxfmt[pk];
+    double acc[NMOM];
+#pragma unroll
+    for (int m = 0; m < NMOM; ++m) acc[m] = 0.0;
+    for (int i = 0; i < NANG; ++i) {
+      const double* gi = geo + (size_t)i * GEO_LD;
+      double v = 0.0;
+      v += pair_potential(cf, gi, fmt, gi + 35, gi + 38, gi + 42);
+      const double* wyi = wy + (size_t)i * NMOM;
+#pragma unroll
+      for (int m = 0; m < NMOM; ++m) acc[m] = __dadd_rn(acc[m], __dmul_rn(wyi[m], v));
+    }
+    // moments, skip rule and normalisation as k_call_setup
+    unsigned long long keep = 0ull;
+    int lmx = 0;
+    double rt = ri1;
+    double rl = h;
+#pragma unroll
+    for (int l = 0; l <= LM; ++l) {
+#pragma unroll
+      for (int j = 0; j <= 2 * l; ++j) {
+        const int m = l * l + j;
+        acc[m] = acc[m] * rl;
+        if (!(fabs((2 * l + 1) * acc[m] * rt) < 1.0e-12)) {
+          keep |= (1ull << m);
+          lmx = l;
+        }
+      }
+      rt *= ri1;
+      rl = h * rl;
+    }
+    CallFO* o = out + (size_t)c * nfo + k;
+    o->keep = keep;
+    o->lmax = lmx;
+    double* mv = momv + ((size_t)c * nfo + k) * MOM_LD;
+#pragma unroll
+    for (int t = 0; t < NMOM; ++t) mv[t] = ((keep >> t) & 1ull) ? acc[t] * s_vf[t] : 0.0;
+#pragma unroll
+    for (int t = NMOM; t < MOM_LD; ++t) mv[t] = 0.0;
+  }
+}
+
 void init_call_setup() {
   cudaFuncSetAttribute(k_call_setup, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(sizeof(double) * (NANG * NMOM + NANG)));
+  cudaFuncSetAttribute(k_call_setup_single, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(double) * NANG * (GEO_LD + NMOM)));
 }
 
-void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, int nspn,
-                       const double* coef, const int8_t* maxfmt, const double* cgp, const MeshDev& M,
-                       const double* boys_tab, CallFO* cfo, double* momv, cudaStream_t st) {
+void launch_call_setup(int ncalls, const int* list, int nsingle, const CallInfo* calls, const PairGeo* pairs,
+                       int nfo, int nspn, const double* coef, const int8_t* maxfmt, const double* cgp,
+                       const MeshDev& M, const double* boys_tab, CallFO* cfo, double* momv, cudaStream_t st) {
   if (ncalls <= 0) return;
-  const size_t smem = sizeof(double) * (NANG * NMOM + NANG);
-  dim3 grid(ncalls, nfo);
-  k_call_setup<<<grid, SETUP_THREADS, smem, st>>>(calls, pairs, nfo, nspn, coef, maxfmt, cgp, M, boys_tab,
-                                                   cfo, momv);
+  if (nsingle > 0)
+    k_call_setup_single<<<nsingle, SETUP1_THREADS, sizeof(double) * NANG * (GEO_LD + NMOM), st>>>(
+        list, calls, pairs, nfo, nspn, coef, maxfmt, M, boys_tab, cfo, momv);
+  if (ncalls > nsingle) {
+    const size_t smem = sizeof(double) * (NANG * NMOM + NANG);
+    dim3 grid(ncalls - nsingle, nfo);
+    k_call_setup<<<grid, SETUP_THREADS, smem, st>>>(list + nsingle, calls, pairs, nfo, nspn, coef, maxfmt, cgp, M,
+                                                     boys_tab, cfo, momv);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -59,9 +59,11 @@ void launch_densold(int npts, int nw0, int nw1, int nspn, int ngrad, const doubl
 // Per (call, FO): CG, RCUT, NPOT, skip mask and normalised multipole moments
 // momv[(c*nfo + k)*MOM_LD + lm] (skipped terms and padding zero).
 void init_call_setup();
-void launch_call_setup(int ncalls, const CallInfo* calls, const PairGeo* pairs, int nfo, int nspn,
-                       const double* coef, const int8_t* maxfmt, const double* cgp, const MeshDev& M,
-                       const double* boys_tab, CallFO* cfo, double* momv, cudaStream_t st);
+// list: the nsingle calls of one slot (one pair, NSPN=1; CG/RCUT/NPOT shared
+// by all FOs, set up once per call), then the other calls (once per FO).
+void launch_call_setup(int ncalls, const int* list, int nsingle, const CallInfo* calls, const PairGeo* pairs,
+                       int nfo, int nspn, const double* coef, const int8_t* maxfmt, const double* cgp,
+                       const MeshDev& M, const double* boys_tab, CallFO* cfo, double* momv, cudaStream_t st);
 
 // Coulomb potential of every FO at every mesh point, vh[k*ldv + p], on the
 // FP64 tensor cores (csrc/coulomb_mma.cu).  Calls whose near/far geometry is

@@ -330,6 +330,8 @@ struct flosic_ctx {
   DevBuf<int8_t> d_maxfmt, d_pairfmt;
   DevBuf<CallShare> d_share;
   DevBuf<int> d_lists, d_tc_err;
+  DevBuf<int> d_setup_list;  // one-slot calls first (nsingle), then the others
+  int nsingle = 0;
   DevBuf<float> d_coef_hl, d_momv_hl;
   bool per_fo_coulomb = false;   // FLOSIC_COULOMB=perfo: every call through the per-FO kernel (A/B checks)
   int precision = FLOSIC_PRECISION_FP64;
@@ -760,8 +762,8 @@ void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
   launch_pair_coef(npairs, c->d_pairs.p, c->d_calls.p, nf, c->nprim, c->d_u.p, dm, c->nspn, c->d_coef.p,
                    c->d_maxfmt.p, c->d_cgp.p, st);
   c->launches++;
-  launch_call_setup(ncalls, c->d_calls.p, c->d_pairs.p, nf, c->nspn, c->d_coef.p, c->d_maxfmt.p, c->d_cgp.p,
-                    c->mesh_dev(), c->d_boys.p, c->d_callfo.p, c->d_mom.p, st);
+  launch_call_setup(ncalls, c->d_setup_list.p, c->nsingle, c->d_calls.p, c->d_pairs.p, nf, c->nspn, c->d_coef.p,
+                    c->d_maxfmt.p, c->d_cgp.p, c->mesh_dev(), c->d_boys.p, c->d_callfo.p, c->d_mom.p, st);
   c->launches++;
   CUDA_CHECK(cudaEventRecord(c->ev[3], st));
   c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
@@ -923,94 +925,69 @@ void spin_sic(flosic_ctx* c, int s) {
 
 // FRMORB2(-s,-1) force branch (frmorb2.F:586-717), with the O(n^4) loops of
 // the second term regrouped into O(n^3) products.
+// C = A B, row-major A (n x k), B (k x m), C (n x m).
+void mat_mul(const double* A, const double* B, double* C, int n, int k, int m) {
+  for (size_t i = 0; i < (size_t)n * m; ++i) C[i] = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double* ci = C + (size_t)i * m;
+    for (int p = 0; p < k; ++p) {
+      const double a = A[(size_t)i * k + p];
+      if (a == 0.0) continue;
+      const double* bp = B + (size_t)p * m;
+      for (int j = 0; j < m; ++j) ci[j] += a * bp[j];
+    }
+  }
+}
+
 void spin_force(flosic_ctx* c, int s, const double* sic /* SIC(j,l) at [l*ld + j] */, int ld, double* deb) {
   fo_setup(c, s);
   SpinCache& S = c->spin[s];
   const int nf = S.nf, nw = S.nw;
-  auto fm = [&](int kwf, int ifm, int K) { return S.fmat[((size_t)K * nf + ifm) * nw + kwf]; };
   auto t0 = std::chrono::steady_clock::now();
   // the Lowdin eigenpairs of the overlap sum_w F(w,i,0) F(w,j,0) (frmorb2.F:460-583)
-  // are those fo_setup computed for TMAT: the same overlap of the same FMAT
-  const std::vector<double>& filo = S.filo;
+  // are those fo_setup computed for TMAT: the same overlap of the same FMAT.
+  // Fm[i][a] = FILO(i,a): component i of eigenvector a.
+  const std::vector<double>& Fm = S.filo;
   const std::vector<double>& Q = S.lam;
-  auto FI = [&](int i, int a) { return filo[(size_t)i * nf + a]; };
+  const size_t n2 = (size_t)nf * nf;
+  std::vector<double> FmT(n2), sicm(n2), tmp(n2), G(n2);
+  for (int i = 0; i < nf; ++i)
+    for (int a = 0; a < nf; ++a) {
+      FmT[(size_t)a * nf + i] = Fm[(size_t)i * nf + a];
+      sicm[(size_t)i * nf + a] = sic[(size_t)a * ld + i];  // SIC(i,a)
+    }
   // G = FILO^T SIC FILO  ->  HAM(b,a) = (G[a][b] - G[b][a]) / sqrt(Qa Qb)
-  std::vector<double> tmp((size_t)nf * nf, 0.0), G((size_t)nf * nf, 0.0);
-  for (int k = 0; k < nf; ++k)      // tmp[a][l] = sum_k FI(k,a) SIC(k,l)
-    for (int l = 0; l < nf; ++l) {
-      const double sv = sic[(size_t)l * ld + k];
-      if (sv == 0.0) continue;
-      for (int a = 0; a < nf; ++a) tmp[(size_t)a * nf + l] += FI(k, a) * sv;
-    }
-  for (int a = 0; a < nf; ++a)      // G[a][b] = sum_l tmp[a][l] FI(l,b)
-    for (int l = 0; l < nf; ++l) {
-      const double t = tmp[(size_t)a * nf + l];
-      for (int b = 0; b < nf; ++b) G[(size_t)a * nf + b] += t * FI(l, b);
-    }
-  std::vector<double> H((size_t)nf * nf);  // H[a*nf+b] = HAM(b,a)
-  for (int a = 0; a < nf; ++a)
-    for (int b = 0; b < nf; ++b)
-      H[(size_t)a * nf + b] = (G[(size_t)a * nf + b] - G[(size_t)b * nf + a]) / (std::sqrt(Q[b]) * std::sqrt(Q[a]));
-  // X[kx][n][m] = sum_w F(w,n,1) F(w,m,kx+1)
-  std::vector<double> X((size_t)3 * nf * nf, 0.0);
-  for (int kx = 0; kx < 3; ++kx)
-    for (int n = 0; n < nf; ++n)
-      for (int m = 0; m < nf; ++m) {
-        double v = 0.0;
-        for (int w = 0; w < nw; ++w) v += fm(w, n, 0) * fm(w, m, kx + 1);
-        X[((size_t)kx * nf + n) * nf + m] = v;
-      }
-  for (int i = 0; i < 3 * nf; ++i) deb[i] = 0.0;
-  // term 1: deb(kx,m) -= sum_a FI(m,a) sum_n SC1_a(n) X(n,m), SC1_a(n) = sum_b HAM(b,a) FI(n,b)
-  std::vector<double> sc1((size_t)nf * nf, 0.0);  // sc1[a][n]
+  mat_mul(FmT.data(), sicm.data(), tmp.data(), nf, nf, nf);
+  mat_mul(tmp.data(), Fm.data(), G.data(), nf, nf, nf);
+  // Both terms of frmorb2.F:612-717 in one matrix:
+  //   term 1: -sum_a FILO(m,a) (HAM^T FILO^T X_kx)[a][m]           (frmorb2.F:616-667)
+  //   term 2: +1/4 sum_ab HAM'(b,a) [FILO(m,a) Y_b(m) + FILO(m,b) Y_a(m)],
+  //           HAM' = HAM (sqrtQb - sqrtQa)/(sqrtQb + sqrtQa), Y = 2 FILO^T X_kx (:673-717)
+  // with X_kx[n][m] = sum_w F(w,n,1) F(w,m,kx+1), so that
+  //   DEBDAX(kx,m) = sum_n L[m][n] X_kx[n][m],  L = FILO (HAM'^T/2 + HAM'/2 - HAM^T) FILO^T
+  // (H[a][b] = HAM(b,a)), i.e. sum_w M[m][w] F(w,m,kx+1) with M = L F_0.
+  std::vector<double> A1(n2);
   for (int a = 0; a < nf; ++a)
     for (int b = 0; b < nf; ++b) {
-      const double h = H[(size_t)a * nf + b];
-      for (int n = 0; n < nf; ++n) sc1[(size_t)a * nf + n] += h * FI(n, b);
+      const double sa = std::sqrt(Q[a]), sb = std::sqrt(Q[b]);
+      const double hab = (G[(size_t)a * nf + b] - G[(size_t)b * nf + a]) / (sb * sa);
+      const double hba = (G[(size_t)b * nf + a] - G[(size_t)a * nf + b]) / (sa * sb);
+      const double hpab = hab * (sb - sa) / (sb + sa);
+      const double hpba = hba * (sa - sb) / (sa + sb);
+      A1[(size_t)a * nf + b] = 0.5 * (hpab + hpba) - hab;
     }
-  for (int kx = 0; kx < 3; ++kx) {
-    std::vector<double> Z((size_t)nf * nf, 0.0);  // Z[a][m] = sum_n sc1[a][n] X(n,m)
-    for (int a = 0; a < nf; ++a)
-      for (int n = 0; n < nf; ++n) {
-        const double t = sc1[(size_t)a * nf + n];
-        const double* xr = &X[((size_t)kx * nf + n) * nf];
-        for (int m = 0; m < nf; ++m) Z[(size_t)a * nf + m] += t * xr[m];
-      }
-    for (int m = 0; m < nf; ++m) {
+  std::vector<double> T(n2), L(n2), M((size_t)nf * nw);
+  mat_mul(Fm.data(), A1.data(), T.data(), nf, nf, nf);
+  mat_mul(T.data(), FmT.data(), L.data(), nf, nf, nf);
+  mat_mul(L.data(), &S.fmat[0], M.data(), nf, nf, nw);  // F_0[n][w] = F(w,n,1)
+  for (int m = 0; m < nf; ++m)
+    for (int kx = 0; kx < 3; ++kx) {
+      const double* fk = &S.fmat[((size_t)(kx + 1) * nf + m) * nw];
+      const double* mr = &M[(size_t)m * nw];
       double v = 0.0;
-      for (int a = 0; a < nf; ++a) v += FI(m, a) * Z[(size_t)a * nf + m];
-      deb[3 * m + kx] -= v;
+      for (int w = 0; w < nw; ++w) v += mr[w] * fk[w];
+      deb[3 * m + kx] = v;
     }
-  }
-  // term 2 with HAM'(b,a) = HAM(b,a) (sqrtQb - sqrtQa)/(sqrtQb + sqrtQa):
-  // deb(kx,m) += 0.25 sum_ab HAM'(b,a) [FI(m,a) Y_b(m) + FI(m,b) Y_a(m)] * 2,
-  // Y_b(m) = sum_i FI(i,b) 2 X(i,m)
-  std::vector<double> Hp((size_t)nf * nf);
-  for (int a = 0; a < nf; ++a)
-    for (int b = 0; b < nf; ++b) {
-      double h = H[(size_t)a * nf + b] * (std::sqrt(Q[b]) - std::sqrt(Q[a]));
-      Hp[(size_t)a * nf + b] = h / (std::sqrt(Q[b]) + std::sqrt(Q[a]));
-    }
-  for (int kx = 0; kx < 3; ++kx) {
-    std::vector<double> Yb((size_t)nf * nf, 0.0);  // Yb[b][m]
-    for (int i = 0; i < nf; ++i)
-      for (int b = 0; b < nf; ++b) {
-        const double f = FI(i, b);
-        const double* xr = &X[((size_t)kx * nf + i) * nf];
-        for (int m = 0; m < nf; ++m) Yb[(size_t)b * nf + m] += f * 2.0 * xr[m];
-      }
-    for (int m = 0; m < nf; ++m) {
-      double v = 0.0;
-      for (int a = 0; a < nf; ++a) {
-        const double fma_ = FI(m, a);
-        for (int b = 0; b < nf; ++b) {
-          const double hp = Hp[(size_t)a * nf + b];
-          v += hp * (fma_ * Yb[(size_t)b * nf + m] + FI(m, b) * Yb[(size_t)a * nf + m]);
-        }
-      }
-      deb[3 * m + kx] += 0.25 * v;
-    }
-  }
   auto t1 = std::chrono::steady_clock::now();
   c->stage_ms[6] += std::chrono::duration<double, std::milli>(t1 - t0).count();
 }
@@ -1135,7 +1112,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_basis.release(); c->d_fodpts.release(); c->d_psig.release(); c->d_tmat.release(); c->d_u.release();
   c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
   c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
-  c->d_share.release(); c->d_lists.release();
+  c->d_share.release(); c->d_lists.release(); c->d_setup_list.release();
   c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_work.release(); c->d_eig_info.release();
   c->d_coef_hl.release(); c->d_momv_hl.release(); c->d_tc_err.release();
   if (c->blas) cublasDestroy(c->blas);
@@ -1262,6 +1239,15 @@ int flosic_sic_set_geometry(flosic_ctx* c, int natoms, const int32_t* atom_type,
     build_pair_plan(c);
     c->d_pairs.upload(c->pairs.data(), c->pairs.size(), st);
     c->d_calls.upload(c->calls.data(), c->calls.size(), st);
+    {
+      std::vector<int> list;
+      for (size_t i = 0; i < c->calls.size(); ++i)
+        if (c->calls[i].slots == 1) list.push_back((int)i);
+      c->nsingle = (int)list.size();
+      for (size_t i = 0; i < c->calls.size(); ++i)
+        if (c->calls[i].slots != 1) list.push_back((int)i);
+      c->d_setup_list.upload(list.data(), list.size(), st);
+    }
     CUDA_CHECK(cudaStreamSynchronize(st));
     c->have_geom = true;
   });
@@ -1683,8 +1669,7 @@ int flosic_sic_mgga_mixin(flosic_ctx* c, int lspx, int iorbx, double* mixin) {
 
 int flosic_sic_adjoint(flosic_ctx* c, int lspn, double* g, int ldg) {
   return guarded([&] {
-    require(c, true);
-    require_whole_mesh(c);
+    require(c, true);  // on a mesh shard: the shard's partial sum
     if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
     if (!g) fail(FLOSIC_ERR_ARG, "null array argument");
     if (ldg < c->nbasis) fail(FLOSIC_ERR_ARG, "ldg smaller than the number of basis functions");
@@ -1727,8 +1712,7 @@ int flosic_sic_adjoint(flosic_ctx* c, int lspn, double* g, int ldg) {
 
 int flosic_sic_siclag_der(flosic_ctx* c, double* dersic, int ldo) {
   return guarded([&] {
-    require(c, true);
-    require_whole_mesh(c);
+    require(c, true);  // on a mesh shard: the shard's partial sum
     if (!dersic) fail(FLOSIC_ERR_ARG, "null array argument");
     const int nwft = c->nfrm[0] + (c->nspn == 2 ? c->nfrm[1] : 0);
     if (ldo < std::max(1, nwft)) fail(FLOSIC_ERR_ARG, "ldo smaller than NFRM(1)+NFRM(2)");

@@ -8,8 +8,38 @@ The sum runs on the GPU buffer with an NCCL process group (over NVLink /
 NVSwitch on one node); with a gloo group the buffer goes through host memory.
 Any object with partial_size(), cycle_partial(address) and
 cycle_combine(address) can be driven: the CUDA library (sic.FlosicSIC) and,
-in the CPU tests, the FP64 CPU restatement of the same decomposition."""
+in the CPU tests, the FP64 CPU restatement of the same decomposition.
+
+The basis-space results (dE/dC_FO and the atomic SIC force terms DERSIC) are
+sums over mesh points too: each rank computes its shard's part and one more
+sum completes them (sharded_adjoint, sharded_siclag_der)."""
 from __future__ import annotations
+
+import numpy as np
+
+
+def allreduce_array(a, group=None, device=None):
+    """Sum a host array over the ranks of `group` (through `device` for NCCL)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
+    if dist.get_backend(group) == "nccl":
+        t = t.to(device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return t.cpu().numpy()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.numpy()
+
+
+def sharded_adjoint(ctx, lspn, group=None, device=None):
+    """G = dE_SIC/dC_FO of spin lspn over the whole mesh from the ranks' shards."""
+    return allreduce_array(ctx.adjoint(lspn), group, device)
+
+
+def sharded_siclag_der(ctx, group=None, device=None):
+    """DERSIC over the whole mesh from the ranks' shards."""
+    return allreduce_array(ctx.siclag_der(), group, device)
 
 
 def sharded_cycle(ctx, group=None, device=None):

@@ -71,3 +71,48 @@ def test_two_rank_gloo_cycle_equals_unsharded(name):
             assert np.allclose(g["debdax"][s][:n], ref["debdax"][s][:n], rtol=1e-9, atol=1e-10)
             assert np.allclose(g["cfrm"][s][:n], ref["cfrm"][s][:n], rtol=1e-10, atol=1e-12)
     assert all(np.array_equal(got[0][k], got[1][k]) for k in ("results", "sic", "debdax"))
+
+
+class _PartialCtx:
+    """A shard context stand-in whose partial sums are known: rank r holds
+    (r + 1) * base, so the sum over two ranks is 3 * base."""
+
+    def __init__(self, rank):
+        self.rank = rank
+
+    def adjoint(self, lspn):
+        return (self.rank + 1) * np.arange(12.0).reshape(4, 3) * lspn
+
+    def siclag_der(self):
+        return (self.rank + 1) * np.linspace(-1.0, 1.0, 18).reshape(3, 2, 3)
+
+
+def _rank_sums(rank, world, port, out):
+    import torch.distributed as dist
+    from publicrelease_2020_b200.shard import sharded_adjoint, sharded_siclag_der
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        c = _PartialCtx(rank)
+        out[rank] = (sharded_adjoint(c, 2), sharded_siclag_der(c))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_basis_space_sums():
+    """sharded_adjoint / sharded_siclag_der add the ranks' partial arrays."""
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_rank_sums, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=300)
+        assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+        got = [out[r] for r in range(2)]
+    for g, d in got:
+        assert np.array_equal(g, 3 * np.arange(12.0).reshape(4, 3) * 2)
+        assert np.allclose(d, 3 * np.linspace(-1.0, 1.0, 18).reshape(3, 2, 3), rtol=0, atol=1e-15)

@@ -61,6 +61,26 @@ def test_shard_partials_sum_to_unsharded_cycle(name, nshards):
             c.close()
 
 
+@pytest.mark.parametrize("name", ["water_lda_nspn2", "water_scan_nspn2", "synthetic_pbe_nspn1"])
+def test_shard_adjoint_and_dersic_sum_to_whole_mesh(name):
+    """dE/dC_FO and DERSIC on mesh shards are partial sums over the shards' points."""
+    sysm = SYSTEMS[name]()
+    whole = S.open_system(sysm)
+    g_ref = [whole.adjoint(sp) for sp in range(1, sysm.nspn + 1)]
+    d_ref = whole.siclag_der()
+    whole.close()
+    ctxs = [S.open_system(sysm, shard=(r, 2)) for r in range(2)]
+    try:
+        for sp in range(1, sysm.nspn + 1):
+            g = sum(c.adjoint(sp) for c in ctxs)
+            assert np.abs(g - g_ref[sp - 1]).max() < 1e-10 * np.abs(g_ref[sp - 1]).max()
+        d = sum(c.siclag_der() for c in ctxs)
+        assert np.abs(d - d_ref).max() < 1e-10 * np.abs(d_ref).max()
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_sharded_context_refuses_whole_mesh_entry_points():
     sysm = SYSTEMS["water_lda_nspn2"]()
     ctx = S.open_system(sysm, shard=(1, 2))
@@ -86,7 +106,7 @@ def _free_port():
 def _rank(rank, world, port, out):
     import torch.distributed as dist
     from publicrelease_2020_b200 import sic as S2
-    from publicrelease_2020_b200.shard import sharded_cycle
+    from publicrelease_2020_b200.shard import sharded_adjoint, sharded_cycle, sharded_siclag_der
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -94,7 +114,10 @@ def _rank(rank, world, port, out):
         sysm = SYSTEMS["synthetic_pbe_nspn1"]()
         ctx = S2.open_system(sysm, shard=(rank, world))
         r = sharded_cycle(ctx, device="cuda:0")
-        out[rank] = {k: (np.array(v) if not isinstance(v, float) else v) for k, v in r.items()}
+        res = {k: (np.array(v) if not isinstance(v, float) else v) for k, v in r.items()}
+        res["g1"] = sharded_adjoint(ctx, 1, device="cuda:0")
+        res["dersic"] = sharded_siclag_der(ctx, device="cuda:0")
+        out[rank] = res
         ctx.close()
     finally:
         dist.destroy_process_group()
@@ -104,6 +127,8 @@ def test_two_ranks_gloo_on_one_gpu():
     sysm = SYSTEMS["synthetic_pbe_nspn1"]()
     whole = S.open_system(sysm)
     ref = whole.cycle()
+    g_ref = whole.adjoint(1)
+    d_ref = whole.siclag_der()
     whole.close()
     ctx = mp.get_context("spawn")
     with ctx.Manager() as mgr:
@@ -118,3 +143,5 @@ def test_two_ranks_gloo_on_one_gpu():
         got = [dict(out[r]) for r in range(2)]
     for g in got:
         _close(g, ref, sysm)
+        assert np.abs(g["g1"] - g_ref).max() < 1e-10 * np.abs(g_ref).max()
+        assert np.abs(g["dersic"] - d_ref).max() < 1e-10 * np.abs(d_ref).max()

@@ -45,15 +45,12 @@ def test_siclag_der_mixed_precision():
     assert np.abs(d - ref).max() < 1e-5 * np.abs(ref).max()
 
 
-def test_siclag_der_refuses_short_ldo_and_shards():
+def test_siclag_der_refuses_short_ldo():
     s = W.water(seed=0, nrad=14)
     ctx = sic.open_system(s)
     try:
         out = np.zeros(s.natoms * 3 * 3)
         with pytest.raises(sic.FlosicError):
             ctx._check(ctx.L.flosic_sic_siclag_der(ctx.h, out, 3))
-        ctx.set_shard(0, 2)
-        with pytest.raises(sic.FlosicError):
-            ctx.siclag_der()
     finally:
         ctx.close()

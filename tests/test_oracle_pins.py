@@ -59,6 +59,50 @@ def test_coulomb_of_s_gaussian_is_erf_over_r(exact):
         assert st[4] > 0  # some points went through the multipole far field
 
 
+def _multipole_potential(s, a, l, pts):
+    """Potential of rho = (c x e^{-a r^2})^2 (l = 1) or (c x^2 e^{-a r^2})^2 (l = 2)
+    by brute-force quadrature: the angular factor split into its degree-l'
+    parts with the addition theorem on the 146-point Lebedev grid (exact to
+    degree 19), the radial Green's-function integrals by adaptive quadrature."""
+    from scipy import integrate
+    from scipy.special import eval_legendre
+    c = s.bfcon[0, l, 0, 0]
+    d = pts - s.rat[0]
+    r = np.linalg.norm(d, axis=1)
+    u = d / r[:, None]
+    ang, w = O.lebedev19()
+    w = w * (4 * math.pi / w.sum())
+    g_leb = (ang[:, 0] if l == 1 else ang[:, 0] ** 2) ** 2
+    rk = np.round(r, 12)
+    V = np.zeros(len(r))
+    for lp in range(0, 2 * l + 1, 2):
+        gl = (2 * lp + 1) / (4 * math.pi) * (eval_legendre(lp, u @ ang.T) * (w * g_leb)[None, :]).sum(1)
+        R = {}
+        for x in np.unique(rk):
+            f_in = lambda t: c * c * t ** (2 * l + lp + 2) * np.exp(-2 * a * t * t)
+            f_out = lambda t: c * c * t ** (2 * l + 1 - lp) * np.exp(-2 * a * t * t)
+            i1 = integrate.quad(f_in, 0, x, epsabs=0, epsrel=1e-13, limit=200)[0]
+            i2 = integrate.quad(f_out, x, np.inf, epsabs=0, epsrel=1e-13, limit=200)[0]
+            R[x] = 4 * math.pi / (2 * lp + 1) * (x ** (-lp - 1) * i1 + x ** lp * i2)
+        V += gl * np.array([R[x] for x in rk])
+    return V
+
+
+@pytest.mark.parametrize("l", [1, 2])
+def test_coulomb_of_p_and_d_densities_vs_radial_quadrature(l):
+    """COUPOT_SIC of one p_x (l=1) or d_xx (l=2) orbital: the pair-polynomial
+    potential against an independent multipole/radial-quadrature evaluation."""
+    a = 0.8
+    s = one_gaussian_system(a, nrad=30, l=l)
+    c0 = s.rat[0]
+    s.fods = [np.array([c0 + [0.1, 0.05, 0.02]]), np.array([c0 + [0.07, -0.04, 0.03]])]
+    o = O.Oracle(s)
+    ref = _multipole_potential(s, a, l, s.rmsh)
+    for exact in (False, True):
+        coul, rhog, _ = o.coupot_sic(1, 1, exact=exact)
+        assert np.max(np.abs(coul - ref) / np.abs(ref)) < 1e-9
+
+
 def test_coupot1_and_densold_of_s_gaussian():
     """DENSOLD and COUPOT1 of one s orbital per spin: rho_s = psi^2 with its
     gradient, Hessian and PHIG = |grad psi|^2 in closed form; the Coulomb

@@ -815,12 +815,13 @@ static void launch_perfo(int ncalls, const int* lists, int acc, const CallInfo* 
 
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
-                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,
+                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
                         bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st) {
+  const bool per_fo_only = cfg.per_fo_only;
   if (npairs > 0) k_pair_fmt<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, nfo, maxfmt, scr.pair_fmt);
   if (ncalls > 0) k_call_share<<<(ncalls + 7) / 8, 256, 0, st>>>(ncalls, nfo, cfo, scr.share);
   k_call_lists<<<1, LIST_THREADS, 0, st>>>(ncalls, per_fo_only ? 1 : 0, scr.share, scr.lists);
-  if (!per_fo_only && mixed) {
+  if (!per_fo_only && mixed && cfg.shared_tc) {
     const size_t nc = (size_t)npairs * nfo * COEF_LD, nm = (size_t)ncalls * nfo * MOM_LD;
     launch_split_tf32((size_t)npairs, nfo, coef, scr.coef_hl, st);
     launch_split_tf32((size_t)ncalls, nfo, momv, scr.momv_hl, st);
@@ -838,10 +839,11 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
                        ldv, cnt, mixed, st);
   }
   const int acc = per_fo_only ? 0 : 1;
-  if (nfo > 64)
+  const int wm = cfg.perfo_wm > 0 ? cfg.perfo_wm : (nfo > 64 ? 4 : (nfo > 32 ? 2 : 1));
+  if (wm == 4)
     launch_perfo<4>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
                     cnt, mixed, st);
-  else if (nfo > 32)
+  else if (wm == 2)
     launch_perfo<2>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
                     cnt, mixed, st);
   else

@@ -82,6 +82,17 @@ struct CoulombScratch {
   float* momv_hl;      // mixed path: TF32 hi/lo split of the moments (2 x ncalls*nfo*MOM_LD)
   int* err;            // mixed path: set when a tensor-core pipeline wait reached its limit
 };
+// Kernel choices (all evaluate the same sums; the results differ only by the
+// rounding of the chosen arithmetic).  per_fo_only: every call through the
+// per-FO kernel (a cross-check of the two forms).  shared_tc: in the mixed
+// path, the shared-geometry calls on tcgen05 (TF32 split products) rather
+// than on the FP64 tensor cores with FP32 columns.  perfo_wm: FO block of the
+// per-FO kernel in units of 32 (1, 2 or 4; 0 chooses by the FO count).
+struct CoulombConfig {
+  bool per_fo_only = false;
+  bool shared_tc = true;
+  int perfo_wm = 0;
+};
 void init_coulomb_mma();
 void init_coulomb_tc();
 // TF32 hi/lo split of nrow x nfo rows of KSEG doubles into the chunk-major
@@ -94,7 +105,7 @@ void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* sha
                               double* vh, int ldv, unsigned long long* cnt, int* err, cudaStream_t st);
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
-                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, bool per_fo_only,
+                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
                         bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st);
 
 // Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as

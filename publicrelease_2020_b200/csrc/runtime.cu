@@ -333,7 +333,7 @@ struct flosic_ctx {
   DevBuf<int> d_setup_list;  // one-slot calls first (nsingle), then the others
   int nsingle = 0;
   DevBuf<float> d_coef_hl, d_momv_hl;
-  bool per_fo_coulomb = false;   // FLOSIC_COULOMB=perfo: every call through the per-FO kernel (A/B checks)
+  CoulombConfig coulomb_cfg;     // FLOSIC_COULOMB=perfo, FLOSIC_SHARED=mma, FLOSIC_PERFO_WM=1|2|4 (A/B checks)
   int precision = FLOSIC_PRECISION_FP64;
   DevBuf<unsigned long long> d_cnt;
   unsigned long long work_near = 0, work_far = 0, work_terms = 0;
@@ -780,9 +780,9 @@ void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
   }
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p, c->d_coef_hl.p, c->d_momv_hl.p, c->d_tc_err.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                     c->d_mom.p, c->eval_mesh(), c->d_boys.p, vh, P, c->per_fo_coulomb, mixed, scr,
+                     c->d_mom.p, c->eval_mesh(), c->d_boys.p, vh, P, c->coulomb_cfg, mixed, scr,
                      c->d_cnt.p, st);
-  c->launches += c->per_fo_coulomb ? 4 : 5;
+  c->launches += c->coulomb_cfg.per_fo_only ? 4 : 5;
   unsigned long long cnt[3];
   int tc_err = 0;
   CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
@@ -1067,7 +1067,12 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     CUDA_CHECK(cudaSetDevice(device));
     auto* c = new flosic_ctx;
     c->device = device;
-    if (const char* e = std::getenv("FLOSIC_COULOMB")) c->per_fo_coulomb = (std::string(e) == "perfo");
+    if (const char* e = std::getenv("FLOSIC_COULOMB")) c->coulomb_cfg.per_fo_only = (std::string(e) == "perfo");
+    if (const char* e = std::getenv("FLOSIC_SHARED")) c->coulomb_cfg.shared_tc = (std::string(e) != "mma");
+    if (const char* e = std::getenv("FLOSIC_PERFO_WM")) {
+      const int wm = std::atoi(e);
+      c->coulomb_cfg.perfo_wm = (wm == 1 || wm == 2 || wm == 4) ? wm : 0;
+    }
     CUDA_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) {
       cudaStreamDestroy(c->st);

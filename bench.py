@@ -63,6 +63,15 @@ def workload(name):
             dict(workload="C2 density of atoms and points in a 7.56 A box: 10 atoms, 128 functions, 2.5e5 points, "
                           "64 FOs (profiling case)", atoms=10, nbasis=128, nmsh=250_000, nfo=64,
                  functional="GGA-PBE*GGA-PBE", nspn=1)
+    if name == "c3":
+        s = W.benzene(seed=3, nrad=228)
+        return s, dict(workload=f"benzene LDA-PW91, 21+21 FODs, {s.nbasis} functions, {s.nmsh} mesh points",
+                       atoms=12, nbasis=s.nbasis, nmsh=s.nmsh, nfo=21, functional="LDA-PW91*LDA-PW91", nspn=2)
+    if name == "c5":
+        s = W.c60(seed=4, nrad=40)
+        return s, dict(workload=f"C60 SCAN, 180+180 FODs, {s.nbasis} functions, {s.nmsh} mesh points "
+                                "(a tenth of the 3e6-point C60 mesh)",
+                       atoms=60, nbasis=s.nbasis, nmsh=s.nmsh, nfo=180, functional="MGGA-SCAN*MGGA-SCAN", nspn=2)
     if name == "water":
         s = W.water(seed=0, nrad=40)
         return s, dict(workload="water LDA-PW91, 5+5 FODs", atoms=3, nbasis=s.nbasis, nmsh=s.nmsh, nfo=5,
@@ -363,7 +372,7 @@ def main():
                     help="time the FP64 path, the mixed path, or both (headline = mixed when it meets the "
                          "|dE_SIC| <= 1e-5 Ha and FOD-force <= 1e-4 Ha/bohr gates)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "water", "small"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "c3", "c5", "water", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -269,15 +269,16 @@ def atom_centred_mesh(rat, nrad=40, rscale=None, seed=0):
             dist = np.linalg.norm(p[:, None, :] - rat[None, :, :], axis=2)
             Rab = np.linalg.norm(rat[:, None] - rat[None, :], axis=2)
             cell = np.ones((len(p), nat))
-            for A in range(nat):
+            # cell[:, A] = prod over B != A (ascending) of s(mu_AB), all A at once
+            with np.errstate(divide="ignore", invalid="ignore"):
                 for B in range(nat):
-                    if A == B:
-                        continue
-                    mu = (dist[:, A] - dist[:, B]) / Rab[A, B]
+                    mu = (dist - dist[:, B:B + 1]) / Rab[:, B]
                     f = mu
                     for _ in range(3):
-                        f = 1.5 * f - 0.5 * f ** 3
-                    cell[:, A] *= 0.5 * (1 - f)
+                        f = 1.5 * f - 0.5 * (f * f * f)
+                    sB = 0.5 * (1 - f)
+                    sB[:, B] = 1.0
+                    cell *= sB
             w = w * cell[:, a] / cell.sum(axis=1)
         keep = w > 1e-14
         pts.append(p[keep])

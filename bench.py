@@ -233,9 +233,14 @@ def run_ours(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
+    tuned = {}
+
     def timed(mode, clk_sampler):
         """W warm-up and K timed SIC cycles in one precision; inputs resident."""
         ctx.set_precision(mode)
+        if not args.no_autotune:
+            width, ms = ctx.autotune(reps=1)
+            tuned[mode] = {"perfo_fo_slots": width, "ms": {str(k): round(v, 3) for k, v in ms.items()}}
         out = new_out()
         for _ in range(args.warmup):
             step(out)
@@ -322,7 +327,8 @@ def run_ours(args, rank, world, local_rank):
     traffic = COULOMB_DRAM_BYTES_PER_TILE * ntiles if args.workload in ("c2", "c2half", "c2tiny") else None
     cfg.update(parallelism=(f"mesh shards x{world}, NCCL all-reduce of the partial sums" if world > 1
                             else "single GPU"), l2="working set >> L2 (126 MB)",
-               npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision=headline)
+               npairs=ctx_stats["npairs"], ncalls=ctx_stats["ncalls"], precision=headline,
+               autotune=tuned or "off")
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": False,
@@ -363,6 +369,132 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rank, world, local_rank):
+    """C4: 64 alkane-like chains and rings of uneven size, every molecule's SIC
+    cycle issued concurrently on one GPU (batch.Batch).  A step is one SIC
+    cycle of every molecule; with N GPUs the molecules are dealt round-robin to
+    the ranks (independent objects, no collective) and the step time is the
+    maximum over ranks."""
+    import torch
+    from publicrelease_2020_b200 import batch as B
+    from publicrelease_2020_b200 import workloads as W
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    systems = W.alkane_batch(64)
+    mine = systems[rank::world]
+    bt = B.Batch(mine, device=local_rank)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    tuned = {}
+
+    def timed(mode, clk_sampler):
+        for c in bt.ctxs:
+            c.set_precision(mode)
+        if not args.no_autotune:
+            widths = [c.autotune(reps=1)[0] for c in bt.ctxs]
+            tuned[mode] = {str(w): widths.count(w) for w in sorted(set(widths))}
+        for _ in range(args.warmup):
+            bt.cycle()
+        acc = dict(near=0, far=0, terms=0, launches=0)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with clk_sampler as clk:
+            e0.record()
+            for _ in range(args.steps):
+                res = bt.cycle()
+                for c in bt.ctxs:
+                    st = c.stats()
+                    acc["near"] += st["near_evals"]
+                    acc["terms"] += st["far_terms"]
+                    acc["far"] += st["far_evals"]
+                    acc["launches"] += st["launches"]
+            e1.record()
+            torch.cuda.synchronize()
+            barrier()
+        return e0.elapsed_time(e1), acc, res, clk.summary()
+
+    modes = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    runs = {m: timed(m, ClockSampler(local_rank)) for m in modes}
+    headline = modes[-1]
+    errors = None
+    if len(runs) == 2:
+        de = max(abs(a["esic"] - b["esic"]) for a, b in zip(runs["fp64"][2], runs["mixed"][2]))
+        df = max(float(np.abs(a["debdax"][s][:m.nfrm[s]] - b["debdax"][s][:m.nfrm[s]]).max())
+                 for a, b, m in zip(runs["fp64"][2], runs["mixed"][2], mine) for s in range(m.nspn))
+        errors = {"max_d_esic_ha": de, "max_d_fod_force_ha_bohr": df,
+                  "gate_esic_1e-5_ha": bool(de <= 1e-5), "gate_force_1e-4_ha_bohr": bool(df <= 1e-4)}
+        if not (errors["gate_esic_1e-5_ha"] and errors["gate_force_1e-4_ha_bohr"]):
+            headline = "fp64"
+    for c in bt.ctxs:
+        c.set_precision(headline)
+    psis = [np.ascontiguousarray(m.psi) for m in mine]
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        for c, m, psi in zip(bt.ctxs, mine, psis):
+            c.set_orbitals(psi, m.nwfs, m.fods)
+        bt.cycle()
+    f1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+    h2d = sum(psi.nbytes + 8 * 3 * c.ld * 2 for c, psi in zip(bt.ctxs, psis))
+    d2h = sum(8 * (2 * c.ld * 13 + 2 * c.ld * c.ld + 4 * c.ld * 3 + 1) for c in bt.ctxs)
+    times = {m: runs[m][0] for m in runs}
+    if dist is not None:
+        keys = sorted(times)
+        t = torch.tensor([times[k] for k in keys] + [e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        times = {k: float(t[i]) for i, k in enumerate(keys)}
+        e2e_ms = float(t[-1])
+    bt.close()
+    if rank != 0:
+        return
+    t_ms, acc, _, clocks = runs[headline]
+    t_ms = times[headline]
+    per_step_s = t_ms / 1e3 / args.steps
+    flops = (acc["near"] * COULOMB_FLOPS_NEAR + acc["terms"] * COULOMB_FLOPS_TERM) / args.steps * world
+    peak = fp64_peak_tflops(torch)
+    achieved = flops / per_step_s / 1e12
+    nb = [m.nbasis for m in systems]
+    npt = [m.nmsh for m in systems]
+    nfo = [max(m.nfrm) for m in systems]
+    cfg = {"workload": f"C4 batch: 64 alkane-like chains and rings (seeds 100-163, 2-29 atoms), {min(nb)}-{max(nb)} "
+                       f"functions, {min(npt)}-{max(npt)} mesh points ({sum(npt)} in all), {min(nfo)}-{max(nfo)} FOs "
+                       "per spin, LDA-PW91, NSPN=2; every molecule's cycle issued concurrently on its own stream",
+           "molecules": len(systems), "parallelism": (f"molecules dealt to {world} GPUs" if world > 1 else "single GPU"),
+           "l2": "working set >> L2 (126 MB)", "precision": headline, "autotune": tuned or "off"}
+    line = {
+        "metric": METRIC, "value": per_step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": False,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64" if headline == "fp64" else "f32+f64",
+        "data": "synthetic (seeded)", "config": cfg,
+        "e2e": {"value": e2e_ms / 1e3 / args.steps, "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(acc["launches"]),
+        "roofline": {"bound": "tensor", "kernel": "k_coulomb_shared + k_coulomb_perfo (whole batch cycle as the "
+                                                  "denominator: the molecules' stages overlap)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                     "traffic": None,
+                     "peak_kind": "FP64 cuBLAS DGEMM measured in this run (MEASURED_PEAKS.json has no FP64 figure)"},
+        "clocks": clocks,
+    }
+    if len(runs) > 1:
+        line["precision"] = {"headline": headline, "s_per_cycle": {m: times[m] / 1e3 / args.steps for m in runs},
+                             "speedup_mixed_vs_fp64": times["fp64"] / times["mixed"],
+                             "mixed_vs_fp64_errors": errors, "clocks": {m: runs[m][3] for m in runs}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,13 +504,21 @@ def main():
                     help="time the FP64 path, the mixed path, or both (headline = mixed when it meets the "
                          "|dE_SIC| <= 1e-5 Ha and FOD-force <= 1e-4 Ha/bohr gates)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "c3", "c5", "water", "small"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "c3", "c4", "c5", "water",
+                                                      "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the per-FO Coulomb kernel's default tile width instead of timing the candidates")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        if args.workload == "c4":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the CPU arm times single systems, "
+                                                                      "not the C4 batch"}), flush=True)
+            return
         run_reference(args, rank, world)
         return
     if world > 1:
@@ -388,7 +528,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "c4":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -124,6 +124,19 @@ int flosic_sic_mgga_mixin(flosic_ctx* ctx, int lspx, int iorbx, double* mixin);
 enum { FLOSIC_PRECISION_FP64 = 0, FLOSIC_PRECISION_MIXED = 1 };
 int flosic_sic_set_precision(flosic_ctx* ctx, int mode);
 
+/* Tile-shape autotuner (no counterpart in the reference, whose POISSON1 batch
+   shapes are compile-time constants: MXPR pairs per call, coupot_sic.F:46, and
+   MPX points per block, poisson1.f:62).  Times the per-FO Coulomb kernel with
+   tiles of 128 mesh points by 32, 64 and 128 FO slots on this context's own
+   COUPOT_SIC evaluation (the spin with the most FOs, the current precision mode
+   and mesh shard; best of reps >= 1 runs after one untimed run) and keeps the
+   fastest for the following calls.  Widths that would leave half a tile or more
+   empty are skipped.  All widths give the same potentials bit for bit.
+   perfo_fos: the chosen width; ms[3] (may be NULL): the times of widths
+   32, 64, 128 in milliseconds, -1 for a skipped width.  Needs
+   flosic_sic_set_orbitals; invalidates that spin's cached potentials. */
+int flosic_sic_autotune(flosic_ctx* ctx, int reps, int* perfo_fos, float* ms);
+
 /* Allocation-free form of flosic_sic_getvlxc on the caller's device buffers (no
    counterpart in the reference).  d_rhog: RHOG(ldr,10) density channels in
    device memory (channel stride ldr >= npts), d_wmsh: the npts mesh weights,

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1515,6 +1516,59 @@ int flosic_sic_set_precision(flosic_ctx* c, int mode) {
         s.sic_valid = false;
       }
     }
+  });
+}
+
+// Tile-shape autotuner of the per-FO Coulomb kernel: its tiles are 128 mesh
+// points by 32, 64 or 128 compacted FO slots.  Each width is timed (CUDA
+// events on the context's stream, best of reps after one untimed run) on the
+// full COUPOT_SIC Coulomb evaluation of the spin with the most FOs, under the
+// context's precision mode and mesh shard, and the fastest is kept.  The
+// widths only regroup FOs into CTAs; every potential is formed by the same
+// operations in the same order, so the choice changes time, not results.
+// Work counters and launch counts are left as they were.
+int flosic_sic_autotune(flosic_ctx* c, int reps, int* perfo_fos, float* ms) {
+  return guarded([&] {
+    require(c, true);
+    if (reps < 1 || reps > 100) fail(FLOSIC_ERR_ARG, "REPS must be in 1..100");
+    if (!perfo_fos) fail(FLOSIC_ERR_ARG, "null output pointer");
+    const int s = (c->nspn == 2 && c->nfrm[1] > c->nfrm[0]) ? 1 : 0;
+    if (c->nfrm[s] < 1) fail(FLOSIC_ERR_STATE, "no FOs to tune on");
+    const unsigned long long wn = c->work_near, wf = c->work_far, wt = c->work_terms;
+    const long long nl = c->launches;
+    fo_setup(c, s);
+    const int nf = c->spin[s].nf;
+    cudaStream_t st = c->st;
+    float best = std::numeric_limits<float>::infinity();
+    int best_wm = 0;
+    for (int i = 0; i < 3; ++i) {
+      const int wm = 1 << i;
+      if (ms) ms[i] = -1.f;
+      if (wm > 1 && 16 * wm >= nf) continue;  // half the block or more would stay empty
+      c->coulomb_cfg.perfo_wm = wm;
+      coulomb(c, s);
+      float t = std::numeric_limits<float>::infinity();
+      for (int r = 0; r < reps; ++r) {
+        CUDA_CHECK(cudaEventRecord(c->ev[5], st));
+        coulomb(c, s);
+        CUDA_CHECK(cudaEventRecord(c->ev[6], st));
+        CUDA_CHECK(cudaEventSynchronize(c->ev[6]));
+        t = std::min(t, elapsed(c->ev[5], c->ev[6]));
+      }
+      if (ms) ms[i] = t;
+      if (t < best) {
+        best = t;
+        best_wm = wm;
+      }
+    }
+    c->coulomb_cfg.perfo_wm = best_wm;
+    c->spin[s].pot_valid = false;
+    c->spin[s].sic_valid = false;
+    c->work_near = wn;
+    c->work_far = wf;
+    c->work_terms = wt;
+    c->launches = nl;
+    *perfo_fos = 32 * best_wm;
   });
 }
 

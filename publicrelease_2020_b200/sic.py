@@ -37,6 +37,7 @@ EXPORTS = [
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
     "flosic_sic_siclag_der", "flosic_sic_sicham", "flosic_sic_densold", "flosic_sic_coupot1",
+    "flosic_sic_autotune",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -70,6 +71,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_getvlxc.argtypes = [_vp, C.c_int, _dp, _dp, _dp]
     L.flosic_sic_getvlxc_mgga.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
+    L.flosic_sic_autotune.argtypes = [_vp, C.c_int, _ip, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")]
     L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
     L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.flosic_sic_siclagm.argtypes = [_vp, C.c_int, _dp, C.c_int]
@@ -190,6 +192,15 @@ class FlosicSIC:
     def set_precision(self, mode):
         """"fp64" (the drop-in, default) or "mixed"."""
         self._check(self.L.flosic_sic_set_precision(self.h, PRECISION[mode]))
+
+    def autotune(self, reps=2):
+        """Time the per-FO Coulomb kernel's FO-slot widths (32, 64, 128) on this
+        system and keep the fastest; returns (width, {width: ms}) with skipped
+        widths left out."""
+        fos = np.zeros(1, dtype=np.int32)
+        ms = np.zeros(3, dtype=np.float32)
+        self._check(self.L.flosic_sic_autotune(self.h, int(reps), fos, ms))
+        return int(fos[0]), {32 << i: float(t) for i, t in enumerate(ms) if t >= 0}
 
     def getvlxc_device(self, npts, d_rhog, ldr, d_wmsh, d_vxc):
         """Allocation-free GETVLXC on device buffers given as raw device addresses

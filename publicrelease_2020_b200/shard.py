@@ -42,6 +42,32 @@ def sharded_siclag_der(ctx, group=None, device=None):
     return allreduce_array(ctx.siclag_der(), group, device)
 
 
+def chunked_cycle(ctx, nchunks, device=None):
+    """One SIC cycle of the whole mesh on one device in nchunks passes, for a
+    system whose per-FO mesh arrays (FO values and their derivatives, Coulomb
+    and SIC potentials, the SIC-weighted Y channels: several doubles per
+    point and FO of each spin) would not fit in device memory at once.  Pass
+    i evaluates mesh shard i of nchunks (flosic_sic_set_shard), so those
+    arrays are sized for one chunk; the packed partial sums of the passes are
+    added and flosic_sic_cycle_combine completes the cycle, exactly as the
+    ranks of sharded_cycle do, so the outputs equal the one-pass cycle to
+    rounding.  The FO set-up and the POISSON1 call set-up are recomputed in
+    every pass.  The context is left on its last chunk."""
+    import torch
+
+    n = ctx.partial_size()
+    on_gpu = device is not None and torch.device(device).type == "cuda"
+    total = torch.zeros(n, dtype=torch.float64, device=device if on_gpu else "cpu")
+    part = torch.zeros_like(total)
+    for i in range(nchunks):
+        ctx.set_shard(i, nchunks)
+        ctx.cycle_partial(part.data_ptr())
+        total += part
+        if on_gpu:   # the next pass rewrites `part` on the library's stream
+            torch.cuda.synchronize(total.device)
+    return ctx.cycle_combine(total.data_ptr())
+
+
 def sharded_cycle(ctx, group=None, device=None):
     """One SIC cycle over the ranks of `group` (torch.distributed default group
     if None).  Every rank calls it with its own shard's context; every rank

@@ -116,3 +116,46 @@ def test_two_rank_gloo_basis_space_sums():
     for g, d in got:
         assert np.array_equal(g, 3 * np.arange(12.0).reshape(4, 3) * 2)
         assert np.allclose(d, 3 * np.linspace(-1.0, 1.0, 18).reshape(3, 2, 3), rtol=0, atol=1e-15)
+
+
+class _OracleChunks:
+    """The oracle behind the set_shard protocol of the CUDA context: shard i
+    of n is the mesh-point range [n_pts * i // n, n_pts * (i + 1) // n)."""
+
+    def __init__(self, orc, npts):
+        self.orc, self.npts, self.cur, self.log = orc, npts, None, []
+
+    def set_shard(self, i, n):
+        from oracle import oracle as O
+        self.cur = O.OracleShard(self.orc, self.npts * i // n, self.npts * (i + 1) // n)
+        self.log.append((i, n))
+
+    def partial_size(self):
+        from oracle import oracle as O
+        return O.OracleShard(self.orc, 0, self.npts).partial_size()
+
+    def cycle_partial(self, address):
+        self.cur.cycle_partial(address)
+
+    def cycle_combine(self, address):
+        return self.cur.cycle_combine(address)
+
+
+@pytest.mark.parametrize("nchunks", [1, 3])
+def test_chunked_cycle_equals_one_pass(nchunks):
+    """chunked_cycle (one device, the mesh in passes) adds every chunk's
+    partial sums once and combines them into the one-pass cycle."""
+    from oracle import oracle as O
+    from publicrelease_2020_b200.shard import chunked_cycle
+    sysm = SYSTEMS["water_scan_nspn2"]()
+    orc = O.Oracle(sysm)
+    ref = orc.sic_cycle(nthreads=4)
+    ch = _OracleChunks(orc, sysm.nmsh)
+    got = chunked_cycle(ch, nchunks)
+    assert ch.log == [(i, nchunks) for i in range(nchunks)]
+    assert abs(got["esic"] - ref["esic"]) < 1e-10 * max(1.0, abs(ref["esic"]))
+    for s in range(sysm.nspn):
+        n = sysm.nfrm[s]
+        assert np.allclose(got["results"][s][:n], ref["results"][s][:n], rtol=1e-10, atol=1e-11)
+        assert np.allclose(got["sic"][s][:n, :n], ref["sic"][s][:n, :n], rtol=1e-10, atol=1e-12)
+        assert np.allclose(got["debdax"][s][:n], ref["debdax"][s][:n], rtol=1e-9, atol=1e-10)

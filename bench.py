@@ -72,6 +72,11 @@ def workload(name):
         return s, dict(workload=f"C60 SCAN, 180+180 FODs, {s.nbasis} functions, {s.nmsh} mesh points "
                                 "(a tenth of the 3e6-point C60 mesh)",
                        atoms=60, nbasis=s.nbasis, nmsh=s.nmsh, nfo=180, functional="MGGA-SCAN*MGGA-SCAN", nspn=2)
+    if name == "c5prof":
+        s = W.c60(seed=4, nrad=8)
+        return s, dict(workload=f"C60 SCAN, 180+180 FODs, {s.nbasis} functions, {s.nmsh} mesh points "
+                                "(profiling case: about 480 tiles)",
+                       atoms=60, nbasis=s.nbasis, nmsh=s.nmsh, nfo=180, functional="MGGA-SCAN*MGGA-SCAN", nspn=2)
     if name == "water":
         s = W.water(seed=0, nrad=40)
         return s, dict(workload="water LDA-PW91, 5+5 FODs", atoms=3, nbasis=s.nbasis, nmsh=s.nmsh, nfo=5,
@@ -504,7 +509,7 @@ def main():
                     help="time the FP64 path, the mixed path, or both (headline = mixed when it meets the "
                          "|dE_SIC| <= 1e-5 Ha and FOD-force <= 1e-4 Ha/bohr gates)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "c3", "c4", "c5", "water",
+    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "c3", "c4", "c5", "c5prof", "water",
                                                       "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",

@@ -1,6 +1,6 @@
 """dE_SIC / d(FOD positions) through the basis-space adjoint, as a
-torch.autograd.Function (north_star's differentiation layer; a thin binding
-over the C ABI).
+torch.autograd.Function (the differentiation layer: a thin binding over the
+C ABI).
 
 Forward: one SIC cycle (flosic_sic_cycle) at the given FODs -> E_SIC.
 Backward: the adjoint G = dE_SIC/dC_FO of each spin (flosic_sic_adjoint, a

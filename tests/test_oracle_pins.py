@@ -1,7 +1,9 @@
 """CPU tests pinning the FP64 oracle (oracle/) against closed forms and
 identities.  The reference ships no kernel-level golden vectors and its
-Fortran cannot be built here, so these analytic pins stand in (SURVEY 8(c)
-substitute pins 1, 3, 4, 5, 6, 7, 8)."""
+Fortran cannot be built here, so these analytic pins stand in: Boys values,
+closed-form Coulomb potentials, the multipole far field against the exact
+mode, the charge and r V(r) asymptote, LDA/PW92/PBE/SCAN reference points,
+Lowdin orthonormality and the force chain rule."""
 import math
 import os
 

@@ -907,6 +907,10 @@ struct Stats {
   long long pairs = 0, batches = 0, weird = 0, near = 0, far = 0;
   long long near_multi = 0, far_multi = 0;  // the part from calls of more than one pair
   long long npot1_multi = 0, calls_multi = 0;
+  // optional record of every POISSON1 call: (CG x3, RCUT, NPOT, pairs) per
+  // call, (call, -C x3, delta, COEFICIENT(1:46)) per pair
+  std::vector<double>* calls = nullptr;
+  std::vector<double>* pairs_out = nullptr;
 };
 
 void poisson1(const Problem& P, const std::vector<PairRec>& prs, int nspn, bool gga, bool exact,
@@ -1020,6 +1024,14 @@ void poisson1(const Problem& P, const std::vector<PairRec>& prs, int nspn, bool 
       jptr.resize(nmsh);
       for (int ip = 0; ip < nmsh; ++ip) jptr[ip] = ip;
     }
+  }
+  if (st && st->calls && st->pairs_out) {
+    const double cid = (double)(st->calls->size() / 6);
+    for (int ip = 0; ip < n; ++ip) {
+      st->pairs_out->insert(st->pairs_out->end(), {cid, Cn[ip][0], Cn[ip][1], Cn[ip][2], delt[ip]});
+      st->pairs_out->insert(st->pairs_out->end(), coef[ip].begin(), coef[ip].end());
+    }
+    st->calls->insert(st->calls->end(), {cg[0], cg[1], cg[2], rcut, (double)npot, (double)n});
   }
   if (st) {
     st->near += (long long)jptr.size() * n;
@@ -2621,6 +2633,28 @@ int orc_coupot_sic(orc_problem* p, int spin, int iorb, int exact, double* coulom
     stats[7] = st.npot1_multi;
     stats[8] = st.calls_multi;
   }
+  return 0;
+}
+
+int orc_pair_dump(orc_problem* p, int spin, int iorb, double* calls, long long maxc, long long* ncalls,
+                  double* pairs, long long maxp, long long* npairs) {
+  Problem& P = p->P;
+  if (!P.have_tmat) {
+    int rc = compute_tmat(P);
+    if (rc) return rc;
+  }
+  std::vector<double> c;
+  fo_coefficients(P, spin - 1, c);
+  std::vector<double> coul(P.nmsh), rhog((size_t)10 * P.nmsh), cv, pv;
+  Stats st;
+  st.calls = &cv;
+  st.pairs_out = &pv;
+  coupot_sic(P, &c[(size_t)(iorb - 1) * P.nbasis], false, coul.data(), rhog.data(), &st);
+  *ncalls = (long long)cv.size() / 6;
+  *npairs = (long long)pv.size() / 51;
+  if (*ncalls > maxc || *npairs > maxp) return fail("orc_pair_dump: output arrays too small");
+  std::memcpy(calls, cv.data(), sizeof(double) * cv.size());
+  std::memcpy(pairs, pv.data(), sizeof(double) * pv.size());
   return 0;
 }
 

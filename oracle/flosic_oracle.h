@@ -101,6 +101,13 @@ int orc_sic_cycle(orc_problem* p, int ld, double* results, double* sic, double* 
    [2]=weird pairs, [3]=near (pair,point) evaluations, [4]=far (batch,point) evaluations */
 int orc_pair_stats(orc_problem* p, int spin, int iorb, long long* stats);
 
+/* The POISSON1 calls of coupot_sic.F for one FO, in call order:
+   calls(6, ncalls) = CG(3), RCUT, NPOT, pairs; pairs(51, npairs) = call index,
+   -C(3) (the pair centre negated, as poisson1.f keeps it), delta = alpha+beta,
+   COEFICIENT(1:46) (gtdncf.F).  Fails if maxc/maxp are too small. */
+int orc_pair_dump(orc_problem* p, int spin, int iorb, double* calls, long long maxc, long long* ncalls,
+                  double* pairs, long long maxp, long long* npairs);
+
 /* One mesh point of SUBVLXC (subvlxc_libxc.F90) with NSPN=2 and zero spin-down
    density: r10 = total-density channels; v2 = spin-up/down potentials; e4 =
    weighted EXL, EXN, ECL, ECN. */

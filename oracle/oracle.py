@@ -65,6 +65,8 @@ def lib():
         L.orc_frmorb2_force.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp]
         L.orc_sic_cycle.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_int]
         L.orc_pair_stats.argtypes = [C.c_void_p, C.c_int, C.c_int, _lp]
+        L.orc_pair_dump.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_longlong, _lp, _dp, C.c_longlong,
+                                    _lp]
         L.orc_xc_point.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_double, _dp, _dp]
         L.orc_boys.argtypes = [C.c_int, C.c_double, _dp]
         L.orc_harmonics.argtypes = [C.c_int, _dp, _dp]
@@ -256,6 +258,16 @@ class Oracle:
         _check(lib().orc_pair_stats(self.h, spin, iorb, st))
         return dict(pairs=int(st[0]), batches=int(st[1]), weird=int(st[2]), near=int(st[3]), far=int(st[4]),
                     near_multi=int(st[5]), far_multi=int(st[6]), npot1_multi=int(st[7]), calls_multi=int(st[8]))
+
+    def pair_dump(self, spin=1, iorb=1, maxc=200000, maxp=400000):
+        """POISSON1 calls of one FO: calls (n, 6) = CG(3), RCUT, NPOT, pairs;
+        pairs (m, 51) = call index, -C(3), delta, COEFICIENT(1:46)."""
+        calls = np.zeros(6 * maxc)
+        pairs = np.zeros(51 * maxp)
+        nc = np.zeros(1, dtype=np.int64)
+        npr = np.zeros(1, dtype=np.int64)
+        _check(lib().orc_pair_dump(self.h, spin, iorb, calls, maxc, nc, pairs, maxp, npr))
+        return calls[:6 * nc[0]].reshape(-1, 6), pairs[:51 * npr[0]].reshape(-1, 51)
 
 
 def xc_point(xc, r10, w=1.0):

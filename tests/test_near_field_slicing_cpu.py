@@ -124,3 +124,32 @@ def test_balanced_int8_slices_reach_fp32_class_accuracy(near_calls):
 
 def test_unbalanced_int8_slices_lose_the_potential(near_calls):
     assert _max_rel_error(near_calls, False, 4) > 1e-4
+
+
+def test_balance_shared_by_an_fo_block(near_calls):
+    """One balance per (pair, row) for a block of FOs (the largest |a_k| over
+    the block), one scale per FO row: every FO keeps the accuracy."""
+    _, orc, s = near_calls
+    dumps = [orc.pair_dump(1, k) for k in range(1, 5)]
+    calls = dumps[0][0]
+    assert all(np.array_equal(d[1][:, :5], dumps[0][1][:, :5]) for d in dumps)  # one pair plan
+    r = np.asarray(s.rmsh).reshape(-1, 3)[::5]
+    err, vmax = np.zeros(4), np.zeros(4)
+    for ci, (c0, c1, c2, rc, npot, n) in enumerate(calls):
+        if n <= 1:
+            continue
+        near = np.ones(len(r), bool) if npot == 1 else ((r - [c0, c1, c2]) ** 2).sum(1) <= rc * rc
+        if not near.any():
+            continue
+        sel = dumps[0][1][:, 0] == ci
+        G = np.concatenate([g_rows(r[near], q[1:4], q[4]) for q in dumps[0][1][sel]], axis=1)
+        A = np.stack([d[1][sel][:, 5:51].reshape(-1) for d in dumps])
+        ga, aa = np.abs(G).max(0), np.abs(A).max(0)
+        d = np.ones(A.shape[1])
+        ok = (ga > 0) & (aa > 0)
+        d[ok] = 2.0 ** np.rint(0.5 * np.log2(ga[ok] / aa[ok]))
+        for f in range(4):
+            exact = G @ A[f]
+            err[f] = max(err[f], np.abs(sliced_dot(G / d, A[f] * d, 4) - exact).max())
+            vmax[f] = max(vmax[f], np.abs(exact).max())
+    assert np.all(err / vmax < 1e-7), err / vmax

@@ -153,3 +153,24 @@ def test_balance_shared_by_an_fo_block(near_calls):
             err[f] = max(err[f], np.abs(sliced_dot(G / d, A[f] * d, 4) - exact).max())
             vmax[f] = max(vmax[f], np.abs(exact).max())
     assert np.all(err / vmax < 1e-7), err / vmax
+
+
+def test_one_g_scale_per_call(near_calls):
+    """The G side needs no per-point scale: one scale per call (the largest
+    balanced |g|) keeps 4 slices within 1e-7."""
+    calls, _, _ = near_calls
+    err, vmax = 0.0, 0.0
+    for G, a in calls:
+        exact = G @ a
+        ga, aa = np.abs(G).max(0), np.abs(a)
+        d = np.ones(len(a))
+        ok = (ga > 0) & (aa > 0)
+        d[ok] = 2.0 ** np.rint(0.5 * np.log2(ga[ok] / aa[ok]))
+        Gb, ab = G / d, a * d
+        sa, sg = np.abs(ab).max(), np.abs(Gb).max()
+        qa, qg = int8_slices(ab, sa, 4), int8_slices(Gb, sg, 4)
+        v = sum((qg[u] @ qa[t]).astype(np.float64) * 2.0 ** (-7 * (t + u + 2))
+                for t in range(4) for u in range(4 - t))
+        err = max(err, np.abs(v * sa * sg - exact).max())
+        vmax = max(vmax, np.abs(exact).max())
+    assert err / vmax < 1e-7

@@ -1534,8 +1534,23 @@ int flosic_sic_autotune(flosic_ctx* c, int reps, int* perfo_fos, float* ms) {
     if (!perfo_fos) fail(FLOSIC_ERR_ARG, "null output pointer");
     const int s = (c->nspn == 2 && c->nfrm[1] > c->nfrm[0]) ? 1 : 0;
     if (c->nfrm[s] < 1) fail(FLOSIC_ERR_STATE, "no FOs to tune on");
-    const unsigned long long wn = c->work_near, wf = c->work_far, wt = c->work_terms;
-    const long long nl = c->launches;
+    // The timing runs overwrite this spin's potentials: drop the cached ones
+    // first, and put the width and counters back on every way out.
+    c->spin[s].pot_valid = false;
+    c->spin[s].sic_valid = false;
+    struct Restore {
+      flosic_ctx* c;
+      int wm;
+      unsigned long long wn, wf, wt;
+      long long nl;
+      ~Restore() {
+        c->coulomb_cfg.perfo_wm = wm;
+        c->work_near = wn;
+        c->work_far = wf;
+        c->work_terms = wt;
+        c->launches = nl;
+      }
+    } restore{c, c->coulomb_cfg.perfo_wm, c->work_near, c->work_far, c->work_terms, c->launches};
     fo_setup(c, s);
     const int nf = c->spin[s].nf;
     cudaStream_t st = c->st;
@@ -1561,13 +1576,7 @@ int flosic_sic_autotune(flosic_ctx* c, int reps, int* perfo_fos, float* ms) {
         best_wm = wm;
       }
     }
-    c->coulomb_cfg.perfo_wm = best_wm;
-    c->spin[s].pot_valid = false;
-    c->spin[s].sic_valid = false;
-    c->work_near = wn;
-    c->work_far = wf;
-    c->work_terms = wt;
-    c->launches = nl;
+    restore.wm = best_wm;
     *perfo_fos = 32 * best_wm;
   });
 }

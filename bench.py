@@ -63,6 +63,11 @@ def workload(name):
             dict(workload="C2 density of atoms and points in a 7.56 A box: 10 atoms, 128 functions, 2.5e5 points, "
                           "64 FOs (profiling case)", atoms=10, nbasis=128, nmsh=250_000, nfo=64,
                  functional="GGA-PBE*GGA-PBE", nspn=1)
+    if name == "c1":
+        s = W.water(seed=0, nrad=60, basis="default")
+        return s, dict(workload=f"C1 water LDA-PW91, default NRLMOL basis ({s.nbasis} functions), 5+5 FODs, "
+                                f"{s.nmsh}-point atom-centred mesh", atoms=3, nbasis=s.nbasis, nmsh=s.nmsh, nfo=5,
+                       functional="LDA-PW91*LDA-PW91", nspn=2)
     if name == "c3":
         s = W.benzene(seed=3, nrad=228)
         return s, dict(workload=f"benzene LDA-PW91, 21+21 FODs, {s.nbasis} functions, {s.nmsh} mesh points",
@@ -509,7 +514,7 @@ def main():
                     help="time the FP64 path, the mixed path, or both (headline = mixed when it meets the "
                          "|dE_SIC| <= 1e-5 Ha and FOD-force <= 1e-4 Ha/bohr gates)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c2half", "c2tiny", "c2prof", "c3", "c4", "c5", "c5prof", "water",
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2half", "c2tiny", "c2prof", "c3", "c4", "c5", "c5prof", "water",
                                                       "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",

@@ -5,9 +5,11 @@ orbitals), so every system here is generated from a seed:
 
 * ``water``      -- O at the origin, H at (+-0.757, 0, 0.587) A, an
   even-tempered basis with the NRLMOL default shapes (O: 13 bare primitives,
-  5s4p3d; H: 6 bare primitives, 4s3p1d; 73 functions), an atom-centred
-  radial x Lebedev mesh standing in for the variational mesh (vmesh.F), 5+5
-  FODs at a 1s + tetrahedral guess perturbed by N(0, 0.05 bohr).
+  5s4p3d; H: 6 bare primitives, 4s3p1d; 73 functions) or, with
+  basis="default", the reference's default NRLMOL basis itself
+  (nrlmol_default_type), an atom-centred radial x Lebedev mesh standing in
+  for the variational mesh (vmesh.F), 5+5 FODs at a 1s + tetrahedral guess
+  perturbed by N(0, 0.05 bohr).
 * ``synthetic``  -- N atoms uniform in a cube (min separation 1.8 bohr),
   contracted Cartesian s/p/d functions with 3 primitives each (exponents
   log-uniform in [0.05, 1e4]), jittered uniform mesh with weights summing to
@@ -22,6 +24,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 
 import numpy as np
 
@@ -178,6 +181,38 @@ def _nrlmol_like_type(nprim, ncon, amin, amax, rng):
     return alp, con
 
 
+_NRLMOL_TABLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "nrlmol_default_basis.npz")
+
+
+def nrlmol_default_type(z):
+    """The reference's default all-electron basis for element z (H, C or O).
+
+    The tables are the NRLMOL bare exponents and full contractions that
+    flosic/bdallbas.f stores, kept in data/nrlmol_default_basis.npz.  To them
+    SALLBAS adds, per l, single-primitive functions with coefficient 1
+    (sallbas.f:86-104, 133-153): three on the most diffuse primitives for s
+    and p, and three on the next-to-most-diffuse ones for d.  An atom without
+    p contractions (H) moves its p singles one primitive tighter and gets one
+    d single on the third most diffuse primitive.  The supplementary set
+    NBASF(2, l) is left out, as READINP does unless EXTRABASIS asks for it
+    (readinp.F:137-186).  The exponents are already in the descending order
+    READINP sorts them into.  Returns (alpha, con[l, c, i], n_con)."""
+    tab = np.load(_NRLMOL_TABLES)
+    nspd, alph, coef = tab[f"nspd_{z}"], tab[f"alph_{z}"], tab[f"coef_{z}"]
+    nalp = len(alph)
+    if not np.all(np.diff(alph) < 0):
+        raise ValueError("NRLMOL exponents must be in descending order")
+    nadd, ibofs = [3, 3, 3], [0, 0, 1]
+    if nspd[1] == 0:
+        ibofs[1], nadd[2], ibofs[2] = 1, 1, 2
+    con = np.zeros((3, MAX_CON, MAX_BARE))
+    for l in range(3):
+        con[l, : nspd[l], :nalp] = coef[l, : nspd[l]]
+        for i in range(1, nadd[l] + 1):
+            con[l, nspd[l] + i - 1, nalp - ibofs[l] - nadd[l] + i - 1] = 1.0
+    return np.array(alph), con, tuple(int(nspd[l] + nadd[l]) for l in range(3))
+
+
 def _pack_types(types):
     nt = len(types)
     n_bare = np.array([len(t[0]) for t in types], dtype=np.int32)
@@ -289,17 +324,22 @@ def atom_centred_mesh(rat, nrad=40, rscale=None, seed=0):
 # ---------------------------------------------------------------------------
 # systems
 # ---------------------------------------------------------------------------
-def water(seed=0, nrad=40, functional="LDA-PW91*LDA-PW91"):
-    """C1: water, NRLMOL-shaped basis, 5+5 FODs, NSPN=2; LDA-PW91*LDA-PW91 unless
-    another functional is named."""
+def water(seed=0, nrad=40, functional="LDA-PW91*LDA-PW91", basis="nrlmol-like"):
+    """C1: water, 5+5 FODs, NSPN=2; LDA-PW91*LDA-PW91 unless another functional
+    is named.  basis="default" is the reference's default NRLMOL basis
+    (nrlmol_default_type: O 5s4p3d, H 4s3p1d, 73 functions); "nrlmol-like"
+    has the same shape with even-tempered exponents."""
     rng = np.random.default_rng(seed)
     b = BOHR_PER_ANG
     rat = np.array([[0.0, 0.0, 0.0], [0.757 * b, 0.0, 0.587 * b], [-0.757 * b, 0.0, 0.587 * b]])
-    types = []
-    alp, con = _nrlmol_like_type(13, (5, 4, 3), 0.12, 6.0e4, rng)
-    types.append((alp, con, (5, 4, 3)))
-    alp, con = _nrlmol_like_type(6, (4, 3, 1), 0.08, 80.0, rng)
-    types.append((alp, con, (4, 3, 1)))
+    if basis == "default":
+        types = [nrlmol_default_type(8), nrlmol_default_type(1)]
+    else:
+        types = []
+        alp, con = _nrlmol_like_type(13, (5, 4, 3), 0.12, 6.0e4, rng)
+        types.append((alp, con, (5, 4, 3)))
+        alp, con = _nrlmol_like_type(6, (4, 3, 1), 0.08, 80.0, rng)
+        types.append((alp, con, (4, 3, 1)))
     n_bare, bfalp, n_con, bfcon = _pack_types(types)
     rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[0.7, 0.5, 0.5], seed=seed + 1)
     sysm = System("water", rat, np.array([0, 1, 1], dtype=np.int32), n_bare, bfalp, n_con, bfcon,
@@ -432,21 +472,27 @@ def _fods_conditioned(sysm, fods, rng, sigma=0.05, min_eig=1e-4, tries=50):
     return out
 
 
-def benzene(seed=3, nrad=40, functional="LDA-PW91*LDA-PW91"):
-    """C3: benzene, planar D6h (C-C 1.39 A, C-H 1.09 A), NRLMOL-shaped basis
-    (C 5s4p3d = 35 functions, H 4s3p1d = 19; 324 in all), 21+21 FODs at core,
-    C-H and C-C bond and pi positions, perturbed by N(0, 0.05 bohr); NSPN=2."""
+def benzene(seed=3, nrad=40, functional="LDA-PW91*LDA-PW91", basis="nrlmol-like"):
+    """C3: benzene, planar D6h (C-C 1.39 A, C-H 1.09 A), C 5s4p3d = 35
+    functions, H 4s3p1d = 19 (324 in all), 21+21 FODs at core, C-H and C-C
+    bond and pi positions, perturbed by N(0, 0.05 bohr); NSPN=2.
+    basis="default" is the reference's default NRLMOL basis
+    (nrlmol_default_type); "nrlmol-like" has the same shape with
+    even-tempered exponents."""
     rng = np.random.default_rng(seed)
     b = BOHR_PER_ANG
     ang = np.arange(6) * np.pi / 3
     ring = np.stack([np.cos(ang), np.sin(ang), np.zeros(6)], axis=1)
     rc, rh = 1.39 * b, (1.39 + 1.09) * b
     rat = np.concatenate([rc * ring, rh * ring])
-    types = []
-    alp, con = _nrlmol_like_type(14, (5, 4, 3), 0.08, 2.2e4, rng)
-    types.append((alp, con, (5, 4, 3)))
-    alp, con = _nrlmol_like_type(6, (4, 3, 1), 0.08, 80.0, rng)
-    types.append((alp, con, (4, 3, 1)))
+    if basis == "default":
+        types = [nrlmol_default_type(6), nrlmol_default_type(1)]
+    else:
+        types = []
+        alp, con = _nrlmol_like_type(14, (5, 4, 3), 0.08, 2.2e4, rng)
+        types.append((alp, con, (5, 4, 3)))
+        alp, con = _nrlmol_like_type(6, (4, 3, 1), 0.08, 80.0, rng)
+        types.append((alp, con, (4, 3, 1)))
     n_bare, bfalp, n_con, bfcon = _pack_types(types)
     rmsh, wmsh = atom_centred_mesh(rat, nrad=nrad, rscale=[0.7] * 6 + [0.5] * 6, seed=seed + 1)
     sysm = System("benzene", rat, np.array([0] * 6 + [1] * 6, dtype=np.int32), n_bare, bfalp, n_con, bfcon,

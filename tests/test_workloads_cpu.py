@@ -49,3 +49,36 @@ def test_generators_are_reproducible(make):
         assert np.array_equal(np.asarray(getattr(a, key)), np.asarray(getattr(b, key))), key
     for s in range(a.nspn):
         assert np.array_equal(np.asarray(a.fods[s]), np.asarray(b.fods[s]))
+
+
+def test_nrlmol_default_basis_shapes():
+    """SALLBAS's default basis: O and C 5s4p3d, H 4s3p1d, singles with
+    coefficient 1 on the primitives sallbas.f picks."""
+    for z, nbare, ncon in ((8, 13, (5, 4, 3)), (6, 12, (5, 4, 3)), (1, 6, (4, 3, 1))):
+        alp, con, n = W.nrlmol_default_type(z)
+        assert len(alp) == nbare and n == ncon and np.all(np.diff(alp) < 0)
+        nspd = (1, 0, 0) if z == 1 else (2, 1, 0)
+        singles = {8: ([10, 11, 12], [10, 11, 12], [9, 10, 11]), 6: ([9, 10, 11], [9, 10, 11], [8, 9, 10]),
+                   1: ([3, 4, 5], [2, 3, 4], [3])}[z]
+        for l in range(3):
+            for i, prim in enumerate(singles[l]):
+                row = con[l, nspd[l] + i]
+                assert row[prim] == 1.0 and np.count_nonzero(row) == 1, (z, l, i)
+            assert np.count_nonzero(con[l, n[l]:]) == 0
+    w = W.water(seed=0, nrad=8, basis="default")
+    b = W.benzene(nrad=6, basis="default")
+    assert w.nbasis == 73 and b.nbasis == 324
+
+
+def test_default_basis_water_sic_cycle_is_physical():
+    """With the reference's default basis the oracle's FO charges integrate
+    to one on the stand-in mesh and the per-FO SIC energies are a few mHa to
+    tens of mHa, as for a real molecule."""
+    from oracle import oracle as O
+    s = W.water(seed=0, nrad=16, basis="default")
+    r = O.Oracle(s).sic_cycle(nthreads=4)
+    for sp in range(2):
+        res = r["results"][sp][:5]
+        assert np.allclose(res[:, 1], 1.0, atol=0.03)          # XCH1
+        assert np.all((res[:, 8] > 0.0) & (res[:, 8] < 0.1))   # per-FO SIC energy
+    assert 0.05 < r["esic"] < 0.5

@@ -69,8 +69,9 @@ def workload(name):
                                 f"{s.nmsh}-point atom-centred mesh", atoms=3, nbasis=s.nbasis, nmsh=s.nmsh, nfo=5,
                        functional="LDA-PW91*LDA-PW91", nspn=2)
     if name == "c3":
-        s = W.benzene(seed=3, nrad=228)
-        return s, dict(workload=f"benzene LDA-PW91, 21+21 FODs, {s.nbasis} functions, {s.nmsh} mesh points",
+        s = W.benzene(seed=3, nrad=228, basis="default")
+        return s, dict(workload=f"benzene LDA-PW91, 21+21 FODs, default NRLMOL basis ({s.nbasis} functions), "
+                                f"{s.nmsh} mesh points",
                        atoms=12, nbasis=s.nbasis, nmsh=s.nmsh, nfo=21, functional="LDA-PW91*LDA-PW91", nspn=2)
     if name == "c5":
         s = W.c60(seed=4, nrad=40)

@@ -36,7 +36,7 @@ enum {
   FLOSIC_ERR_ZERO_DENSITY = 4,  /* zero density at an FOD                        */
   FLOSIC_ERR_NFRM = 5,          /* MORB .NE. NFRM (frmiorb.f:418)                */
   FLOSIC_ERR_ZERO_COULOMB = 6,  /* "COUPOT IS ZERO" (apotnl_sic.F:277-283)       */
-  FLOSIC_ERR_CUDA = 7,          /* CUDA / cuBLAS failure                         */
+  FLOSIC_ERR_CUDA = 7,          /* CUDA failure, or a kernel wait that gave up    */
   FLOSIC_ERR_STATE = 8          /* call order: geometry/orbitals not set         */
 };
 
@@ -124,6 +124,16 @@ int flosic_sic_mgga_mixin(flosic_ctx* ctx, int lspx, int iorbx, double* mixin);
 enum { FLOSIC_PRECISION_FP64 = 0, FLOSIC_PRECISION_MIXED = 1 };
 int flosic_sic_set_precision(flosic_ctx* ctx, int mode);
 
+/* Poll limit of every wait between the roles of the mixed-precision
+   tensor-core Coulomb kernel (no counterpart in the reference).  Each wait on
+   a pipeline barrier gives up after `polls` polls (polls <= 0: the default,
+   2^25, far above any legitimate wait); the kernel then stops its roles,
+   drains its own copies and tensor-core operations, frees its tensor memory
+   and returns, and the call reports FLOSIC_ERR_CUDA with the context still
+   usable.  A small limit makes the waits run out on purpose, which is how the
+   error path is tested without a GPU fault; restore the default afterwards. */
+int flosic_sic_set_wait_limit(flosic_ctx* ctx, int64_t polls);
+
 /* Tile-shape autotuner (no counterpart in the reference, whose POISSON1 batch
    shapes are compile-time constants: MXPR pairs per call, coupot_sic.F:46, and
    MPX points per block, poisson1.f:62).  Times the per-FO Coulomb kernel with
@@ -183,6 +193,15 @@ int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, doub
    FO construction.  On a mesh shard the result is the shard's partial sum,
    to be summed over the shards (the dE/dC part of the exchange). */
 int flosic_sic_adjoint(flosic_ctx* ctx, int lspn, double* g, int ldg);
+
+/* dE_SIC/d(FOD positions) of spin lspn, grad(3, ld) as DEBDAX (ld >= NFRM):
+   the adjoint G of flosic_sic_adjoint carried through the FO construction
+   (the Lowdin-orthonormalised Fermi transformation of frmiorb.f:351-480 and
+   FMAT's FOD derivatives, frmorb2.F:296-346) inside the library.  It equals
+   the FOD force of FRMORB2(-LSPN,-1) (frmorb2.F:586-717) times 2/NSPN, reached
+   without the SIC matrix; the reference has no single routine for it.  Whole
+   mesh only. */
+int flosic_sic_adjoint_fod(flosic_ctx* ctx, int lspn, double* grad, int ld);
 
 /* SICLAG_DER / SICLM_DERSLV (siclag_der.F:2-688): the basis-centre (Pulay)
    terms of the SIC atomic forces,

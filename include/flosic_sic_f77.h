@@ -56,6 +56,7 @@ void flosic_sic_getvlxc_mgga_(const int64_t* ctx, const int32_t* ndim, const dou
 void flosic_sic_mgga_mixin_(const int64_t* ctx, const int32_t* lspx, const int32_t* iorbx, double* mixin,
                             int32_t* ierr);
 void flosic_sic_set_precision_(const int64_t* ctx, const int32_t* mode, int32_t* ierr);
+void flosic_sic_set_wait_limit_(const int64_t* ctx, const int64_t* polls, int32_t* ierr);
 void flosic_sic_autotune_(const int64_t* ctx, const int32_t* reps, int32_t* perfo_fos, float* ms,
                           int32_t* ierr);
 void flosic_sic_getvlxc_device_(const int64_t* ctx, const int32_t* npts, const int64_t* d_rhog,
@@ -71,6 +72,8 @@ void flosic_sic_cycle_(const int64_t* ctx, const int32_t* ld, double* results, d
                        double* cfrm, double* esic, int32_t* ierr);
 void flosic_sic_adjoint_(const int64_t* ctx, const int32_t* lspn, double* g, const int32_t* ldg,
                          int32_t* ierr);
+void flosic_sic_adjoint_fod_(const int64_t* ctx, const int32_t* lspn, double* grad, const int32_t* ld,
+                             int32_t* ierr);
 void flosic_sic_siclag_der_(const int64_t* ctx, double* dersic, const int32_t* ldo, int32_t* ierr);
 void flosic_sic_sicham_(const int64_t* ctx, const int32_t* lspn, double* ham, const int32_t* ldh,
                         const int32_t* packed, int32_t* ierr);

@@ -96,6 +96,10 @@ struct Problem {
   std::vector<int> aoff;         // per atom: basis offset
   int nbasis = 0;
   std::vector<double> rmsh, wmsh;
+  // Weight of each mesh point in the POISSON1 cost model (poisson1.f:569-583):
+  // 1 for the real mesh; m when the mesh is every m-th point of a larger one,
+  // so that a timing sample makes the near/far choices of the full mesh.
+  double count_scale = 1.0;
   int igga[2] = {0, 0}, idftyp[2] = {6, 6};
   // orbitals
   int nwfs[2] = {0, 0};
@@ -1016,8 +1020,9 @@ void poisson1(const Problem& P, const std::vector<PairRec>& prs, int nspn, bool 
   }
   int npot = 2;
   {
-    double cost1 = 1.36 * ((double)jptr.size() + NANG) * nslots + 0.99 * (double)iptr.size();
-    double cost2 = 1.36 * ((double)iptr.size() + (double)jptr.size()) * nslots;
+    const double cs = P.count_scale;
+    double cost1 = 1.36 * ((double)jptr.size() * cs + NANG) * nslots + 0.99 * (double)iptr.size() * cs;
+    double cost2 = 1.36 * ((double)iptr.size() + (double)jptr.size()) * cs * nslots;
     if (cost2 < cost1) {
       npot = 1;
       iptr.clear();
@@ -3036,6 +3041,11 @@ int orc_fo_energy(orc_problem* p, int spin, const double* cfo, double* results) 
 
 int orc_set_xc_exact_density(orc_problem* p, int on) {
   p->P.xc_exact_density = on != 0;
+  return 0;
+}
+
+int orc_set_count_scale(orc_problem* p, double scale) {
+  p->P.count_scale = scale > 0.0 ? scale : 1.0;
   return 0;
 }
 

@@ -64,6 +64,8 @@ int orc_fo_tau(orc_problem* p, int spin, int iorb, double* tau);
 /* Test knob: XC on the untruncated (every point near) pair density while the
    Coulomb potential keeps the near/far split (0 = the reference's behaviour). */
 int orc_set_xc_exact_density(orc_problem* p, int on);
+/* weight of a mesh point in POISSON1's near/far cost model (timing samples of a larger mesh) */
+int orc_set_count_scale(orc_problem* p, double scale);
 /* SICLAG_DER: DERSIC(3, ldo, natoms) as dersic[(A*ldo + lfn)*3 + ix] */
 int orc_siclag_der(orc_problem* p, double* dersic, int ldo);
 /* APOTNL_SIC RESULTS(13) of one orbital given by its basis coefficients */

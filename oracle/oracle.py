@@ -50,6 +50,7 @@ def lib():
         L.orc_getvlxc_mgga.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.orc_fo_tau.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.orc_set_xc_exact_density.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_count_scale.argtypes = [C.c_void_p, C.c_double]
         L.orc_siclag_der.argtypes = [C.c_void_p, _dp, C.c_int]
         L.orc_fo_energy.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.orc_sicham.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
@@ -229,6 +230,11 @@ class Oracle:
     def set_xc_exact_density(self, on):
         """XC on the untruncated pair density (the GPU's phi^2), Coulomb unchanged."""
         _check(lib().orc_set_xc_exact_density(self.h, int(bool(on))))
+
+    def set_count_scale(self, scale):
+        """Weight of each mesh point in POISSON1's near/far cost model: m when this
+        mesh is every m-th point of a larger one (timing samples)."""
+        _check(lib().orc_set_count_scale(self.h, float(scale)))
 
     def fo_tau(self, spin, iorb):
         """tau = |grad phi_k|^2 / 2 of one FO at the mesh points (GETTAU_PAR)."""

@@ -826,7 +826,7 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
     launch_split_tf32((size_t)npairs, nfo, coef, scr.coef_hl, st);
     launch_split_tf32((size_t)ncalls, nfo, momv, scr.momv_hl, st);
     launch_coulomb_shared_tc(ncalls, scr.lists, scr.share, calls, nfo, scr.coef_hl, nc, scr.pair_fmt, pairs,
-                             scr.momv_hl, nm, M, boys_tab, vh, ldv, cnt, scr.err, st);
+                             scr.momv_hl, nm, M, boys_tab, vh, ldv, cnt, scr.err, cfg.wait_limit, st);
   } else if (!per_fo_only) {
     if (nfo > 64)
       launch_shared<4>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,

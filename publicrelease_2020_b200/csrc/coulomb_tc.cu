@@ -43,7 +43,7 @@ constexpr int TC_NPROD = 256;            // producer threads: two per point, alt
 constexpr int TC_NSTAGE = 128;           // calls staged per chunk
 constexpr int TC_BAR_PROD = 5;           // named barrier of the producer warps
 constexpr uint32_t TC_TMEM_COLS = 512;   // D0 | D1 | V_hi | V_lo, 128 columns each
-constexpr long TC_SPIN_LIMIT = 1L << 25;
+constexpr long TC_SPIN_LIMIT = 1L << 25;  // default poll limit of every wait; drains always use it
 
 // One shared-geometry call as the producers walk it.
 struct TcCall {
@@ -86,9 +86,9 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase with the given parity; false (and the abort flag
-// set) when the limit is reached or another role has aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
-  for (long it = 0; it < TC_SPIN_LIMIT; ++it) {
+// set) when `limit` polls are reached or another role has aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, long limit) {
+  for (long it = 0; it < limit; ++it) {
     if (mbar_try(b, parity)) return true;
     if ((it & 255) == 255) {
       if (*abort) return false;
@@ -282,7 +282,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
                     const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
                     const float* __restrict__ momv_hl, size_t coef_part, size_t mom_part, MeshDev M,
                     const double* __restrict__ boys_tab, double* __restrict__ vh, int ldv,
-                    unsigned long long* __restrict__ cnt, int* __restrict__ err) {
+                    unsigned long long* __restrict__ cnt, int* __restrict__ err, long wait_limit) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
   const int tile = blockIdx.x;
@@ -342,7 +342,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
     bool open = false, ok = true;
     auto win_open = [&]() {
       buf = w % TC_NB;
-      if (w >= TC_NB && !mbar_wait(&S.empty[buf], (uint32_t)((w / TC_NB - 1) & 1), abort)) ok = false;
+      if (w >= TC_NB && !mbar_wait(&S.empty[buf], (uint32_t)((w / TC_NB - 1) & 1), abort, wait_limit)) ok = false;
       fill = 0;
       open = true;
     };
@@ -494,14 +494,14 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
       int a = 0, nin = 0, g = 0;
       for (int w = 0;; ++w) {
         const int b = w % TC_NB;
-        if (!mbar_wait(&S.full[b], (uint32_t)((w / TC_NB) & 1), abort)) break;
+        if (!mbar_wait(&S.full[b], (uint32_t)((w / TC_NB) & 1), abort, wait_limit)) break;
         // the window's cp.async data (generic proxy) is read by the tensor core
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         tc_fence_after();
         const int r = S.win_rows[b], last = S.win_last[b];
         if (r > 0) {
           if (nin == 0 && g >= 2) {
-            if (!mbar_wait(&S.accempty[a], (uint32_t)((g / 2 - 1) & 1), abort)) break;
+            if (!mbar_wait(&S.accempty[a], (uint32_t)((g / 2 - 1) & 1), abort, wait_limit)) break;
             tc_fence_after();
           }
           const uint32_t d = tmem + (uint32_t)(a * TILE);
@@ -549,7 +549,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
     for (int g = 0;; ++g) {
       const int a = g & 1;
       bool have = false;
-      for (long it = 0; it < TC_SPIN_LIMIT; ++it) {
+      for (long it = 0; it < wait_limit; ++it) {
         if (mbar_try(&S.accfull[a], (uint32_t)((g / 2) & 1))) {
           have = true;
           break;
@@ -559,7 +559,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
           if (mbar_try(&S.done, 0u) && g >= S.ngroups) break;
           __nanosleep(128);
         }
-        if (it == TC_SPIN_LIMIT - 1) *abort = 1;
+        if (it == wait_limit - 1) *abort = 1;
       }
       if (!have) break;
       tc_fence_after();
@@ -646,11 +646,13 @@ void launch_split_tf32(size_t nrow, int nfo, const double* src, float* out, cuda
 void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
                               const float* coef_hl, size_t coef_part, const int8_t* pair_fmt, const PairGeo* pairs,
                               const float* momv_hl, size_t mom_part, const MeshDev& M, const double* boys_tab,
-                              double* vh, int ldv, unsigned long long* cnt, int* err, cudaStream_t st) {
+                              double* vh, int ldv, unsigned long long* cnt, int* err, long long wait_limit,
+                              cudaStream_t st) {
   dim3 grid(M.ntiles, (nfo + TILE - 1) / TILE);
+  const long lim = wait_limit > 0 ? (long)wait_limit : TC_SPIN_LIMIT;
   k_coulomb_shared_tc<<<grid, TC_THREADS, sizeof(TcSmem), st>>>(ncalls, lists, share, calls, nfo, coef_hl,
                                                                    pair_fmt, pairs, momv_hl, coef_part, mom_part, M,
-                                                                   boys_tab, vh, ldv, cnt, err);
+                                                                   boys_tab, vh, ldv, cnt, err, lim);
 }
 
 }  // namespace flosic

@@ -91,6 +91,10 @@ void flosic_sic_set_precision_(const int64_t* ctx, const int32_t* mode, int32_t*
   *ierr = flosic_sic_set_precision(handle(ctx), *mode);
 }
 
+void flosic_sic_set_wait_limit_(const int64_t* ctx, const int64_t* polls, int32_t* ierr) {
+  *ierr = flosic_sic_set_wait_limit(handle(ctx), *polls);
+}
+
 void flosic_sic_autotune_(const int64_t* ctx, const int32_t* reps, int32_t* perfo_fos, float* ms, int32_t* ierr) {
   *ierr = flosic_sic_autotune(handle(ctx), *reps, perfo_fos, ms);
 }
@@ -122,6 +126,11 @@ void flosic_sic_cycle_(const int64_t* ctx, const int32_t* ld, double* results, d
 
 void flosic_sic_adjoint_(const int64_t* ctx, const int32_t* lspn, double* g, const int32_t* ldg, int32_t* ierr) {
   *ierr = flosic_sic_adjoint(handle(ctx), *lspn, g, *ldg);
+}
+
+void flosic_sic_adjoint_fod_(const int64_t* ctx, const int32_t* lspn, double* grad, const int32_t* ld,
+                             int32_t* ierr) {
+  *ierr = flosic_sic_adjoint_fod(handle(ctx), *lspn, grad, *ld);
 }
 
 void flosic_sic_siclag_der_(const int64_t* ctx, double* dersic, const int32_t* ldo, int32_t* ierr) {

@@ -1077,6 +1077,16 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc_rhog(MeshDev M, int gga, XCPa
   block_reduce_parts(pv, part + (size_t)blockIdx.x * NPART);
 }
 
+// Loads the two kernels of the GETVLXC-on-device-buffers path on the current
+// device.  With CUDA's lazy loading a kernel's code is placed in device memory
+// at its first launch; doing that here, at context creation, keeps that
+// allocation out of the allocation-free entry point.
+cudaError_t preload_xc_rhog() {
+  cudaFuncAttributes a;
+  const cudaError_t e = cudaFuncGetAttributes(&a, k_xc_rhog);
+  return e != cudaSuccess ? e : cudaFuncGetAttributes(&a, k_reduce_parts);
+}
+
 void launch_xc_rhog(const MeshDev& M, int gga, const int* xc, const double* rhog, int ldr, double* vxc,
                     double* part, int nblk, cudaStream_t st) {
   XCParams xp;

@@ -92,6 +92,7 @@ struct CoulombConfig {
   bool per_fo_only = false;
   bool shared_tc = true;
   int perfo_wm = 0;
+  long long wait_limit = 0;  // polls of each tensor-core pipeline wait before it gives up (0: the default)
 };
 void init_coulomb_mma();
 void init_coulomb_tc();
@@ -102,7 +103,8 @@ void launch_split_tf32(size_t nrow, int nfo, const double* src, float* out, cuda
 void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
                               const float* coef_hl, size_t coef_part, const int8_t* pair_fmt, const PairGeo* pairs,
                               const float* momv_hl, size_t mom_part, const MeshDev& M, const double* boys_tab,
-                              double* vh, int ldv, unsigned long long* cnt, int* err, cudaStream_t st);
+                              double* vh, int ldv, unsigned long long* cnt, int* err, long long wait_limit,
+                              cudaStream_t st);
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
@@ -125,6 +127,27 @@ void launch_xc_mgga_rhog(const MeshDev& M, const double* rhog, int ldr, const do
                          double* mixin, double* part, int nblk, cudaStream_t st);
 
 // Vxc of given density channels (GETVLXC entry point): vxc[2*n], parts as above (1 FO).
+// Dense products on the FP64 tensor cores (csrc/contract.cu).
+// dgemm: C = alpha op(A) op(B) + beta C, column-major as BLAS DGEMM; work holds
+// dgemm_work(M, N, K) doubles (split-K partial products; 0: none needed).
+size_t dgemm_work(int M, int N, int K);
+void dgemm(bool ta, bool tb, int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+           double beta, double* C, int ldc, double* work, cudaStream_t st);
+// out[(ch*ncol + k)*ldo + p] = sum_f B_ch(p, f) coef[k*ldc + f]: basis values
+// (nderv 0, 1, 2 -> 1, 4, 10 channels) at npts points times ncol coefficient columns.
+cudaError_t init_contract();
+void launch_fo_values(const BasisDev& B, int nderv, int npts, const double* px, const double* py, const double* pz,
+                      const double* coef, int ldc, int ncol, double* out, size_t ldo, cudaStream_t st);
+// out[k*ldo + p] = w[p] a[k*lda + p]
+void launch_scale_rows(int P, int N, const double* a, int lda, const double* w, double* out, int ldo,
+                       cudaStream_t st);
+// Symmetric eigen-decomposition (one CTA, cyclic Jacobi; csrc/eigen.cu): a is
+// n x n row-major, work holds sym_eigen_work(n) doubles; w ascending,
+// v[k*n + m] = component k of eigenvector m; info 0, or 1 without convergence.
+cudaError_t init_sym_eigen();
+size_t sym_eigen_work(int n);
+bool launch_sym_eigen(int n, const double* a, double* work, double* w, double* v, int* info, cudaStream_t st);
+cudaError_t preload_xc_rhog();
 void launch_xc_rhog(const MeshDev& M, int gga, const int* xc, const double* rhog, int ldr, double* vxc,
                     double* part, int nblk, cudaStream_t st);
 

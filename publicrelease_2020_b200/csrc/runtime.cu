@@ -7,8 +7,6 @@
 // A spin's FO potentials are computed for all FOs in batched launches and
 // cached in GPU memory; APOTNL_SIC / SICLAGM / FRMORB2 entry points read from
 // that cache instead of the ZPOT#### files.
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,11 +45,6 @@ struct Fail {
   do {                                                                                  \
     cudaError_t e_ = (x);                                                               \
     if (e_ != cudaSuccess) fail(FLOSIC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-#define BLAS_CHECK(x)                                                              \
-  do {                                                                             \
-    cublasStatus_t s_ = (x);                                                       \
-    if (s_ != CUBLAS_STATUS_SUCCESS) fail(FLOSIC_ERR_CUDA, std::string(#x) + " failed"); \
   } while (0)
 
 const int kNcomp[3] = {1, 3, 6};
@@ -286,9 +279,8 @@ struct SpinCache {
 struct flosic_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
-  cublasHandle_t blas = nullptr;
-  cusolverDnHandle_t solver = nullptr;
-  DevBuf<double> d_eig_a, d_eig_w, d_eig_work;
+  DevBuf<double> d_gemm_ws;  // split-K partial products of dgemm
+  DevBuf<double> d_eig_a, d_eig_w, d_eig_v, d_eig_work;
   DevBuf<int> d_eig_info;
   bool have_geom = false, have_orb = false;
   // geometry
@@ -606,38 +598,38 @@ void set_eval_range(flosic_ctx* c) {
 // ---------------------------------------------------------------------------
 // FO construction (FRMORB2(0,0) and FRMIORB(1,1)) for one spin
 // ---------------------------------------------------------------------------
-#define SOLVER_CHECK(x)                                                                 \
-  do {                                                                                  \
-    cusolverStatus_t s_ = (x);                                                          \
-    if (s_ != CUSOLVER_STATUS_SUCCESS) fail(FLOSIC_ERR_CUDA, std::string(#x) + " failed (" + std::to_string((int)s_) + ")"); \
-  } while (0)
+// C = alpha op(A) op(B) + beta C on the context stream (column-major, as BLAS
+// DGEMM), on the FP64 tensor cores (csrc/contract.cu).
+void gemm(flosic_ctx* c, bool ta, bool tb, int M, int N, int K, double alpha, const double* A, int lda,
+          const double* B, int ldb, double beta, double* C, int ldc) {
+  const size_t w = dgemm_work(M, N, K);
+  if (w) c->d_gemm_ws.ensure(w);
+  dgemm(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, c->d_gemm_ws.p, c->st);
+  c->launches += w ? 2 : 1;
+}
 
-// Symmetric eigen-decomposition on the GPU (cuSOLVER syevd, FP64, ascending
-// eigenvalues) in the convention lowsic expects.
+// Symmetric eigen-decomposition on the GPU (k_sym_eigen, cyclic Jacobi,
+// FP64, ascending eigenvalues) in the convention lowsic expects.
 auto device_eigen(flosic_ctx* c) {
   return [c](int n, const std::vector<double>& a, std::vector<double>& w, std::vector<double>& v) {
     cudaStream_t st = c->st;
     c->d_eig_a.upload(a.data(), (size_t)n * n, st);
     c->d_eig_w.ensure(n);
+    c->d_eig_v.ensure((size_t)n * n);
+    c->d_eig_work.ensure(sym_eigen_work(n));
     c->d_eig_info.ensure(1);
-    int lwork = 0;
-    SOLVER_CHECK(cusolverDnDsyevd_bufferSize(c->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
-                                             c->d_eig_a.p, n, c->d_eig_w.p, &lwork));
-    c->d_eig_work.ensure((size_t)std::max(lwork, 1));
-    SOLVER_CHECK(cusolverDnDsyevd(c->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, c->d_eig_a.p, n,
-                                  c->d_eig_w.p, c->d_eig_work.p, lwork, c->d_eig_info.p));
-    std::vector<double> vc((size_t)n * n);
+    if (!launch_sym_eigen(n, c->d_eig_a.p, c->d_eig_work.p, c->d_eig_w.p, c->d_eig_v.p, c->d_eig_info.p, st))
+      fail(FLOSIC_ERR_CAPACITY, "LOWSIC: more FOs per spin than the eigen-solver holds");
+    c->launches++;
+    CUDA_CHECK(cudaGetLastError());
+    v.resize((size_t)n * n);
     w.resize(n);
     int info = 0;
-    CUDA_CHECK(cudaMemcpyAsync(vc.data(), c->d_eig_a.p, sizeof(double) * vc.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaMemcpyAsync(v.data(), c->d_eig_v.p, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, st));
     CUDA_CHECK(cudaMemcpyAsync(w.data(), c->d_eig_w.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     CUDA_CHECK(cudaMemcpyAsync(&info, c->d_eig_info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_CHECK(cudaStreamSynchronize(st));
-    if (info != 0) fail(FLOSIC_ERR_LOWDEN, "LOWSIC: eigen-decomposition of the FO overlap failed (syevd info " +
-                                               std::to_string(info) + ")");
-    v.resize((size_t)n * n);
-    for (int m = 0; m < n; ++m)
-      for (int k = 0; k < n; ++k) v[(size_t)k * n + m] = vc[(size_t)m * n + k];  // column m = eigenvector m
+    if (info != 0) fail(FLOSIC_ERR_LOWDEN, "LOWSIC: eigen-decomposition of the FO overlap did not converge");
   };
 }
 
@@ -656,19 +648,12 @@ void fo_setup(flosic_ctx* c, int s) {
   for (int k = 0; k < nf; ++k)
     for (int d = 0; d < 3; ++d) pts[(size_t)d * nf + k] = c->fods[s][3 * k + d];
   c->d_fodpts.upload(pts.data(), pts.size(), st);
-  c->d_basis.ensure((size_t)4 * nb * nf);
-  launch_basis_values(c->basis_dev(), 1, nf, c->d_fodpts.p, c->d_fodpts.p + nf, c->d_fodpts.p + 2 * nf,
-                      c->d_basis.p, nf, st);
-  c->launches++;
   c->d_psig.ensure((size_t)4 * nf * nw);
-  const double one = 1.0, zero = 0.0;
   const double* cthr = c->d_psi_thr.p + (size_t)s * c->nwfs[0] * nb;
-  for (int ch = 0; ch < 4; ++ch) {
-    // PSIG_ch (nf x nw) = B_ch^T (nf x nb) * C (nb x nw)
-    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nf, nw, nb, &one, c->d_basis.p + (size_t)ch * nb * nf,
-                           nf, cthr, nb, &zero, c->d_psig.p + (size_t)ch * nf * nw, nf));
-    c->launches++;
-  }
+  // PSIG_ch (nf x nw) = B_ch (FODs x nb) * C (nb x nw), basis values formed in the kernel
+  launch_fo_values(c->basis_dev(), 1, nf, c->d_fodpts.p, c->d_fodpts.p + nf, c->d_fodpts.p + 2 * nf, cthr, nb, nw,
+                   c->d_psig.p, nf, st);
+  c->launches++;
   std::vector<double> psig((size_t)4 * nf * nw);
   CUDA_CHECK(cudaMemcpyAsync(psig.data(), c->d_psig.p, sizeof(double) * psig.size(), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
@@ -713,9 +698,7 @@ void fo_setup(flosic_ctx* c, int s) {
   c->d_tmat.upload(S.tmat.data(), S.tmat.size(), st);
   S.cfo.ensure((size_t)nb * nf);
   const double* cks = c->d_psi.p + (size_t)s * c->nwfs[0] * nb;
-  BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nf, nw, &one, cks, nb, c->d_tmat.p, nw, &zero,
-                         S.cfo.p, nb));
-  c->launches++;
+  gemm(c, false, false, nb, nf, nw, 1.0, cks, nb, c->d_tmat.p, nw, 0.0, S.cfo.p, nb);
   S.fo_valid = true;
 }
 
@@ -726,24 +709,11 @@ void fo_values(flosic_ctx* c, int s) {
   const int nch = c->nch();
   const int nderv = c->nderv();
   S.phi.ensure((size_t)nch * nf * P);
-  const size_t budget = (size_t)3 << 30;  // bytes of basis scratch
-  int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nch * nb)));
-  chunk = std::max(TILE, chunk / TILE * TILE);
-  c->d_basis.ensure((size_t)nch * nb * chunk);
-  const double one = 1.0, zero = 0.0;
-  for (int p0 = 0; p0 < P; p0 += chunk) {
-    const int np = std::min(chunk, P - p0);
-    const size_t q0 = (size_t)c->eval_p0 + p0;
-    launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
-                        c->st);
-    c->launches++;
-    for (int ch = 0; ch < nch; ++ch) {
-      BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, np, nf, nb, &one,
-                             c->d_basis.p + (size_t)ch * nb * np, np, S.cfo.p, nb, &zero,
-                             S.phi.p + (size_t)ch * nf * P + p0, P));
-      c->launches++;
-    }
-  }
+  // Phi_ch (P x nf) = B_ch (P x nb) C_FO, basis values formed in shared memory
+  const size_t q0 = (size_t)c->eval_p0;
+  launch_fo_values(c->basis_dev(), nderv, P, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, S.cfo.p, nb, nf, S.phi.p,
+                   P, c->st);
+  c->launches++;
 }
 
 // Pair coefficients, POISSON1 call set-up and the Coulomb kernels for nf
@@ -909,13 +879,10 @@ void spin_sic(flosic_ctx* c, int s) {
   cudaStream_t st = c->st;
   CUDA_CHECK(cudaEventRecord(c->ev[0], st));
   c->d_sic.ensure((size_t)nf * nf);
-  const double mone = -1.0, zero = 0.0, one = 1.0;
   const int nyc = c->mgga ? 4 : 1;
-  for (int ch = 0; ch < nyc; ++ch) {
-    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nf, nf, P, &mone, S.phi.p + (size_t)ch * nf * P, P,
-                           S.y.p + (size_t)ch * nf * P, P, ch == 0 ? &zero : &one, c->d_sic.p, nf));
-    c->launches++;
-  }
+  for (int ch = 0; ch < nyc; ++ch)
+    gemm(c, true, false, nf, nf, P, -1.0, S.phi.p + (size_t)ch * nf * P, P, S.y.p + (size_t)ch * nf * P, P,
+         ch == 0 ? 0.0 : 1.0, c->d_sic.p, nf);
   S.sic.resize((size_t)nf * nf);
   CUDA_CHECK(cudaMemcpyAsync(S.sic.data(), c->d_sic.p, sizeof(double) * nf * nf, cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaEventRecord(c->ev[1], st));
@@ -1034,7 +1001,9 @@ constexpr int XC_SCRATCH_POINTS = XC_SCRATCH_BLOCKS * 256;
 static __device__ __align__(256) double g_xc_scratch[(XC_SCRATCH_BLOCKS + 1) * NPART];
 
 // Device address of g_xc_scratch for the current device, looked up once per
-// device by the first call (cudaGetSymbolAddress with that device current).
+// device with that device current.  flosic_sic_create calls it, so the module
+// that holds the array is loaded (and the array placed in device memory) when
+// the first context on a device is made, not inside the entry point.
 double* xc_scratch_address(int device) {
   static std::mutex mu;
   static double* addr[64] = {};
@@ -1048,6 +1017,93 @@ double* xc_scratch_address(int device) {
     addr[device] = ptr;
   }
   return addr[device];
+}
+
+// dE_SIC/dC_FO (nb x nf, column k = FO k) of spin s on the device, summed over
+// this context's points: -(4/NSPN) sum_c sum_p chi_c,mu(p) Y_c,k(p).  E_SIC =
+// (2/NSPN) sum_k XENG_k and dXENG_k/dphi_k(p) = -2 w V_k phi_k (+ the meta-GGA
+// gradient terms, carried by Y_1..3).  The basis values are recomputed in mesh
+// chunks, so no per-FO array beyond the cycle's is kept.
+void adjoint_device(flosic_ctx* c, int s, DevBuf<double>& dg) {
+  spin_potentials(c, s);
+  SpinCache& S = c->spin[s];
+  const int nf = S.nf, nb = c->nbasis, P = c->eval_n;
+  const int nyc = c->mgga ? 4 : 1;
+  const int nderv = c->mgga ? 1 : 0;
+  const size_t budget = (size_t)3 << 30;
+  int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nyc * nb)));
+  chunk = std::max(TILE, chunk / TILE * TILE);
+  c->d_basis.ensure((size_t)nyc * nb * chunk);
+  dg.ensure((size_t)nb * nf);
+  const double alpha = -4.0 / c->nspn;
+  bool first = true;
+  for (int p0 = 0; p0 < P; p0 += chunk) {
+    const int np = std::min(chunk, P - p0);
+    const size_t q0 = (size_t)c->eval_p0 + p0;
+    launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
+                        c->st);
+    c->launches++;
+    for (int ch = 0; ch < nyc; ++ch) {
+      gemm(c, true, false, nb, nf, np, alpha, c->d_basis.p + (size_t)ch * nb * np, np,
+           S.y.p + (size_t)ch * nf * P + p0, P, first ? 0.0 : 1.0, dg.p, nb);
+      first = false;
+    }
+  }
+}
+
+// dE_SIC/dFOD of spin s, grad[k*3 + d], from the adjoint G by the chain rule
+// through the FO construction.  C_FO = U C_KS with U = S^-1/2 T the
+// Lowdin-orthonormalised Fermi transformation (frmiorb.f:351-480), T_kj =
+// psi_j(a_k)/sqrt(rho(a_k)) = FMAT(j,k,1), S = T T^T = V diag(q) V^T (the
+// eigenpairs LOWSIC kept); row k of T depends on FOD a_k only, with
+// derivatives FMAT(.,k,2:4) (frmorb2.F:296-346).  With M = C_KS G and A = T M:
+//   W = V ((V^T A V) o F) V^T,  F_ab = -1 / (sqrt q_a sqrt q_b (sqrt q_a + sqrt q_b)),
+//   dE/dT = (W + W^T) T + (M S^-1/2)^T,  dE/da_m = sum_j (dE/dT)_mj dT_mj/da_m.
+// This is the reference's FOD force (frmorb2.F:586-717, times 2/NSPN) reached
+// through the basis-space adjoint instead of the SIC matrix.
+void fod_gradient(flosic_ctx* c, int s, double* grad) {
+  DevBuf<double> dg, dm;
+  adjoint_device(c, s, dg);
+  SpinCache& S = c->spin[s];
+  const int n = S.nf, nw = S.nw, nb = c->nbasis;
+  if (n != nw) fail(FLOSIC_ERR_NFRM, "FRMIORB: MORB .NE. NFRM");
+  const double* cks = c->d_psi.p + (size_t)s * c->nwfs[0] * nb;
+  dm.ensure((size_t)nw * n);
+  gemm(c, true, false, nw, n, nb, 1.0, cks, nb, dg.p, nb, 0.0, dm.p, nw);  // M(j,k) = sum_mu C_KS(mu,j) G(mu,k)
+  std::vector<double> mh((size_t)nw * n);
+  CUDA_CHECK(cudaMemcpyAsync(mh.data(), dm.p, sizeof(double) * mh.size(), cudaMemcpyDeviceToHost, c->st));
+  CUDA_CHECK(cudaStreamSynchronize(c->st));
+  const size_t nn = (size_t)n * n;
+  std::vector<double> T(nn), M(nn), V(nn), Vt(nn), rq(n), A(nn), B(nn), X(nn), W(nn), Sm(nn), MS(nn), D(nn);
+  for (int a = 0; a < n; ++a)
+    for (int j = 0; j < n; ++j) {
+      T[(size_t)a * n + j] = S.fmat[(size_t)a * nw + j];
+      M[(size_t)j * n + a] = mh[(size_t)a * nw + j];
+      V[(size_t)a * n + j] = S.filo[(size_t)a * n + j];
+      Vt[(size_t)j * n + a] = S.filo[(size_t)a * n + j];
+    }
+  for (int a = 0; a < n; ++a) rq[a] = std::sqrt(S.lam[a]);
+  mat_mul(T.data(), M.data(), A.data(), n, n, n);    // A = T M
+  mat_mul(Vt.data(), A.data(), X.data(), n, n, n);   // V^T A
+  mat_mul(X.data(), V.data(), B.data(), n, n, n);    // V^T A V
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) B[(size_t)a * n + b] *= -1.0 / (rq[a] * rq[b] * (rq[a] + rq[b]));
+  mat_mul(V.data(), B.data(), X.data(), n, n, n);
+  mat_mul(X.data(), Vt.data(), W.data(), n, n, n);   // W = V (B o F) V^T
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) X[(size_t)a * n + b] = V[(size_t)a * n + b] / rq[b];
+  mat_mul(X.data(), Vt.data(), Sm.data(), n, n, n);  // S^-1/2
+  mat_mul(M.data(), Sm.data(), MS.data(), n, n, n);  // M S^-1/2
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) X[(size_t)a * n + b] = W[(size_t)a * n + b] + W[(size_t)b * n + a];
+  mat_mul(X.data(), T.data(), D.data(), n, n, n);    // (W + W^T) T
+  for (int m = 0; m < n; ++m)
+    for (int d = 0; d < 3; ++d) {
+      double acc = 0.0;
+      for (int j = 0; j < n; ++j)
+        acc += (D[(size_t)m * n + j] + MS[(size_t)j * n + m]) * S.fmat[((size_t)(1 + d) * n + m) * nw + j];
+      grad[(size_t)m * 3 + d] = acc;
+    }
 }
 
 }  // namespace
@@ -1075,20 +1131,6 @@ int flosic_sic_create(int device, flosic_ctx** out) {
       c->coulomb_cfg.perfo_wm = (wm == 1 || wm == 2 || wm == 4) ? wm : 0;
     }
     CUDA_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
-    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) {
-      cudaStreamDestroy(c->st);
-      delete c;
-      fail(FLOSIC_ERR_CUDA, "cusolverDnCreate failed");
-    }
-    cusolverDnSetStream(c->solver, c->st);
-    if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
-      cusolverDnDestroy(c->solver);
-      cudaStreamDestroy(c->st);
-      delete c;
-      fail(FLOSIC_ERR_CUDA, "cublasCreate failed");
-    }
-    cublasSetStream(c->blas, c->st);
-    cublasSetMathMode(c->blas, CUBLAS_PEDANTIC_MATH);
     for (auto& e : c->ev) CUDA_CHECK(cudaEventCreate(&e));
     std::vector<double> ang, w;
     lebedev19(ang, w);
@@ -1096,6 +1138,10 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     init_call_setup();
     init_coulomb_mma();
     init_coulomb_tc();
+    CUDA_CHECK(init_sym_eigen());
+    CUDA_CHECK(init_contract());
+    CUDA_CHECK(preload_xc_rhog());
+    xc_scratch_address(device);
     std::vector<double> bt = boys_table();
     c->d_boys.upload(bt.data(), bt.size(), c->st);
     CUDA_CHECK(cudaStreamSynchronize(c->st));
@@ -1119,10 +1165,9 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_coef.release(); c->d_cgp.release(); c->d_mom.release(); c->d_part.release(); c->d_sums.release();
   c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
   c->d_share.release(); c->d_lists.release(); c->d_setup_list.release();
-  c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_work.release(); c->d_eig_info.release();
+  c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_v.release(); c->d_eig_work.release(); c->d_eig_info.release();
   c->d_coef_hl.release(); c->d_momv_hl.release(); c->d_tc_err.release();
-  if (c->blas) cublasDestroy(c->blas);
-  if (c->solver) cusolverDnDestroy(c->solver);
+  c->d_gemm_ws.release();
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return FLOSIC_OK;
@@ -1505,6 +1550,13 @@ int flosic_sic_getvlxc_mgga(flosic_ctx* c, int ndim, const double* rhog, const d
   });
 }
 
+int flosic_sic_set_wait_limit(flosic_ctx* c, int64_t polls) {
+  return guarded([&] {
+    if (!c) fail(FLOSIC_ERR_ARG, "null context");
+    c->coulomb_cfg.wait_limit = polls > 0 ? (long long)polls : 0;
+  });
+}
+
 int flosic_sic_set_precision(flosic_ctx* c, int mode) {
   return guarded([&] {
     if (!c) fail(FLOSIC_ERR_ARG, "null context");
@@ -1595,7 +1647,7 @@ int flosic_sic_getvlxc_device(flosic_ctx* c, int npts, const double* d_rhog, int
                                     "-point capacity of the allocation-free GETVLXC scratch");
     double* part = xc_scratch_address(c->device);
     double* sums = part + (size_t)XC_SCRATCH_BLOCKS * NPART;
-    const int nblk = (npts + 255) / 256;
+    const int nblk = std::min(1024, (npts + 255) / 256);  // k_xc_rhog strides over the rest
     MeshDev M{};
     M.n = npts;
     M.w = d_wmsh;
@@ -1742,39 +1794,29 @@ int flosic_sic_adjoint(flosic_ctx* c, int lspn, double* g, int ldg) {
     if (!g) fail(FLOSIC_ERR_ARG, "null array argument");
     if (ldg < c->nbasis) fail(FLOSIC_ERR_ARG, "ldg smaller than the number of basis functions");
     const int s = lspn - 1;
-    spin_potentials(c, s);
-    SpinCache& S = c->spin[s];
-    const int nf = S.nf, nb = c->nbasis, P = c->eval_n;
-    // dE_SIC/dC[mu][k] = -(4/NSPN) sum_c sum_p chi_c,mu(p) Y_c,k(p): E_SIC = (2/NSPN) sum_k XENG_k and
-    // dXENG_k/dphi_k(p) = -2 w V_k phi_k (+ the meta-GGA gradient terms, carried by Y_1..3)
-    const int nyc = c->mgga ? 4 : 1;
-    const int nderv = c->mgga ? 1 : 0;
-    const size_t budget = (size_t)3 << 30;
-    int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * nyc * nb)));
-    chunk = std::max(TILE, chunk / TILE * TILE);
-    c->d_basis.ensure((size_t)nyc * nb * chunk);
     DevBuf<double> dg;
-    dg.ensure((size_t)nb * nf);
-    const double alpha = -4.0 / c->nspn, zero = 0.0, one = 1.0;
-    bool first = true;
-    for (int p0 = 0; p0 < P; p0 += chunk) {
-      const int np = std::min(chunk, P - p0);
-      const size_t q0 = (size_t)c->eval_p0 + p0;
-      launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
-                          c->st);
-      for (int ch = 0; ch < nyc; ++ch) {
-        BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &alpha,
-                               c->d_basis.p + (size_t)ch * nb * np, np, S.y.p + (size_t)ch * nf * P + p0, P,
-                               first ? &zero : &one, dg.p, nb));
-        first = false;
-      }
-    }
+    adjoint_device(c, s, dg);
+    const int nf = c->spin[s].nf, nb = c->nbasis;
     std::vector<double> h((size_t)nb * nf);
     CUDA_CHECK(cudaMemcpyAsync(h.data(), dg.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
     CUDA_CHECK(cudaStreamSynchronize(c->st));
     dg.release();
     for (int k = 0; k < nf; ++k)
       for (int mu = 0; mu < nb; ++mu) g[(size_t)k * ldg + mu] = h[(size_t)k * nb + mu];
+  });
+}
+
+int flosic_sic_adjoint_fod(flosic_ctx* c, int lspn, double* grad, int ld) {
+  return guarded([&] {
+    require(c, true);
+    require_whole_mesh(c);
+    if (lspn < 1 || lspn > c->nspn) fail(FLOSIC_ERR_ARG, "LSPN out of range");
+    if (!grad) fail(FLOSIC_ERR_ARG, "null array argument");
+    const int s = lspn - 1;
+    if (ld < std::max(1, c->nfrm[s])) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+    std::fill(grad, grad + (size_t)3 * ld, 0.0);
+    if (c->nfrm[s] == 0) return;
+    fod_gradient(c, s, grad);
   });
 }
 
@@ -1801,7 +1843,6 @@ int flosic_sic_siclag_der(flosic_ctx* c, double* dersic, int ldo) {
       // H_ix = B_{1+ix}^T Y_0 (+ sum_c B_{h(ix,c)}^T Y_{1+c}), nb x nf each
       DevBuf<double> dh;
       dh.ensure((size_t)3 * nb * nf);
-      const double one = 1.0, zero = 0.0;
       bool first = true;
       for (int p0 = 0; p0 < P; p0 += chunk) {
         const int np = std::min(chunk, P - p0);
@@ -1813,10 +1854,8 @@ int flosic_sic_siclag_der(flosic_ctx* c, double* dersic, int ldo) {
           const int nterm = c->mgga ? 4 : 1;
           for (int t = 0; t < nterm; ++t) {
             const int bch = t == 0 ? 1 + ix : hch[ix][t - 1];
-            BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &one,
-                                   c->d_basis.p + (size_t)bch * nb * np, np, S.y.p + (size_t)t * nf * P + p0, P,
-                                   (first && t == 0) ? &zero : &one, dh.p + (size_t)ix * nb * nf, nb));
-            c->launches++;
+            gemm(c, true, false, nb, nf, np, 1.0, c->d_basis.p + (size_t)bch * nb * np, np,
+                 S.y.p + (size_t)t * nf * P + p0, P, (first && t == 0) ? 0.0 : 1.0, dh.p + (size_t)ix * nb * nf, nb);
           }
         }
         first = false;
@@ -1866,33 +1905,29 @@ int flosic_sic_sicham(flosic_ctx* c, int lspn, double* ham, int ldh, int packed)
     chunk = std::max(TILE, chunk / TILE * TILE);
     c->d_basis.ensure((size_t)nyc * nb * chunk);
     c->d_tmp.ensure((size_t)nf * P);
-    BLAS_CHECK(cublasDdgmm(c->blas, CUBLAS_SIDE_LEFT, P, nf, S.phi.p, P, c->d_w.p + c->eval_p0, 1, c->d_tmp.p, P));
+    launch_scale_rows(P, nf, S.phi.p, P, c->d_w.p + c->eval_p0, c->d_tmp.p, P, c->st);
+    c->launches++;
     DevBuf<double> dab, dh;
     dab.ensure((size_t)2 * nb * nf);
     dh.ensure((size_t)nb * nb);
     double* da = dab.p;
     double* db = dab.p + (size_t)nb * nf;
-    const double zero = 0.0, one = 1.0, mhalf = -0.5;
     for (int p0 = 0; p0 < P; p0 += chunk) {
       const int np = std::min(chunk, P - p0);
       const size_t q0 = (size_t)c->eval_p0 + p0;
       launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, c->d_basis.p, np,
                           c->st);
       c->launches++;
-      const double* beta = p0 == 0 ? &zero : &one;
+      const double beta = p0 == 0 ? 0.0 : 1.0;
       for (int ch = 0; ch < nyc; ++ch)
-        BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &one,
-                               c->d_basis.p + (size_t)ch * nb * np, np, S.y.p + (size_t)ch * nf * P + p0, P,
-                               ch == 0 ? beta : &one, da, nb));
-      BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nf, np, &one, c->d_basis.p, np,
-                             c->d_tmp.p + p0, P, beta, db, nb));
-      c->launches += nyc + 1;
+        gemm(c, true, false, nb, nf, np, 1.0, c->d_basis.p + (size_t)ch * nb * np, np,
+             S.y.p + (size_t)ch * nf * P + p0, P, ch == 0 ? beta : 1.0, da, nb);
+      gemm(c, true, false, nb, nf, np, 1.0, c->d_basis.p, np, c->d_tmp.p + p0, P, beta, db, nb);
     }
     // APATCH: HSTOR += (HAM + HAM^T)/2 with HAM(j,i) = BASPHI(i,2) BASPHI(j,1), summed
     // over the spin's FOs: H = -(a b^T + b a^T)/2
-    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, nf, &mhalf, da, nb, db, nb, &zero, dh.p, nb));
-    BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, nf, &mhalf, db, nb, da, nb, &one, dh.p, nb));
-    c->launches += 2;
+    gemm(c, false, true, nb, nb, nf, -0.5, da, nb, db, nb, 0.0, dh.p, nb);
+    gemm(c, false, true, nb, nb, nf, -0.5, db, nb, da, nb, 1.0, dh.p, nb);
     std::vector<double> h((size_t)nb * nb);
     CUDA_CHECK(cudaMemcpyAsync(h.data(), dh.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
     CUDA_CHECK(cudaStreamSynchronize(c->st));
@@ -1922,25 +1957,18 @@ int flosic_sic_densold(flosic_ctx* c, int ngrad, double* rhog, double* phig) {
     const size_t budget = (size_t)3 << 30;
     int chunk = (int)std::min<size_t>(P, std::max<size_t>(TILE, budget / (sizeof(double) * ngrad * (nb + nwf))));
     chunk = std::max(TILE, chunk / TILE * TILE);
-    c->d_basis.ensure((size_t)ngrad * nb * chunk);
     DevBuf<double> dv, dr, dph;
     dv.ensure((size_t)ngrad * std::max(nwf, 1) * chunk);
     dr.ensure((size_t)ns * ngrad * P);
     if (phig) dph.ensure((size_t)ns * P);
-    const double one = 1.0, zero = 0.0;
     for (int p0 = 0; p0 < P; p0 += chunk) {
       const int np = std::min(chunk, P - p0);
-      launch_basis_values(c->basis_dev(), nderv, np, c->d_x.p + p0, c->d_y.p + p0, c->d_z.p + p0, c->d_basis.p, np,
-                          c->st);
-      c->launches++;
       // PSIG (densold.F:160-185): coefficients at or below 1e-10 are skipped, as in d_psi_thr
-      if (nwf > 0)
-        for (int ch = 0; ch < ngrad; ++ch) {
-          BLAS_CHECK(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, np, nwf, nb, &one,
-                                 c->d_basis.p + (size_t)ch * nb * np, np, c->d_psi_thr.p, nb, &zero,
-                                 dv.p + (size_t)ch * nwf * np, np));
-          c->launches++;
-        }
+      if (nwf > 0) {
+        launch_fo_values(c->basis_dev(), nderv, np, c->d_x.p + p0, c->d_y.p + p0, c->d_z.p + p0, c->d_psi_thr.p, nb,
+                         nwf, dv.p, np, c->st);
+        c->launches++;
+      }
       launch_densold(np, nw0, nw1, ns, ngrad, dv.p, np, dr.p + p0, phig ? dph.p + p0 : nullptr, P, c->st);
       c->launches++;
     }

@@ -5,9 +5,10 @@ fully contracted s/p/d functions and their coefficients COEF.  The seeded
 workloads (publicrelease_2020_b200/workloads.py) build the reference's
 default basis from these tables with the supplement rule of flosic/sallbas.f.
 
-Run in a checkout next to the reference tree (reads it once, as data):
+Run once with the path of a reference checkout (the directory that holds
+flosic/bdallbas.f), which it reads as data:
 
-    python publicrelease_2020_b200/data/make_nrlmol_default_basis.py /root/reference
+    python publicrelease_2020_b200/data/make_nrlmol_default_basis.py <reference checkout>
 """
 import os
 import re
@@ -50,7 +51,9 @@ def parse(path):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_nrlmol_default_basis.py <reference checkout holding flosic/bdallbas.f>")
+    ref = sys.argv[1]
     tables = parse(os.path.join(ref, "flosic", "bdallbas.f"))
     arrays = {}
     for z, (nspd, alph, coef) in tables.items():

@@ -37,7 +37,7 @@ EXPORTS = [
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
     "flosic_sic_siclag_der", "flosic_sic_sicham", "flosic_sic_densold", "flosic_sic_coupot1",
-    "flosic_sic_autotune",
+    "flosic_sic_autotune", "flosic_sic_adjoint_fod", "flosic_sic_set_wait_limit",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -71,6 +71,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_getvlxc.argtypes = [_vp, C.c_int, _dp, _dp, _dp]
     L.flosic_sic_getvlxc_mgga.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
+    L.flosic_sic_set_wait_limit.argtypes = [_vp, C.c_int64]
     L.flosic_sic_autotune.argtypes = [_vp, C.c_int, _ip, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")]
     L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
     L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
@@ -80,6 +81,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_stats.argtypes = [_vp, _i64, _dp, _i64, _i64, _i64]
     L.flosic_sic_set_shard.argtypes = [_vp, C.c_int, C.c_int]
     L.flosic_sic_adjoint.argtypes = [_vp, C.c_int, _dp, C.c_int]
+    L.flosic_sic_adjoint_fod.argtypes = [_vp, C.c_int, _dp, C.c_int]
     L.flosic_sic_mgga_mixin.argtypes = [_vp, C.c_int, C.c_int, _dp]
     L.flosic_sic_siclag_der.argtypes = [_vp, _dp, C.c_int]
     L.flosic_sic_sicham.argtypes = [_vp, C.c_int, _dp, C.c_int, C.c_int]
@@ -140,6 +142,7 @@ class FlosicSIC:
         self._check(self.L.flosic_sic_set_orbitals(self.h, np.array(list(nwfs) + [0] * (2 - len(nwfs)), dtype=np.int32),
                                                    psi, psi.shape[1], nf, bfrm, self.ld))
         self.nfrm = tuple(int(x) for x in nf)
+        self._adjoint_fods = None  # FODs set through publicrelease_2020_b200.adjoint, if any
 
     # -- reference routines ------------------------------------------------
     def gorbdrv(self, nderv, pts, ifnct):
@@ -192,6 +195,11 @@ class FlosicSIC:
     def set_precision(self, mode):
         """"fp64" (the drop-in, default) or "mixed"."""
         self._check(self.L.flosic_sic_set_precision(self.h, PRECISION[mode]))
+
+    def set_wait_limit(self, polls):
+        """Poll limit of the mixed-precision tensor-core kernel's pipeline waits
+        (<= 0: the default)."""
+        self._check(self.L.flosic_sic_set_wait_limit(self.h, int(polls)))
 
     def autotune(self, reps=2):
         """Time the per-FO Coulomb kernel's FO-slot widths (32, 64, 128) on this
@@ -254,6 +262,14 @@ class FlosicSIC:
         g = np.zeros(nb * self.nfrm[lspn - 1])
         self._check(self.L.flosic_sic_adjoint(self.h, lspn, g, nb))
         return g.reshape(self.nfrm[lspn - 1], nb).T
+
+    def adjoint_fod(self, lspn):
+        """dE_SIC/dFOD (nfrm, 3) of spin lspn from the adjoint, chain rule in the
+        library (flosic_sic_adjoint_fod)."""
+        n = self.nfrm[lspn - 1]
+        g = np.zeros(3 * max(n, 1))
+        self._check(self.L.flosic_sic_adjoint_fod(self.h, lspn, g, max(n, 1)))
+        return g.reshape(-1, 3)[:n]
 
     def siclag_der(self):
         """DERSIC (natoms, nfrm(1)+nfrm(2), 3): the basis-centre SIC force terms

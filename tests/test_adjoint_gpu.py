@@ -1,9 +1,11 @@
 """Basis-space adjoint G = dE_SIC/dC_FO (flosic_sic_adjoint) and the FOD
-gradient built on it (publicrelease_2020_b200.adjoint), through the C ABI.
+gradient built on it inside the library (flosic_sic_adjoint_fod, used by
+publicrelease_2020_b200.adjoint), through the C ABI.
 
 Checks: (1) C_FO^T G = (4/NSPN) SIC, the FO-space projection of the adjoint
 is the SIC matrix (rounding level); (2) the FOD gradient from G through the
-Lowdin chain rule equals the reference's FOD force formula (frmorb2.F,
+Lowdin chain rule (in the library, and restated here in numpy) equals the
+reference's FOD force formula (frmorb2.F,
 computed by the library from the SIC matrix), times 2/NSPN: DEBDAX is the
 force on one spin's FODs, and with NSPN=1 they stand for both spins in E_SIC;
 (3) on benzene (C3) the torch.autograd.Function returns that gradient, and
@@ -54,13 +56,37 @@ def test_adjoint_projects_to_sic_matrix(case):
         assert np.max(np.abs(proj - 4.0 / sysm.nspn * lam)) <= 1e-10 * np.abs(lam).max(), name
 
 
+def _chain_rule_numpy(ctx, psi, nwfs):
+    """The chain rule of flosic_sic_adjoint_fod restated in numpy from the
+    adjoint G and FMAT returned through the C ABI (independent eigen-solver)."""
+    fm = ctx.frmorb2_fmat()                       # [s][K][jfm][jwf]
+    out = np.zeros((ctx.sysm.nspn, ctx.ld, 3))
+    for s in range(ctx.sysm.nspn):
+        n = ctx.nfrm[s]
+        G = ctx.adjoint(s + 1)                    # (nbasis, n)
+        cks = np.asarray(psi)[s * nwfs[0]: s * nwfs[0] + n]
+        M = cks @ G
+        T = fm[s, 0, :n, :n]
+        q, V = np.linalg.eigh(T @ T.T)
+        rq = np.sqrt(q)
+        Sm = (V / rq) @ V.T
+        F = -1.0 / (rq[:, None] * rq[None, :] * (rq[:, None] + rq[None, :]))
+        W = V @ ((V.T @ (T @ M) @ V) * F) @ V.T
+        dEdT = (W + W.T) @ T + (M @ Sm).T
+        for d in range(3):
+            out[s, :n, d] = np.einsum("mj,mj->m", dEdT, fm[s, 1 + d, :n, :n])
+    return out
+
+
 def test_adjoint_fod_gradient_equals_reference_force(case):
     name, sysm, ctx, r = case
-    g = fod_gradient(ctx, sysm.psi, sysm.nwfs)
+    g = fod_gradient(ctx)
+    gn = _chain_rule_numpy(ctx, sysm.psi, sysm.nwfs)
     for s in range(sysm.nspn):
         n = sysm.nfrm[s]
         ref = (2.0 / sysm.nspn) * r["debdax"][s][:n]
         assert np.max(np.abs(g[s, :n] - ref)) <= 1e-8 * max(1.0, np.abs(ref).max()), (name, g[s, :n], ref)
+        assert np.max(np.abs(g[s, :n] - gn[s, :n])) <= 1e-10 * max(1.0, np.abs(ref).max()), name
 
 
 def test_autograd_benzene_gradient_and_finite_differences():

@@ -92,6 +92,8 @@ def _stub_source(sigs):
         for t, v in params:
             if t == "int":
                 body.append(f'  snprintf(b, sizeof b, " {v}=%d", {v}); rec(b);')
+            elif t == "int64_t":
+                body.append(f'  snprintf(b, sizeof b, " {v}=%lld", (long long){v}); rec(b);')
             elif t == "flosic_ctx**":
                 body.append(f'  *{v} = (flosic_ctx*)0xabc0; snprintf(b, sizeof b, " {v}=set"); rec(b);')
             else:
@@ -127,6 +129,11 @@ def test_f77_forms_forward_to_the_c_entry_points(stub):
                 expect.append(f"{v}={hex(h.value)}")
             elif t == "int":
                 x = C.c_int32(7 * i + j - 3)
+                keep.append(x)
+                args.append(C.byref(x))
+                expect.append(f"{v}={x.value}")
+            elif t == "int64_t":
+                x = C.c_int64(1000003 * i + j)
                 keep.append(x)
                 args.append(C.byref(x))
                 expect.append(f"{v}={x.value}")

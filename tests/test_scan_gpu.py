@@ -69,7 +69,20 @@ def test_scan_getvlxc_matches_oracle(pair):
         m = r0 > 1e-6 * r0.max()
         # measured: <= 1e-9 of max|V| pointwise (differences of nearly equal terms in d alpha / d rho)
         assert np.max(np.abs(vg[0] - vo[0])[m]) <= 1e-8 * np.abs(vo[0][m]).max(), (name, k)
-        assert np.sum(np.abs(vg[0] - vo[0]) * r0 * w) <= 1e-10, (name, k)
+        # Density-weighted over all points, the bound is the potential's own
+        # conditioning: how far the oracle's V moves when its inputs move by one
+        # unit in the last place.  The device code, compiled for the host
+        # without multiply-add contraction, equals the oracle to 1e-15 here;
+        # the GPU contracts multiply-adds, which moves the sum by 2.1e-10 on
+        # water FO 2 (one point, rho = 2e-5 max(rho), V = 1.5e5, where
+        # tau - tau_W cancels), 10-100x below this spread for every FO.
+        rng = np.random.default_rng(k)
+        spread = np.zeros(n)
+        for _ in range(4):
+            vp, _, _ = orc.getvlxc_mgga(rho * (1 + 2.0**-52 * rng.uniform(-1, 1, rho.shape)),
+                                        tau * (1 + 2.0**-52 * rng.uniform(-1, 1, tau.shape)))
+            spread = np.maximum(spread, np.abs(vp[0] - vo[0]))
+        assert np.sum(np.abs(vg[0] - vo[0]) * r0 * w) <= np.sum(spread * r0 * w), (name, k)
         for d in range(4):
             scale = np.abs(mo[:, d][m]).max()
             assert np.max(np.abs(mg[:n, d] - mo[:, d])[m]) <= 1e-8 * scale, (name, k, d)

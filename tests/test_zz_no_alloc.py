@@ -5,6 +5,9 @@ The device buffers belong to the caller (torch CUDA tensors here); the entry
 point keeps its block partial sums in a file-scope device array.  Two calls in
 a row must both agree with the allocating path: the scratch is reused without
 being cleared, and every output entry must be written (outputs start as NaN).
+The device's free memory, read before the first call on a new context and
+after each call with torch's allocator idle, must not change: the scratch and
+the kernels' code are placed on the device when the context is created.
 The per-point potential comes from the same XC kernel in both paths, so it
 agrees to rounding; the energies are summed over a different block partition,
 so they agree to 1e-12 relative."""
@@ -40,9 +43,16 @@ def test_getvlxc_device_matches_getvlxc(name):
         r_dev = torch.zeros((10, ldr), dtype=torch.float64, device="cuda")
         r_dev[:, :n] = torch.from_numpy(np.ascontiguousarray(rho))
         w_dev = torch.from_numpy(np.ascontiguousarray(sysm.wmsh, dtype=np.float64)).to("cuda")
+        v_devs = [torch.full((2 * n,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
+        torch.cuda.synchronize()
+        free = [torch.cuda.mem_get_info()[0]]
         for call in range(2):
-            v_dev = torch.full((2 * n,), float("nan"), dtype=torch.float64, device="cuda")
+            v_dev = v_devs[call]
             e = ctx.getvlxc_device(n, r_dev.data_ptr(), ldr, w_dev.data_ptr(), v_dev.data_ptr())
+            torch.cuda.synchronize()
+            free.append(torch.cuda.mem_get_info()[0])
+            # no device memory taken by the call, the first one on this context included
+            assert free[-1] == free[0], (name, call, free)
             v = v_dev.cpu().numpy()
             assert np.all(np.isfinite(v)), (name, call)
             assert np.max(np.abs(v - v_ref)) <= 1e-13 * np.abs(v_ref).max(), (name, call)

@@ -184,6 +184,26 @@ int flosic_sic_frmorb2_force(flosic_ctx* ctx, int lspn, const double* sic, int l
 int flosic_sic_cycle(flosic_ctx* ctx, int ld, double* results, double* sic, double* debdax,
                      double* cfrm, double* esic);
 
+/* One SIC cycle of many molecules (no single reference counterpart: the
+   reference runs one molecule per job and spreads the FOs of one molecule over
+   MPI groups, global_call.F90:113-160).  ctxs[0..n) are contexts on one device
+   in one precision, each with its own geometry, orbitals and FODs.  Every
+   molecule's FO construction, FO values, pair coefficients and call set-up run
+   on its own stream; then the Coulomb potentials of all FOs of all molecules
+   and both spins are evaluated by two persistent launches over one list of
+   (molecule-spin, 128-point tile, block of 32*wm FOs) items (shared-geometry
+   calls, then per-FO calls added); then each molecule's XC, energies, SIC
+   matrix and forces.  wm = 1, 2 or 4 sets the FO block (0: from the largest
+   FO count).  Outputs per molecule m at the offsets of flosic_sic_cycle times
+   m: RESULTS(13,ld,2), SIC(ld,ld,2), DEBDAX(3,ld,2), CFRM(3,ld,2) and
+   esic[m].  Every potential is computed by the same operations in the same
+   order as in flosic_sic_cycle on the shared-geometry tensor-core GEMM
+   (FLOSIC_PRECISION_FP64: bit for bit the per-molecule results; in the mixed
+   mode the shared-geometry calls use the FP32-column FP64 GEMM rather than
+   the tcgen05 kernel). */
+int flosic_sic_batch_cycle(flosic_ctx** ctxs, int n, int wm, int ld, double* results, double* sic,
+                           double* debdax, double* cfrm, double* esic);
+
 /* Adjoint of the SIC energy with respect to the FO coefficients (no single
    reference counterpart: the basis-space form of the SIC-matrix quadrature of
    SICLMSLV, frmorb_mpi.F:184-572).  G(ldg, nfrm) = dE_SIC/dC_FO for the FOs of

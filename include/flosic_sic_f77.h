@@ -72,6 +72,9 @@ void flosic_sic_cycle_(const int64_t* ctx, const int32_t* ld, double* results, d
                        double* cfrm, double* esic, int32_t* ierr);
 void flosic_sic_adjoint_(const int64_t* ctx, const int32_t* lspn, double* g, const int32_t* ldg,
                          int32_t* ierr);
+void flosic_sic_batch_cycle_(const int64_t* ctxs, const int32_t* n, const int32_t* wm, const int32_t* ld,
+                             double* results, double* sic, double* debdax, double* cfrm, double* esic,
+                             int32_t* ierr);
 void flosic_sic_adjoint_fod_(const int64_t* ctx, const int32_t* lspn, double* grad, const int32_t* ld,
                              int32_t* ierr);
 void flosic_sic_siclag_der_(const int64_t* ctx, double* dersic, const int32_t* ldo, int32_t* ierr);

@@ -232,6 +232,7 @@ struct FoValSmem {
   double As[2][FV_KC][S::LDR];     // basis values: k = function, row = channel * BP + point
   double Bs[2][FV_KC][FV_BN + 4];  // coefficients: k = function, column = FO
   double g[S::BP][MAX_BARE];       // exp(-alpha r^2) of the atom's bare primitives
+  double R[S::BP][3 * MAX_CON][NDERV + 1];  // radial sums per contraction (l, c): sum c g (2 alpha)^d
   double rel[S::BP][3];            // point - atom centre
   double px[S::BP], py[S::BP], pz[S::BP];
   int kpad[2];                     // k rows of the stage in each buffer, -1 = end
@@ -248,27 +249,16 @@ __device__ __forceinline__ void fv_bar_arrive(int id, int n) {
 __constant__ int c_fv_pow[10][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0},
                                     {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
 
-// Values (and derivatives) of one contracted Cartesian function at one point:
-// radial sums over the bare primitives (gorbdrv.f:196-230), then the
-// Cartesian factor x^a y^b z^c (a, b, c <= 2) and the product rule, written
-// as NCH channels into column k of As (channel stride bp).
+// Values (and derivatives) of one contracted Cartesian function at one point
+// from its radial sums R0 = sum c g, R1 = sum c g 2 alpha, R2 = sum c g
+// (2 alpha)^2 (gorbdrv.f:196-230): the Cartesian factor x^a y^b z^c
+// (a, b, c <= 2) and the product rule, written as NCH channels into column k
+// of As (channel stride bp).
 template <int NDERV>
-__device__ __forceinline__ void fv_function(const BasisDev& B, int t, int l, int c, int mu, const double* g,
-                                            const double* xyz, double* col, int bp) {
+__device__ __forceinline__ void fv_function(int l, int mu, const double* Rv, const double* xyz, double* col,
+                                            int bp) {
   constexpr int NCH = FoValShape<NDERV>::NCH;
-  const int nbare = B.type_nbare[t];
-  const double* con = B.type_bfcon + ((size_t)(t * 3 + l) * MAX_CON + c) * MAX_BARE;
-  const double* alp = B.type_alpha + t * MAX_BARE;
-  double R0 = 0.0, R1 = 0.0, R2 = 0.0;
-  for (int ib = 0; ib < nbare; ++ib) {
-    const double cg = con[ib] * g[ib];
-    R0 += cg;
-    if (NDERV > 0) {
-      const double a2 = 2.0 * alp[ib];
-      R1 += cg * a2;
-      if (NDERV > 1) R2 += cg * a2 * a2;
-    }
-  }
+  const double R0 = Rv[0], R1 = NDERV > 0 ? Rv[1] : 0.0, R2 = NDERV > 1 ? Rv[2] : 0.0;
   const int shift = (l == 0) ? 0 : (l == 1 ? 1 : 4);
   const int* pw = c_fv_pow[shift + mu];
   const double x = xyz[0], y = xyz[1], z = xyz[2];
@@ -371,10 +361,34 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
         }
       }
       fv_bar_sync(FV_BAR_PROD, FV_PROD);
-      // the atom's functions: l-major, then Cartesian component, then contraction
+      // radial sums of every contraction (l, c) at every point, once per atom
       const int lmax = B.type_lmax[t];
-      int nfa = 0;
-      for (int l = 0; l <= lmax; ++l) nfa += ((l == 0) ? 1 : (l == 1 ? 3 : 6)) * B.type_ncon[t * 3 + l];
+      const int nc0 = B.type_ncon[t * 3], nc1 = lmax >= 1 ? B.type_ncon[t * 3 + 1] : 0;
+      const int nc2 = lmax >= 2 ? B.type_ncon[t * 3 + 2] : 0;
+      const int nlc = nc0 + nc1 + nc2;
+      const double* alp = B.type_alpha + t * MAX_BARE;
+      for (int e = pt; e < S::BP * nlc; e += FV_PROD) {
+        const int lc = e / S::BP, i = e - lc * S::BP;
+        const int l = lc < nc0 ? 0 : (lc < nc0 + nc1 ? 1 : 2);
+        const int c = lc - (l == 0 ? 0 : (l == 1 ? nc0 : nc0 + nc1));
+        const double* con = B.type_bfcon + ((size_t)(t * 3 + l) * MAX_CON + c) * MAX_BARE;
+        double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+        for (int ib = 0; ib < nbare; ++ib) {
+          const double cg = con[ib] * sm.g[i][ib];
+          R0 += cg;
+          if (NDERV > 0) {
+            const double a2 = 2.0 * alp[ib];
+            R1 += cg * a2;
+            if (NDERV > 1) R2 += cg * a2 * a2;
+          }
+        }
+        sm.R[i][lc][0] = R0;
+        if (NDERV > 0) sm.R[i][lc][1] = R1;
+        if (NDERV > 1) sm.R[i][lc][2] = R2;
+      }
+      fv_bar_sync(FV_BAR_PROD, FV_PROD);
+      // the atom's functions: l-major, then Cartesian component, then contraction
+      const int nfa = nc0 + 3 * nc1 + 6 * nc2;
       const int b0 = B.atom_boff[a];
       for (int f0 = 0; f0 < nfa; f0 += FV_KC) {
         const int nfc = min(FV_KC, nfa - f0), kp = (nfc + 3) & ~3;
@@ -388,16 +402,24 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
             for (int ch = 0; ch < S::NCH; ++ch) col[ch * S::BP] = 0.0;
             continue;
           }
-          int f = f0 + fi, l = 0;
-          int ncomp = 1, ncon = B.type_ncon[t * 3];
-          while (f >= ncomp * ncon) {
-            f -= ncomp * ncon;
-            ++l;
-            ncomp = (l == 1) ? 3 : 6;
-            ncon = B.type_ncon[t * 3 + l];
+          int f = f0 + fi, l, lc0, ncon;
+          if (f < nc0) {
+            l = 0;
+            lc0 = 0;
+            ncon = nc0;
+          } else if (f < nc0 + 3 * nc1) {
+            f -= nc0;
+            l = 1;
+            lc0 = nc0;
+            ncon = nc1;
+          } else {
+            f -= nc0 + 3 * nc1;
+            l = 2;
+            lc0 = nc0 + nc1;
+            ncon = nc2;
           }
           const int mu = f / ncon, c = f - mu * ncon;
-          fv_function<NDERV>(B, t, l, c, mu, sm.g[i], sm.rel[i], col, S::BP);
+          fv_function<NDERV>(l, mu, sm.R[i][lc0 + c], sm.rel[i], col, S::BP);
         }
         for (int e = pt; e < kp * FV_BN; e += FV_PROD) {
           const int n = e / kp, fi = e - n * kp;

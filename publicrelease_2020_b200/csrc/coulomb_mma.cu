@@ -252,19 +252,22 @@ struct SharedSmem {
   int rows[2];                  // rows of the stage in each buffer, -1 = end
 };
 
+// One (tile, FO block) of the shared-geometry calls; the body of
+// k_coulomb_shared (one CTA per item) and of k_coulomb_shared_batch
+// (persistent CTAs over the items of many molecules).
 template <int WM, bool MIXED>
-__global__ void __launch_bounds__(WS_THREADS, 1)
-k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __restrict__ share,
-                 const CallInfo* __restrict__ calls, int nfo, const double* __restrict__ coef,
-                 const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
-                 const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
-                 double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
+__device__ __forceinline__ void shared_tile(int tile, int fob, int ncalls, const int* __restrict__ lists,
+                                            const CallShare* __restrict__ share, const CallInfo* __restrict__ calls,
+                                            int nfo, const double* __restrict__ coef,
+                                            const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
+                                            const double* __restrict__ momv, const MeshDev& M,
+                                            const double* __restrict__ boys_tab, double* __restrict__ vh, int ldv,
+                                            unsigned long long* __restrict__ cnt) {
   constexpr int FOB = 32 * WM, WN = CONS_WARPS / WM, WPTS = TILE / WN, NT = WPTS / 8;
   using PT = typename std::conditional<MIXED, float, double>::type;  // producer arithmetic
   extern __shared__ __align__(128) unsigned char smraw[];
   SharedSmem<WM>& S = *reinterpret_cast<SharedSmem<WM>*>(smraw);
-  const int tile = blockIdx.x;
-  const int k0 = blockIdx.y * FOB;
+  const int k0 = fob * FOB;
   const int nk = min(FOB, nfo - k0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int p0 = tile * TILE;
@@ -282,7 +285,7 @@ k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __r
     // ---- producers
     const int pt = tid - NCONS;
     const bool leader = pt == 0;
-    const bool count_terms = blockIdx.y == 0;  // kept terms are summed over all FOs once per (call, point)
+    const bool count_terms = fob == 0;  // kept terms are summed over all FOs once per (call, point)
     SegmentWalker W;
     W.list = lists;
     W.n = lists[2 * ncalls];
@@ -473,13 +476,16 @@ __device__ __forceinline__ void far_points(const T* __restrict__ mv, const doubl
   }
 }
 
+// One (tile, FO block) of the per-FO-geometry calls; the body of
+// k_coulomb_perfo and of k_coulomb_perfo_batch.
 template <int WM, bool MIXED>
-__global__ void __launch_bounds__(WS_THREADS, 1)
-k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
-                const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
-                const int8_t* __restrict__ pair_fmt, const CallFO* __restrict__ cfo,
-                const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
-                double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
+__device__ __forceinline__ void perfo_tile(int tile, int fob, int ncalls, const int* __restrict__ lists,
+                                           int accumulate, const CallInfo* __restrict__ calls,
+                                           const PairGeo* __restrict__ pairs, int nfo,
+                                           const double* __restrict__ coef, const int8_t* __restrict__ pair_fmt,
+                                           const CallFO* __restrict__ cfo, const double* __restrict__ momv,
+                                           const MeshDev& M, const double* __restrict__ boys_tab,
+                                           double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
   constexpr int FOB = 32 * WM, WC = PerFOSmem<WM>::WC, SC = 32 * WC;
   using PT = typename std::conditional<MIXED, float, double>::type;  // producer and far-field arithmetic
   constexpr int WN = CONS_WARPS / WC, WPTS = TILE / WN, NT = WPTS / 8;
@@ -488,8 +494,7 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
   if (accumulate && nl == 0) return;
   extern __shared__ __align__(128) unsigned char smraw[];
   PerFOSmem<WM>& S = *reinterpret_cast<PerFOSmem<WM>*>(smraw);
-  const int tile = blockIdx.x;
-  const int k0 = blockIdx.y * FOB;
+  const int k0 = fob * FOB;
   const int nk = min(FOB, nfo - k0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int p0 = tile * TILE;
@@ -669,6 +674,62 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
   count_add(cnt, my_near, my_far, my_terms);
 }
 
+template <int WM, bool MIXED>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+k_coulomb_shared(int ncalls, const int* __restrict__ lists, const CallShare* __restrict__ share,
+                 const CallInfo* __restrict__ calls, int nfo, const double* __restrict__ coef,
+                 const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
+                 const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
+                 double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
+  shared_tile<WM, MIXED>(blockIdx.x, blockIdx.y, ncalls, lists, share, calls, nfo, coef, pair_fmt, pairs, momv, M,
+                         boys_tab, vh, ldv, cnt);
+}
+
+template <int WM, bool MIXED>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const CallInfo* __restrict__ calls,
+                const PairGeo* __restrict__ pairs, int nfo, const double* __restrict__ coef,
+                const int8_t* __restrict__ pair_fmt, const CallFO* __restrict__ cfo,
+                const double* __restrict__ momv, MeshDev M, const double* __restrict__ boys_tab,
+                double* __restrict__ vh, int ldv, unsigned long long* __restrict__ cnt) {
+  perfo_tile<WM, MIXED>(blockIdx.x, blockIdx.y, ncalls, lists, accumulate, calls, pairs, nfo, coef, pair_fmt, cfo,
+                        momv, M, boys_tab, vh, ldv, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// Many molecules in one launch
+// ---------------------------------------------------------------------------
+// Persistent CTAs (one per SM) walk a list of (job, tile, FO block) items
+// spanning every molecule and spin of a batch, CTA b taking items b, b + grid,
+// ...; a job is one (molecule, spin) with its own calls, coefficients, mesh
+// and output.  Each item is the same work as one CTA of the per-molecule
+// kernels, so every potential is the same bit for bit whichever CTA runs it.
+template <int WM, bool MIXED>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+k_coulomb_shared_batch(const CoulombJob* __restrict__ jobs, const int4* __restrict__ items, int nitems,
+                       const double* __restrict__ boys_tab) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const CoulombJob J = jobs[w.x];
+    shared_tile<WM, MIXED>(w.y, w.z, J.ncalls, J.lists, J.share, J.calls, J.nfo, J.coef, J.pair_fmt, J.pairs,
+                           J.momv, J.M, boys_tab, J.vh, J.ldv, J.cnt);
+    __syncthreads();  // shared memory is reused by the next item
+  }
+}
+
+template <int WM, bool MIXED>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+k_coulomb_perfo_batch(const CoulombJob* __restrict__ jobs, const int4* __restrict__ items, int nitems,
+                      const double* __restrict__ boys_tab) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const CoulombJob J = jobs[w.x];
+    perfo_tile<WM, MIXED>(w.y, w.z, J.ncalls, J.lists, 1, J.calls, J.pairs, J.nfo, J.coef, J.pair_fmt, J.cfo,
+                          J.momv, J.M, boys_tab, J.vh, J.ldv, J.cnt);
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Call classification
 // ---------------------------------------------------------------------------
@@ -768,6 +829,18 @@ static void set_shared_attr() {
 }
 
 template <int WM>
+static void set_batch_attr() {
+  cudaFuncSetAttribute(k_coulomb_shared_batch<WM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(SharedSmem<WM>));
+  cudaFuncSetAttribute(k_coulomb_shared_batch<WM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(SharedSmem<WM>));
+  cudaFuncSetAttribute(k_coulomb_perfo_batch<WM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PerFOSmem<WM>));
+  cudaFuncSetAttribute(k_coulomb_perfo_batch<WM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PerFOSmem<WM>));
+}
+
+template <int WM>
 static void set_perfo_attr() {
   cudaFuncSetAttribute(k_coulomb_perfo<WM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(PerFOSmem<WM>));
@@ -783,6 +856,9 @@ void init_coulomb_mma() {
   set_perfo_attr<1>();
   set_perfo_attr<2>();
   set_perfo_attr<4>();
+  set_batch_attr<1>();
+  set_batch_attr<2>();
+  set_batch_attr<4>();
 }
 
 template <int WM>
@@ -813,14 +889,42 @@ static void launch_perfo(int ncalls, const int* lists, int acc, const CallInfo* 
         ncalls, lists, acc, calls, pairs, nfo, coef, pair_fmt, cfo, momv, M, boys_tab, vh, ldv, cnt);
 }
 
+void launch_coulomb_classify(int ncalls, int npairs, int nfo, const int8_t* maxfmt, const CallFO* cfo,
+                             const CoulombScratch& scr, bool per_fo_only, cudaStream_t st) {
+  if (npairs > 0) k_pair_fmt<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, nfo, maxfmt, scr.pair_fmt);
+  if (ncalls > 0) k_call_share<<<(ncalls + 7) / 8, 256, 0, st>>>(ncalls, nfo, cfo, scr.share);
+  k_call_lists<<<1, LIST_THREADS, 0, st>>>(ncalls, per_fo_only ? 1 : 0, scr.share, scr.lists);
+}
+
+template <int WM>
+static void launch_batch_wm(const CoulombJob* jobs, const int4* items, int nitems, bool mixed,
+                            const double* boys_tab, int nctas, cudaStream_t st) {
+  if (mixed) {
+    k_coulomb_shared_batch<WM, true><<<nctas, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(jobs, items, nitems, boys_tab);
+    k_coulomb_perfo_batch<WM, true><<<nctas, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(jobs, items, nitems, boys_tab);
+  } else {
+    k_coulomb_shared_batch<WM, false><<<nctas, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(jobs, items, nitems,
+                                                                                           boys_tab);
+    k_coulomb_perfo_batch<WM, false><<<nctas, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(jobs, items, nitems,
+                                                                                         boys_tab);
+  }
+}
+
+void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems, int wm, bool mixed,
+                          const double* boys_tab, int nctas, cudaStream_t st) {
+  if (nitems <= 0) return;
+  nctas = std::max(1, std::min(nctas, nitems));
+  if (wm == 4) launch_batch_wm<4>(jobs, items, nitems, mixed, boys_tab, nctas, st);
+  else if (wm == 2) launch_batch_wm<2>(jobs, items, nitems, mixed, boys_tab, nctas, st);
+  else launch_batch_wm<1>(jobs, items, nitems, mixed, boys_tab, nctas, st);
+}
+
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
                         bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st) {
   const bool per_fo_only = cfg.per_fo_only;
-  if (npairs > 0) k_pair_fmt<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, nfo, maxfmt, scr.pair_fmt);
-  if (ncalls > 0) k_call_share<<<(ncalls + 7) / 8, 256, 0, st>>>(ncalls, nfo, cfo, scr.share);
-  k_call_lists<<<1, LIST_THREADS, 0, st>>>(ncalls, per_fo_only ? 1 : 0, scr.share, scr.lists);
+  launch_coulomb_classify(ncalls, npairs, nfo, maxfmt, cfo, scr, per_fo_only, st);
   if (!per_fo_only && mixed && cfg.shared_tc) {
     const size_t nc = (size_t)npairs * nfo * COEF_LD, nm = (size_t)ncalls * nfo * MOM_LD;
     launch_split_tf32((size_t)npairs, nfo, coef, scr.coef_hl, st);

@@ -124,6 +124,17 @@ void flosic_sic_cycle_(const int64_t* ctx, const int32_t* ld, double* results, d
   *ierr = flosic_sic_cycle(handle(ctx), *ld, results, sic, debdax, cfrm, esic);
 }
 
+// The handles of a batch as an INTEGER*8 array: the same bytes as the
+// C array of context pointers on a 64-bit host.
+static_assert(sizeof(flosic_ctx*) == sizeof(int64_t), "context handles are INTEGER*8");
+
+void flosic_sic_batch_cycle_(const int64_t* ctxs, const int32_t* n, const int32_t* wm, const int32_t* ld,
+                             double* results, double* sic, double* debdax, double* cfrm, double* esic,
+                             int32_t* ierr) {
+  *ierr = flosic_sic_batch_cycle(reinterpret_cast<flosic_ctx**>(const_cast<int64_t*>(ctxs)), *n, *wm, *ld, results,
+                                 sic, debdax, cfrm, esic);
+}
+
 void flosic_sic_adjoint_(const int64_t* ctx, const int32_t* lspn, double* g, const int32_t* ldg, int32_t* ierr) {
   *ierr = flosic_sic_adjoint(handle(ctx), *lspn, g, *ldg);
 }

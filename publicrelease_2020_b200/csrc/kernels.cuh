@@ -94,7 +94,32 @@ struct CoulombConfig {
   int perfo_wm = 0;
   long long wait_limit = 0;  // polls of each tensor-core pipeline wait before it gives up (0: the default)
 };
+// One (molecule, spin) of a batched Coulomb launch: the arguments of the
+// per-molecule kernels (shared-geometry and per-FO calls of one spin).
+struct CoulombJob {
+  int ncalls, nfo, ldv, pad;
+  const int* lists;
+  const CallShare* share;
+  const CallInfo* calls;
+  const PairGeo* pairs;
+  const double* coef;
+  const int8_t* pair_fmt;
+  const CallFO* cfo;
+  const double* momv;
+  MeshDev M;
+  double* vh;
+  unsigned long long* cnt;
+};
 void init_coulomb_mma();
+// Pair Boys variants, shared-geometry flags and the two call lists (the set-up
+// of launch_coulomb_mma before its kernels).
+void launch_coulomb_classify(int ncalls, int npairs, int nfo, const int8_t* maxfmt, const CallFO* cfo,
+                             const CoulombScratch& scr, bool per_fo_only, cudaStream_t st);
+// Every (job, tile, FO block) item of a batch in two persistent launches
+// (shared-geometry calls, then per-FO calls added): items[i] = {job, tile,
+// FO block of 32*wm FOs, 0}; nctas persistent CTAs.
+void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems, int wm, bool mixed,
+                          const double* boys_tab, int nctas, cudaStream_t st);
 void init_coulomb_tc();
 // TF32 hi/lo split of nrow x nfo rows of KSEG doubles into the chunk-major
 // [nrow][KSEG/4][nfo][4] layout (hi, then lo at + nrow*nfo*KSEG floats).

@@ -246,6 +246,28 @@ struct TypeInfo {
   double con[3][MAX_CON][MAX_BARE];
 };
 
+// Coulomb inputs of one spin for a batched launch over many molecules (the
+// per-molecule path keeps them in the context and reuses them per spin).
+struct CoulBufs {
+  DevBuf<double> coef, cgp, mom;
+  DevBuf<int8_t> maxfmt, pairfmt;
+  DevBuf<CallFO> callfo;
+  DevBuf<CallShare> share;
+  DevBuf<int> lists;
+  DevBuf<unsigned long long> cnt;
+  void release() {
+    coef.release();
+    cgp.release();
+    mom.release();
+    maxfmt.release();
+    pairfmt.release();
+    callfo.release();
+    share.release();
+    lists.release();
+    cnt.release();
+  }
+};
+
 struct SpinCache {
   bool fo_valid = false;       // FMAT/TMAT/CFO
   bool pot_valid = false;      // potentials, RESULTS
@@ -265,7 +287,9 @@ struct SpinCache {
   DevBuf<double> vh;           // raw Coulomb [k][P]
   DevBuf<double> vpot;         // SIC potential [k][P]
   DevBuf<double> y;            // w V phi [k][P]
+  CoulBufs bc;                 // batched Coulomb launch only
   void release() {
+    bc.release();
     cfo.release();
     phi.release();
     vh.release();
@@ -280,6 +304,8 @@ struct flosic_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   DevBuf<double> d_gemm_ws;  // split-K partial products of dgemm
+  DevBuf<CoulombJob> d_jobs;  // batched Coulomb launch led by this context
+  DevBuf<int4> d_items;
   DevBuf<double> d_eig_a, d_eig_w, d_eig_v, d_eig_work;
   DevBuf<int> d_eig_info;
   bool have_geom = false, have_orb = false;
@@ -786,6 +812,8 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 void results_from_parts(const flosic_ctx* c, int nf, const double* parts, const double* asy,
                         std::vector<double>& results, std::vector<double>& cfrm);
 
+void spin_xc(flosic_ctx* c, int s);
+
 // Everything of APOTNL_SIC for all FOs of spin s (apotnl_sic.F:232-623).
 void spin_potentials(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
@@ -798,6 +826,19 @@ void spin_potentials(flosic_ctx* c, int s) {
   CUDA_CHECK(cudaEventRecord(c->ev[7], st));
   coulomb(c, s);
   CUDA_CHECK(cudaEventRecord(c->ev[4], st));
+  spin_xc(c, s);
+  c->stage_ms[0] += elapsed(c->ev[0], c->ev[1]);
+  c->stage_ms[1] += elapsed(c->ev[1], c->ev[7]);
+  c->stage_ms[2] += elapsed(c->ev[7], c->ev[3]);
+  c->stage_ms[3] += elapsed(c->ev[3], c->ev[4]);
+  c->stage_ms[4] += elapsed(c->ev[4], c->ev[5]);
+}
+
+// XC and the APOTNL_SIC mesh sums of spin s from its FO values and raw
+// Coulomb potentials (S.phi, S.vh), then RESULTS; marks the potentials valid.
+void spin_xc(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  cudaStream_t st = c->st;
   const int nf = S.nf, P = c->eval_n;
   S.vpot.ensure((size_t)nf * P);
   S.y.ensure((size_t)(c->mgga ? 4 : 1) * nf * P);
@@ -823,11 +864,6 @@ void spin_potentials(flosic_ctx* c, int s) {
                                  sizeof(double), nf, cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaEventRecord(c->ev[5], st));
   CUDA_CHECK(cudaStreamSynchronize(st));
-  c->stage_ms[0] += elapsed(c->ev[0], c->ev[1]);
-  c->stage_ms[1] += elapsed(c->ev[1], c->ev[7]);
-  c->stage_ms[2] += elapsed(c->ev[7], c->ev[3]);
-  c->stage_ms[3] += elapsed(c->ev[3], c->ev[4]);
-  c->stage_ms[4] += elapsed(c->ev[4], c->ev[5]);
   results_from_parts(c, nf, sums.data(), S.asy.data(), S.results, S.cfrm);
   S.pot_valid = true;
 }
@@ -1061,6 +1097,56 @@ void adjoint_device(flosic_ctx* c, int s, DevBuf<double>& dg) {
 //   dE/dT = (W + W^T) T + (M S^-1/2)^T,  dE/da_m = sum_j (dE/dT)_mj dT_mj/da_m.
 // This is the reference's FOD force (frmorb2.F:586-717, times 2/NSPN) reached
 // through the basis-space adjoint instead of the SIC matrix.
+// Batch of molecules: everything of spin s before its Coulomb evaluation --
+// FO construction, FO values, pair coefficients, POISSON1 call set-up and
+// call classification -- into the spin's own buffers, on the context's stream.
+// Returns the spin's job for the batched Coulomb launch.
+CoulombJob batch_prepare(flosic_ctx* c, int s) {
+  SpinCache& S = c->spin[s];
+  fo_setup(c, s);
+  fo_values(c, s);
+  const int nf = S.nf, P = c->eval_n;
+  const int npairs = (int)c->pairs.size(), ncalls = (int)c->calls.size();
+  cudaStream_t st = c->st;
+  c->d_u.ensure((size_t)nf * c->nprim * 10);
+  launch_prim_u(c->basis_dev(), nf, S.cfo.p, c->nbasis, c->d_u.p, st);
+  CoulBufs& B = S.bc;
+  B.coef.ensure((size_t)std::max(npairs, 1) * nf * COEF_LD);
+  B.maxfmt.ensure((size_t)std::max(npairs, 1) * nf);
+  B.cgp.ensure((size_t)std::max(npairs, 1) * nf * 4);
+  B.callfo.ensure((size_t)std::max(ncalls, 1) * nf);
+  B.mom.ensure((size_t)std::max(ncalls, 1) * nf * MOM_LD);
+  B.pairfmt.ensure((size_t)std::max(npairs, 1));
+  B.share.ensure((size_t)std::max(ncalls, 1));
+  B.lists.ensure((size_t)2 * ncalls + 2);
+  B.cnt.ensure(3);
+  launch_pair_coef(npairs, c->d_pairs.p, c->d_calls.p, nf, c->nprim, c->d_u.p, nullptr, c->nspn, B.coef.p,
+                   B.maxfmt.p, B.cgp.p, st);
+  launch_call_setup(ncalls, c->d_setup_list.p, c->nsingle, c->d_calls.p, c->d_pairs.p, nf, c->nspn, B.coef.p,
+                    B.maxfmt.p, B.cgp.p, c->mesh_dev(), c->d_boys.p, B.callfo.p, B.mom.p, st);
+  CUDA_CHECK(cudaMemsetAsync(B.cnt.p, 0, 3 * sizeof(unsigned long long), st));
+  CoulombScratch scr{B.pairfmt.p, B.share.p, B.lists.p, nullptr, nullptr, nullptr};
+  launch_coulomb_classify(ncalls, npairs, nf, B.maxfmt.p, B.callfo.p, scr, false, st);
+  c->launches += 6;
+  S.vh.ensure((size_t)nf * P);
+  CoulombJob J{};
+  J.ncalls = ncalls;
+  J.nfo = nf;
+  J.ldv = P;
+  J.lists = B.lists.p;
+  J.share = B.share.p;
+  J.calls = c->d_calls.p;
+  J.pairs = c->d_pairs.p;
+  J.coef = B.coef.p;
+  J.pair_fmt = B.pairfmt.p;
+  J.cfo = B.callfo.p;
+  J.momv = B.mom.p;
+  J.M = c->eval_mesh();
+  J.vh = S.vh.p;
+  J.cnt = B.cnt.p;
+  return J;
+}
+
 void fod_gradient(flosic_ctx* c, int s, double* grad) {
   DevBuf<double> dg, dm;
   adjoint_device(c, s, dg);
@@ -1168,6 +1254,8 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_v.release(); c->d_eig_work.release(); c->d_eig_info.release();
   c->d_coef_hl.release(); c->d_momv_hl.release(); c->d_tc_err.release();
   c->d_gemm_ws.release();
+  c->d_jobs.release();
+  c->d_items.release();
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return FLOSIC_OK;
@@ -1746,6 +1834,108 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
       spin_force(c, s, ps, ld, debdax + (size_t)s * ld * 3);
     }
     *esic = zsic;
+  });
+}
+
+int flosic_sic_batch_cycle(flosic_ctx** ctxs, int n, int wm, int ld, double* results, double* sic,
+                           double* debdax, double* cfrm, double* esic) {
+  return guarded([&] {
+    if (!ctxs || n < 1) fail(FLOSIC_ERR_ARG, "empty batch");
+    if (!results || !sic || !debdax || !cfrm || !esic) fail(FLOSIC_ERR_ARG, "null array argument");
+    if (wm != 0 && wm != 1 && wm != 2 && wm != 4) fail(FLOSIC_ERR_ARG, "FO block width must be 0, 1, 2 or 4 warps");
+    flosic_ctx* c0 = ctxs[0];
+    for (int m = 0; m < n; ++m) {
+      flosic_ctx* c = ctxs[m];
+      require(c, true);
+      require_whole_mesh(c);
+      if (c->device != c0->device) fail(FLOSIC_ERR_ARG, "batch contexts on different devices");
+      if (c->precision != c0->precision) fail(FLOSIC_ERR_ARG, "batch contexts in different precisions");
+      for (int s = 0; s < c->nspn; ++s)
+        if (c->nfrm[s] > ld) fail(FLOSIC_ERR_ARG, "ld smaller than NFRM");
+      for (int j = 0; j < m; ++j)
+        if (ctxs[j] == c) fail(FLOSIC_ERR_ARG, "a context appears twice in the batch");
+    }
+    CUDA_CHECK(cudaSetDevice(c0->device));
+    if (wm == 0) {  // widest block that the largest FO count fills at least half
+      int nfmax = 1;
+      for (int m = 0; m < n; ++m)
+        for (int s = 0; s < ctxs[m]->nspn; ++s) nfmax = std::max(nfmax, ctxs[m]->nfrm[s]);
+      wm = nfmax > 64 ? 4 : (nfmax > 32 ? 2 : 1);
+    }
+    // 1. every (molecule, spin) up to its Coulomb evaluation, on its own stream
+    std::vector<CoulombJob> jobs;
+    std::vector<std::pair<int, int>> owner;  // (molecule, spin) of each job
+    std::vector<int4> items;
+    for (int m = 0; m < n; ++m) {
+      flosic_ctx* c = ctxs[m];
+      c->launches = 0;
+      c->work_near = c->work_far = c->work_terms = 0;
+      for (double& x : c->stage_ms) x = 0.0;
+      invalidate(c);
+      CUDA_CHECK(cudaEventRecord(c->ev[0], c->st));
+      for (int s = 0; s < c->nspn; ++s) {
+        if (c->nfrm[s] == 0) continue;
+        const CoulombJob J = batch_prepare(c, s);
+        const int job = (int)jobs.size();
+        jobs.push_back(J);
+        owner.push_back({m, s});
+        const int nfb = (J.nfo + 32 * wm - 1) / (32 * wm);
+        for (int t = 0; t < J.M.ntiles; ++t)
+          for (int b = 0; b < nfb; ++b) items.push_back(make_int4(job, t, b, 0));
+      }
+      CUDA_CHECK(cudaEventRecord(c->ev[3], c->st));
+      if (m > 0) CUDA_CHECK(cudaStreamWaitEvent(c0->st, c->ev[3], 0));
+    }
+    // 2. all potentials of all molecules: two persistent launches on the first context's stream
+    int nsm = 148;
+    CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c0->device));
+    c0->d_jobs.ensure(std::max<size_t>(jobs.size(), 1));
+    c0->d_items.ensure(std::max<size_t>(items.size(), 1));
+    if (!jobs.empty()) {
+      CUDA_CHECK(cudaMemcpyAsync(c0->d_jobs.p, jobs.data(), sizeof(CoulombJob) * jobs.size(), cudaMemcpyHostToDevice,
+                                 c0->st));
+      CUDA_CHECK(cudaMemcpyAsync(c0->d_items.p, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice,
+                                 c0->st));
+      launch_coulomb_batch(c0->d_jobs.p, c0->d_items.p, (int)items.size(), wm,
+                           c0->precision == FLOSIC_PRECISION_MIXED, c0->d_boys.p, nsm, c0->st);
+      CUDA_CHECK(cudaGetLastError());
+      c0->launches += 2;
+    }
+    CUDA_CHECK(cudaEventRecord(c0->ev[4], c0->st));
+    for (int m = 1; m < n; ++m) CUDA_CHECK(cudaStreamWaitEvent(ctxs[m]->st, c0->ev[4], 0));
+    CUDA_CHECK(cudaStreamSynchronize(c0->st));  // the host job and item arrays may go
+    // 3. per molecule: work counts, XC and energies, SIC matrix, forces
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      flosic_ctx* c = ctxs[owner[j].first];
+      unsigned long long cnt[3];
+      CUDA_CHECK(cudaMemcpyAsync(cnt, c->spin[owner[j].second].bc.cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, c->st));
+      CUDA_CHECK(cudaStreamSynchronize(c->st));
+      c->work_near += cnt[0];
+      c->work_far += cnt[1];
+      c->work_terms += cnt[2];
+      spin_xc(c, owner[j].second);
+    }
+    for (int m = 0; m < n; ++m) {
+      flosic_ctx* c = ctxs[m];
+      double zsic = 0.0;
+      for (int s = 0; s < c->nspn; ++s) {
+        const int nf = c->nfrm[s];
+        if (nf == 0) continue;
+        spin_sic(c, s);
+        const SpinCache& S = c->spin[s];
+        const size_t o = (size_t)m * 2 + s;
+        for (int k = 0; k < nf; ++k) {
+          for (int i = 0; i < 13; ++i) results[(o * ld + k) * 13 + i] = S.results[(size_t)k * 13 + i];
+          for (int d = 0; d < 3; ++d) cfrm[(o * ld + k) * 3 + d] = S.cfrm[(size_t)k * 3 + d];
+          zsic += S.results[(size_t)k * 13 + 8];
+        }
+        double* ps = sic + o * ld * ld;
+        for (int l = 0; l < nf; ++l)
+          for (int jj = 0; jj < nf; ++jj) ps[(size_t)l * ld + jj] = S.sic[(size_t)l * nf + jj];
+        spin_force(c, s, ps, ld, debdax + o * ld * 3);
+      }
+      esic[m] = zsic;
+    }
   });
 }
 

@@ -37,7 +37,7 @@ EXPORTS = [
     "flosic_sic_set_precision", "flosic_sic_getvlxc_mgga", "flosic_sic_set_shard", "flosic_sic_partial_size",
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
     "flosic_sic_siclag_der", "flosic_sic_sicham", "flosic_sic_densold", "flosic_sic_coupot1",
-    "flosic_sic_autotune", "flosic_sic_adjoint_fod", "flosic_sic_set_wait_limit",
+    "flosic_sic_autotune", "flosic_sic_adjoint_fod", "flosic_sic_set_wait_limit", "flosic_sic_batch_cycle",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -72,6 +72,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_getvlxc_mgga.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
     L.flosic_sic_set_wait_limit.argtypes = [_vp, C.c_int64]
+    L.flosic_sic_batch_cycle.argtypes = [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_autotune.argtypes = [_vp, C.c_int, _ip, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")]
     L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
     L.flosic_sic_apotnl_sic.argtypes = [_vp, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
@@ -338,6 +339,26 @@ class FlosicSIC:
         self._check(self.L.flosic_sic_stats(self.h, la, ms, npairs, ncalls, work))
         return dict(launches=int(la[0]), stage_ms=ms, npairs=int(npairs[0]), ncalls=int(ncalls[0]),
                     near_evals=int(work[0]), far_evals=int(work[1]), far_terms=int(work[2]))
+
+
+def batch_cycle(ctxs, wm=0):
+    """One SIC cycle of every context in ctxs (flosic_sic_batch_cycle: the
+    Coulomb potentials of all molecules in two persistent launches); a list of
+    outputs shaped as FlosicSIC.cycle's."""
+    n = len(ctxs)
+    L = load_library()
+    ld = max(c.ld for c in ctxs)
+    res, sic = np.zeros(n * 2 * ld * 13), np.zeros(n * 2 * ld * ld)
+    deb, cfr, es = np.zeros(n * 2 * ld * 3), np.zeros(n * 2 * ld * 3), np.zeros(n)
+    arr = (_vp * n)(*[c.h for c in ctxs])
+    rc = L.flosic_sic_batch_cycle(arr, n, int(wm), ld, res, sic, deb, cfr, es)
+    if rc != 0:
+        raise FlosicError(rc, L.flosic_sic_last_error().decode())
+    out = []
+    for m in range(n):
+        out.append(dict(results=res.reshape(n, 2, ld, 13)[m], sic=sic.reshape(n, 2, ld, ld)[m],
+                        debdax=deb.reshape(n, 2, ld, 3)[m], cfrm=cfr.reshape(n, 2, ld, 3)[m], esic=float(es[m])))
+    return out
 
 
 def open_system(sysm, device=0, shard=None):

@@ -1,8 +1,11 @@
 """C4 shape at test size: a batch of uneven alkane chains and rings
-(workloads.alkane_batch), one context per molecule, cycles issued
-concurrently (publicrelease_2020_b200.batch).  Each molecule's result equals
-its own serial cycle bit for bit, and the smallest molecules match the FP64
-oracle at the parity tolerances of tests/test_parity_gpu.py (LDA)."""
+(workloads.alkane_batch), one context per molecule
+(publicrelease_2020_b200.batch).  The batched cycle evaluates the Coulomb
+potentials of all molecules in two persistent launches
+(flosic_sic_batch_cycle); each molecule's result equals its own serial cycle
+bit for bit, at every FO block width and in both precisions, and the
+smallest molecules match the FP64 oracle at the parity tolerances of
+tests/test_parity_gpu.py (LDA)."""
 import time
 
 import numpy as np
@@ -23,19 +26,52 @@ def batch():
     b.close()
 
 
-def test_concurrent_batch_equals_serial_cycles(batch):
+def _same(systems, a, b, what):
+    for s, p, q in zip(systems, a, b):
+        assert p["esic"] == q["esic"], (what, s.name)
+        for k in ("results", "sic", "debdax", "cfrm"):
+            n = q[k].shape[1]
+            assert np.array_equal(p[k][:, :n, ...][..., : q[k].shape[-1]], q[k]), (what, s.name, k)
+
+
+def test_batched_launch_equals_serial_cycles(batch):
     systems, b = batch
     b.cycle()                       # first cycle: buffers allocated
     t0 = time.perf_counter()
-    par = b.cycle()
+    bat = b.cycle()
     t1 = time.perf_counter()
     ser = b.cycle_serial()
     t2 = time.perf_counter()
-    print(f"batch of {len(systems)}: concurrent {t1 - t0:.3f} s, serial {t2 - t1:.3f} s")
-    for s, p, q in zip(systems, par, ser):
-        assert p["esic"] == q["esic"], s.name
-        for k in ("results", "sic", "debdax", "cfrm"):
-            assert np.array_equal(p[k], q[k]), (s.name, k)
+    con = b.cycle_streams()
+    t3 = time.perf_counter()
+    print(f"batch of {len(systems)}: batched launch {t1 - t0:.3f} s, serial {t2 - t1:.3f} s, "
+          f"concurrent streams {t3 - t2:.3f} s")
+    _same(systems, bat, ser, "batched")
+    _same(systems, con, ser, "streams")
+
+
+def test_batch_widths_and_autotune(batch):
+    systems, b = batch
+    ref = b.cycle_serial()
+    for wm in (1, 2, 4):
+        b.wm = wm
+        _same(systems, b.cycle(), ref, f"wm={wm}")
+    width, times = b.autotune(reps=1)
+    assert width in (32, 64, 128) and set(times) == {32, 64, 128}
+    _same(systems, b.cycle(), ref, "tuned")
+
+
+def test_mixed_batch_equals_serial_mixed_cycles(monkeypatch):
+    """Mixed precision: the batched launch runs the shared-geometry calls on
+    the FP32-column FP64 GEMM, which the per-molecule path selects with
+    FLOSIC_SHARED=mma; the two agree bit for bit."""
+    monkeypatch.setenv("FLOSIC_SHARED", "mma")
+    systems = W.alkane_batch(n=4, seed=120, max_carbons=4, nrad=(6, 8))
+    b = Batch(systems, precision="mixed")
+    try:
+        _same(systems, b.cycle(), b.cycle_serial(), "mixed")
+    finally:
+        b.close()
 
 
 def test_batch_molecules_match_oracle(batch):

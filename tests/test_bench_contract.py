@@ -57,9 +57,17 @@ class _Ctx:
 class _Batch:
     def __init__(self, systems, device=0):
         self.ctxs = [_Ctx(sysm=s) for s in systems]
+        self.wm = 0
 
     def cycle(self):
         return [c.cycle() for c in self.ctxs]
+
+    def cycle_streams(self):
+        return [c.cycle() for c in self.ctxs]
+
+    def autotune(self, reps=2):
+        self.wm = 2
+        return 64, {32: 0.3, 64: 0.2, 128: 0.25}
 
     def close(self):
         pass
@@ -143,3 +151,5 @@ def test_batch_line(fakes, capsys):
     _check_line(line, 2)
     assert line["config"]["molecules"] == 2
     assert line["gpu_launches"] == 2 * 2 * 7
+    assert line["config"]["autotune"]["mixed"]["fo_block"] == 64
+    assert set(line["config"]["per_molecule_streams_s_per_cycle"]) == {"fp64", "mixed"}

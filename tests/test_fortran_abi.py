@@ -94,7 +94,7 @@ def _stub_source(sigs):
                 body.append(f'  snprintf(b, sizeof b, " {v}=%d", {v}); rec(b);')
             elif t == "int64_t":
                 body.append(f'  snprintf(b, sizeof b, " {v}=%lld", (long long){v}); rec(b);')
-            elif t == "flosic_ctx**":
+            elif t == "flosic_ctx**" and v != "ctxs":
                 body.append(f'  *{v} = (flosic_ctx*)0xabc0; snprintf(b, sizeof b, " {v}=set"); rec(b);')
             else:
                 body.append(f'  snprintf(b, sizeof b, " {v}=%p", (const void*){v}); rec(b);')

@@ -166,6 +166,17 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def tf32_peak_tflops():
+    """Dense TF32 tensor rate for the roofline of the tcgen05 TF32 kernel: half
+    the bf16 burst rate the driver measured on this pool (MEASURED_PEAKS.json),
+    as kind::tf32 issues half the MACs of kind::f16 per cycle; None without it."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]) / 2.0
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def cpu_baseline(sysm, threads, reps=3):
     """The oracle (the reference algorithm restated in C++) timed on the host
     cores on a bounded sample, scaled to one full SCF cycle.
@@ -286,7 +297,8 @@ def run_ours(args, rank, world, local_rank):
         out = new_out()
         for _ in range(args.warmup):
             step(out)
-        acc = dict(coul_ms=0.0, near=0, far=0, terms=0, launches=0, stage=np.zeros(7))
+        acc = dict(coul_ms=0.0, near=0, far=0, terms=0, launches=0, stage=np.zeros(7),
+                   kern={"shared": np.zeros(4), "perfo": np.zeros(4)})
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -301,6 +313,8 @@ def run_ours(args, rank, world, local_rank):
                 acc["terms"] += st["far_terms"]
                 acc["launches"] += st["launches"]
                 acc["stage"] += st["stage_ms"]
+                for k, v in ctx.kernel_stats().items():
+                    acc["kern"][k] += np.array(v, dtype=np.float64)
             e1.record()
             torch.cuda.synchronize()
             barrier()
@@ -365,6 +379,25 @@ def run_ours(args, rank, world, local_rank):
     flops = (st_acc["near"] * COULOMB_FLOPS_NEAR + st_acc["terms"] * COULOMB_FLOPS_TERM) / args.steps / world
     peak = fp64_peak_tflops(torch)
     achieved = flops / coul_s / 1e12 if coul_s > 0 else 0.0
+    # per kernel: the counted work of each Coulomb kernel over its own event-timed
+    # span, against the peak of the tensor path it runs on
+    kernels = {}
+    for k, (ms, near, far, terms) in st_acc["kern"].items():
+        if ms <= 0 or (near == 0 and terms == 0):
+            continue
+        kflops = (near * COULOMB_FLOPS_NEAR + terms * COULOMB_FLOPS_TERM) / args.steps / world
+        kach = kflops / (ms / 1e3 / args.steps) / 1e12
+        if k == "shared" and headline == "mixed":
+            tf32 = tf32_peak_tflops()
+            kernels["k_coulomb_shared_tc"] = {
+                "achieved": kach, "ms_per_cycle": ms / args.steps, "unit": "TFLOP/s",
+                "peak": tf32 / 3 if tf32 else None, "frac": kach / (tf32 / 3) if tf32 else None,
+                "peak_kind": "tcgen05 kind::tf32 dense rate (half the measured bf16 burst rate in "
+                             "MEASURED_PEAKS.json) / 3: each counted product runs as three TF32 products"}
+        else:
+            kernels["k_coulomb_shared" if k == "shared" else "k_coulomb_perfo"] = {
+                "achieved": kach, "ms_per_cycle": ms / args.steps, "unit": "TFLOP/s", "peak": peak,
+                "frac": kach / peak if peak else None, "peak_kind": "FP64 DMMA (cuBLAS DGEMM measured in this run)"}
     ntiles = (cfg["nmsh"] + 127) // 128
     traffic = COULOMB_DRAM_BYTES_PER_TILE * ntiles if args.workload in ("c2", "c2half", "c2tiny") else None
     cfg.update(parallelism=(f"mesh shards x{world}, NCCL all-reduce of the partial sums" if world > 1
@@ -386,7 +419,8 @@ def run_ours(args, rank, world, local_rank):
                      "peak_kind": "FP64 cuBLAS DGEMM measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                      "work": f"{st_acc['near'] / args.steps:.4g} near (pair,point,FO) x {COULOMB_FLOPS_NEAR:.0f} + "
                              f"{st_acc['terms'] / args.steps:.4g} kept multipole terms x {COULOMB_FLOPS_TERM:.0f} flops "
-                             f"({st_acc['far'] / args.steps:.4g} far (call,point,FO) evaluations)"},
+                             f"({st_acc['far'] / args.steps:.4g} far (call,point,FO) evaluations)",
+                     "kernels": kernels},
         "stage_ms": {k: round(float(v) / args.steps, 3) for k, v in
                      zip(["fo", "orbitals", "coul_setup", "coul_eval", "xc", "sicmat", "forces"], st_acc["stage"])},
         "esic": r["esic"],

@@ -300,6 +300,14 @@ int flosic_sic_cycle_combine(flosic_ctx* ctx, const double* d_partial, int ld, d
 int flosic_sic_stats(flosic_ctx* ctx, int64_t* launches, double* stage_ms, int64_t* npairs,
                      int64_t* ncalls, int64_t* work);
 
+/* The Coulomb evaluation of the last cycle split by kernel (no counterpart in
+   the reference): ms[0] = the shared-geometry calls (call classification,
+   operand splits and the shared-geometry kernel: k_coulomb_shared_tc or
+   k_coulomb_shared), ms[1] = the per-FO kernel (k_coulomb_perfo), device
+   milliseconds summed over the spins; work[0..2] = near / far / kept-term
+   counts of the shared-geometry kernel, work[3..5] of the per-FO kernel. */
+int flosic_sic_kernel_stats(flosic_ctx* ctx, double* ms, int64_t* work);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,7 @@ void flosic_sic_cycle_(const int64_t* ctx, const int32_t* ld, double* results, d
                        double* cfrm, double* esic, int32_t* ierr);
 void flosic_sic_adjoint_(const int64_t* ctx, const int32_t* lspn, double* g, const int32_t* ldg,
                          int32_t* ierr);
+void flosic_sic_kernel_stats_(const int64_t* ctx, double* ms, int64_t* work, int32_t* ierr);
 void flosic_sic_batch_cycle_(const int64_t* ctxs, const int32_t* n, const int32_t* wm, const int32_t* ld,
                              double* results, double* sic, double* debdax, double* cfrm, double* esic,
                              int32_t* ierr);

@@ -210,29 +210,32 @@ void launch_scale_rows(int P, int N, const double* a, int lda, const double* w, 
 // ---------------------------------------------------------------------------
 // Basis values fused with the FO coefficients
 // ---------------------------------------------------------------------------
-constexpr int FV_BN = 64;                // FOs per CTA
 constexpr int FV_KC = 32;                // basis functions per stage (one atom, or a part of one)
-constexpr int FV_CONS = 256;             // 8 consumer warps: 4 along the rows x 2 along the FOs (32 columns)
-constexpr int FV_PROD = 128;             // 4 producer warps
+constexpr int FV_CONS = 256;             // 8 consumer warps, 32 FO columns each
+constexpr int FV_PROD = 256;             // 8 producer warps
 constexpr int FV_THREADS = FV_CONS + FV_PROD;
 constexpr int FV_BAR_FULL = 1, FV_BAR_EMPTY = 3, FV_BAR_PROD = 5;  // named barriers 1-2, 3-4, 5
 
-template <int NDERV>
+// A CTA's product: ROWS = NCH x BP rows of (channel, point) by BN FO columns.
+// BN = 64: 4 warp rows x 2 warp columns; BN = 128: half the points, 2 x 4, so
+// each point's basis values serve 128 FOs (formed once for up to 128 FOs).
+template <int NDERV, int BN>
 struct FoValShape {
   static constexpr int NCH = NDERV == 0 ? 1 : (NDERV == 1 ? 4 : 10);
-  static constexpr int BP = NDERV == 0 ? 128 : (NDERV == 1 ? 32 : 16);  // points per CTA
-  static constexpr int ROWS = NCH * BP;                                 // 128, 128, 160
-  static constexpr int MTW = ROWS / 32;                                 // m-tiles per consumer warp
+  static constexpr int BP0 = NDERV == 0 ? 128 : (NDERV == 1 ? 32 : 16);
+  static constexpr int BP = BN == 64 ? BP0 : BP0 / 2;  // points per CTA
+  static constexpr int ROWS = NCH * BP;                 // 128/128/160 (BN 64), 64/64/80 (BN 128)
+  static constexpr int WR = BN == 64 ? 4 : 2;           // consumer warps along the rows
+  static constexpr int MTW = ROWS / 8 / WR;             // m-tiles per consumer warp
   static constexpr int LDR = ROWS + 4;
 };
 
-template <int NDERV>
+template <int NDERV, int BN>
 struct FoValSmem {
-  using S = FoValShape<NDERV>;
+  using S = FoValShape<NDERV, BN>;
   double As[2][FV_KC][S::LDR];     // basis values: k = function, row = channel * BP + point
-  double Bs[2][FV_KC][FV_BN + 4];  // coefficients: k = function, column = FO
+  double Bs[3][FV_KC][BN + 4];     // coefficients: k = function, column = FO (stage qi in Bs[qi % 3])
   double g[S::BP][MAX_BARE];       // exp(-alpha r^2) of the atom's bare primitives
-  double R[S::BP][3 * MAX_CON][NDERV + 1];  // radial sums per contraction (l, c): sum c g (2 alpha)^d
   double rel[S::BP][3];            // point - atom centre
   double px[S::BP], py[S::BP], pz[S::BP];
   int kpad[2];                     // k rows of the stage in each buffer, -1 = end
@@ -249,23 +252,19 @@ __device__ __forceinline__ void fv_bar_arrive(int id, int n) {
 __constant__ int c_fv_pow[10][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0},
                                     {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
 
-// Values (and derivatives) of one contracted Cartesian function at one point
-// from its radial sums R0 = sum c g, R1 = sum c g 2 alpha, R2 = sum c g
-// (2 alpha)^2 (gorbdrv.f:196-230): the Cartesian factor x^a y^b z^c
-// (a, b, c <= 2) and the product rule, written as NCH channels into column k
-// of As (channel stride bp).
+// Values (and derivatives) of one contracted Cartesian function x^a y^b z^cz
+// (a, b, cz <= 2) at one point from its radial sums R0 = sum c g, R1 = sum
+// c g 2 alpha, R2 = sum c g (2 alpha)^2 (gorbdrv.f:196-230), by the product
+// rule, written as NCH channels into column col of As (channel stride bp).
+// Called with powers known at compile time, so the polynomial code folds.
 template <int NDERV>
-__device__ __forceinline__ void fv_function(int l, int mu, const double* Rv, const double* xyz, double* col,
-                                            int bp) {
-  constexpr int NCH = FoValShape<NDERV>::NCH;
-  const double R0 = Rv[0], R1 = NDERV > 0 ? Rv[1] : 0.0, R2 = NDERV > 1 ? Rv[2] : 0.0;
-  const int shift = (l == 0) ? 0 : (l == 1 ? 1 : 4);
-  const int* pw = c_fv_pow[shift + mu];
+__device__ __forceinline__ void fv_function(int a, int b, int cz, double R0, double R1, double R2,
+                                            const double* xyz, double* col, int bp) {
+  constexpr int NCH = NDERV == 0 ? 1 : (NDERV == 1 ? 4 : 10);
   const double x = xyz[0], y = xyz[1], z = xyz[2];
   // v^e for e = 0..2, and 0 for e < 0 (derivatives of lower powers)
   auto pw2 = [](double v, int e) -> double { return e < 0 ? 0.0 : (e == 0 ? 1.0 : (e == 1 ? v : v * v)); };
-  auto P3 = [&](int a, int b, int cc) -> double { return pw2(x, a) * pw2(y, b) * pw2(z, cc); };
-  const int a = pw[0], b = pw[1], cz = pw[2];
+  auto P3 = [&](int i, int j, int k) -> double { return pw2(x, i) * pw2(y, j) * pw2(z, k); };
   const double P = P3(a, b, cz);
   col[0] = P * R0;
   if (NCH == 1) return;
@@ -288,6 +287,25 @@ __device__ __forceinline__ void fv_function(int l, int mu, const double* Rv, con
   }
 }
 
+// The Cartesian components of one contraction of angular momentum L (s; x y z;
+// xx yy zz xy xz yz, the order of gorbdrv.f) whose function index lies in the
+// stage: component mu is function fbase + mu * ncon of the stage.
+template <int NDERV, int L>
+__device__ __forceinline__ void fv_contraction(double R0, double R1, double R2, const double* xyz, double* As_b,
+                                               int ldr, int bp, int i, int fbase, int ncon, int nfc) {
+  constexpr int NCOMP = L == 0 ? 1 : (L == 1 ? 3 : 6);
+  constexpr int SHIFT = L == 0 ? 0 : (L == 1 ? 1 : 4);
+  constexpr int PW[10][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0},
+                             {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+#pragma unroll
+  for (int mu = 0; mu < NCOMP; ++mu) {
+    const int fi = fbase + mu * ncon;
+    if (fi < 0 || fi >= nfc) continue;
+    fv_function<NDERV>(PW[SHIFT + mu][0], PW[SHIFT + mu][1], PW[SHIFT + mu][2], R0, R1, R2, xyz,
+                       As_b + (size_t)fi * ldr + i, bp);
+  }
+}
+
 // out[(ch * ncol + k) * ldo + p] = sum_f B_ch(p, f) coef[k * ldc + f] for the
 // npts points (px, py, pz) and ncol columns of coef.  Warp specialised: four
 // producer warps form the basis values of one atom (or 32 of its functions)
@@ -296,16 +314,16 @@ __device__ __forceinline__ void fv_function(int l, int mu, const double* Rv, con
 // barriers FULL+b (producers arrive, consumers wait) and EMPTY+b (consumers
 // arrive, producers wait before refilling); every stage, including the final
 // end marker, is waited on exactly once on each side.
-template <int NDERV>
+template <int NDERV, int BN>
 __global__ void __launch_bounds__(FV_THREADS, 1)
 k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* __restrict__ py,
             const double* __restrict__ pz, const double* __restrict__ coef, int ldc, int ncol,
             double* __restrict__ out, size_t ldo) {
-  using S = FoValShape<NDERV>;
+  using S = FoValShape<NDERV, BN>;
   extern __shared__ __align__(16) unsigned char fv_raw[];
-  FoValSmem<NDERV>& sm = *reinterpret_cast<FoValSmem<NDERV>*>(fv_raw);
+  FoValSmem<NDERV, BN>& sm = *reinterpret_cast<FoValSmem<NDERV, BN>*>(fv_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int p0 = blockIdx.x * S::BP, n0 = blockIdx.y * FV_BN;
+  const int p0 = blockIdx.x * S::BP, n0 = blockIdx.y * BN;
   const int np = min(S::BP, npts - p0);
   for (int i = tid; i < S::BP; i += FV_THREADS) {
     const bool v = i < np;
@@ -328,10 +346,27 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
       fv_bar_arrive(FV_BAR_FULL + b, FV_THREADS);
       ++qi;
     };
+    // coefficient rows of one stage into Bs[qi % 3] by cp.async (zero outside
+    // the matrix); issued early so their latency overlaps the stage's basis
+    // values.  Bs[qi % 3] was last read by stage qi - 3, which the consumers
+    // released before the producers passed begin() of stage qi - 1.
+    auto fetch_coef = [&](int q, int row0, int nfc, int kp) {
+      for (int e = pt; e < kp * BN; e += FV_PROD) {
+        const int n = e / kp, fi = e - n * kp;
+        const bool v = fi < nfc && n0 + n < ncol;
+        cp_async8(&sm.Bs[q % 3][fi][n], v ? coef + (size_t)(n0 + n) * ldc + row0 + fi : coef, v);
+      }
+      cp_commit();
+    };
     for (int a = 0; a < B.natoms; ++a) {
       const int t = B.atom_type[a];
       const double ax = B.atom_pos[3 * a], ay = B.atom_pos[3 * a + 1], az = B.atom_pos[3 * a + 2];
       const double amin = B.type_amin[t];
+      const int lmax = B.type_lmax[t];
+      const int nc0 = B.type_ncon[t * 3], nc1 = lmax >= 1 ? B.type_ncon[t * 3 + 1] : 0;
+      const int nc2 = lmax >= 2 ? B.type_ncon[t * 3 + 2] : 0;
+      const int nfa = nc0 + 3 * nc1 + 6 * nc2;
+      const int b0 = B.atom_boff[a];
       // primitive screen of the whole atom (gorbdrv.f:186-195): skipped when no
       // point of the block is in range (all its values are then zero)
       bool near = false;
@@ -343,13 +378,17 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
       if (pt == 0) sm.near[(a + 1) % 3] = 0;
       fv_bar_sync(FV_BAR_PROD, FV_PROD);  // also: every producer is done with g of the previous atom
       if (!sm.near[a % 3]) continue;
+      {
+        const int nfc = min(FV_KC, nfa);
+        fetch_coef(qi, b0, nfc, (nfc + 3) & ~3);  // lands while the basis values are formed
+      }
       const int nbare = B.type_nbare[t];
-      for (int e = pt; e < S::BP * MAX_BARE; e += FV_PROD) {
-        const int i = e / MAX_BARE, ib = e - i * MAX_BARE;
+      for (int e = pt; e < S::BP * nbare; e += FV_PROD) {
+        const int i = e / nbare, ib = e - i * nbare;
         const double x = sm.px[i] - ax, y = sm.py[i] - ay, z = sm.pz[i] - az;
         const double r2 = x * x + y * y + z * z;
         double v = 0.0;
-        if (i < np && ib < nbare && r2 * amin < CUTEXP) {
+        if (i < np && r2 * amin < CUTEXP) {
           const double rex = B.type_alpha[t * MAX_BARE + ib] * r2;
           v = (rex < CUTEXP) ? exp(-rex) : 0.0;
         }
@@ -361,71 +400,45 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
         }
       }
       fv_bar_sync(FV_BAR_PROD, FV_PROD);
-      // radial sums of every contraction (l, c) at every point, once per atom
-      const int lmax = B.type_lmax[t];
-      const int nc0 = B.type_ncon[t * 3], nc1 = lmax >= 1 ? B.type_ncon[t * 3 + 1] : 0;
-      const int nc2 = lmax >= 2 ? B.type_ncon[t * 3 + 2] : 0;
+      // the atom's functions: l-major, then Cartesian component, then contraction
       const int nlc = nc0 + nc1 + nc2;
       const double* alp = B.type_alpha + t * MAX_BARE;
-      for (int e = pt; e < S::BP * nlc; e += FV_PROD) {
-        const int lc = e / S::BP, i = e - lc * S::BP;
-        const int l = lc < nc0 ? 0 : (lc < nc0 + nc1 ? 1 : 2);
-        const int c = lc - (l == 0 ? 0 : (l == 1 ? nc0 : nc0 + nc1));
-        const double* con = B.type_bfcon + ((size_t)(t * 3 + l) * MAX_CON + c) * MAX_BARE;
-        double R0 = 0.0, R1 = 0.0, R2 = 0.0;
-        for (int ib = 0; ib < nbare; ++ib) {
-          const double cg = con[ib] * sm.g[i][ib];
-          R0 += cg;
-          if (NDERV > 0) {
-            const double a2 = 2.0 * alp[ib];
-            R1 += cg * a2;
-            if (NDERV > 1) R2 += cg * a2 * a2;
-          }
-        }
-        sm.R[i][lc][0] = R0;
-        if (NDERV > 0) sm.R[i][lc][1] = R1;
-        if (NDERV > 1) sm.R[i][lc][2] = R2;
-      }
-      fv_bar_sync(FV_BAR_PROD, FV_PROD);
-      // the atom's functions: l-major, then Cartesian component, then contraction
-      const int nfa = nc0 + 3 * nc1 + 6 * nc2;
-      const int b0 = B.atom_boff[a];
       for (int f0 = 0; f0 < nfa; f0 += FV_KC) {
         const int nfc = min(FV_KC, nfa - f0), kp = (nfc + 3) & ~3;
         const int b = qi & 1;
+        if (f0 > 0) fetch_coef(qi, b0 + f0, nfc, kp);  // later chunks of a large atom
         begin(b);
-        for (int e = pt; e < S::BP * kp; e += FV_PROD) {
-          const int fi = e / S::BP, i = e - fi * S::BP;
-          double* col = &sm.As[b][fi][i];
-          if (fi >= nfc) {
+        // one item per (point, contraction): its radial sums, then the
+        // components that fall in this stage
+        for (int e = pt; e < S::BP * nlc; e += FV_PROD) {
+          const int lc = e / S::BP, i = e - lc * S::BP;
+          const int l = lc < nc0 ? 0 : (lc < nc0 + nc1 ? 1 : 2);
+          const int c = lc - (l == 0 ? 0 : (l == 1 ? nc0 : nc0 + nc1));
+          const double* con = B.type_bfcon + ((size_t)(t * 3 + l) * MAX_CON + c) * MAX_BARE;
+          double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+          for (int ib = 0; ib < nbare; ++ib) {
+            const double cg = con[ib] * sm.g[i][ib];
+            R0 += cg;
+            if (NDERV > 0) {
+              const double a2 = 2.0 * alp[ib];
+              R1 += cg * a2;
+              if (NDERV > 1) R2 += cg * a2 * a2;
+            }
+          }
+          double* As_b = &sm.As[b][0][0];
+          if (l == 0) fv_contraction<NDERV, 0>(R0, R1, R2, sm.rel[i], As_b, S::LDR, S::BP, i, c - f0, nc0, nfc);
+          else if (l == 1)
+            fv_contraction<NDERV, 1>(R0, R1, R2, sm.rel[i], As_b, S::LDR, S::BP, i, nc0 + c - f0, nc1, nfc);
+          else
+            fv_contraction<NDERV, 2>(R0, R1, R2, sm.rel[i], As_b, S::LDR, S::BP, i, nc0 + 3 * nc1 + c - f0, nc2,
+                                     nfc);
+        }
+        for (int e = pt; e < S::BP * (kp - nfc); e += FV_PROD) {  // zero rows up to the k-step of 4
+          const int fi = nfc + e / S::BP, i = e % S::BP;
 #pragma unroll
-            for (int ch = 0; ch < S::NCH; ++ch) col[ch * S::BP] = 0.0;
-            continue;
-          }
-          int f = f0 + fi, l, lc0, ncon;
-          if (f < nc0) {
-            l = 0;
-            lc0 = 0;
-            ncon = nc0;
-          } else if (f < nc0 + 3 * nc1) {
-            f -= nc0;
-            l = 1;
-            lc0 = nc0;
-            ncon = nc1;
-          } else {
-            f -= nc0 + 3 * nc1;
-            l = 2;
-            lc0 = nc0 + nc1;
-            ncon = nc2;
-          }
-          const int mu = f / ncon, c = f - mu * ncon;
-          fv_function<NDERV>(l, mu, sm.R[i][lc0 + c], sm.rel[i], col, S::BP);
+          for (int ch = 0; ch < S::NCH; ++ch) sm.As[b][fi][ch * S::BP + i] = 0.0;
         }
-        for (int e = pt; e < kp * FV_BN; e += FV_PROD) {
-          const int n = e / kp, fi = e - n * kp;
-          const bool v = fi < nfc && n0 + n < ncol;
-          sm.Bs[b][fi][n] = v ? coef[(size_t)(n0 + n) * ldc + b0 + f0 + fi] : 0.0;
-        }
+        cp_wait<0>();  // this thread's coefficient copies have landed
         finish(b, kp);
       }
     }
@@ -438,7 +451,7 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
     }
   } else {
     // ---------------- consumers
-    const int wr = warp & 3, wc = warp >> 2;
+    const int wr = warp % S::WR, wc = warp / S::WR;
     double acc[S::MTW][4][2];
 #pragma unroll
     for (int x = 0; x < S::MTW; ++x)
@@ -453,7 +466,7 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
 #pragma unroll
         for (int mt = 0; mt < S::MTW; ++mt) af[mt] = sm.As[b][kk + (lane & 3)][(wr * S::MTW + mt) * 8 + (lane >> 2)];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) bf[nt] = sm.Bs[b][kk + (lane & 3)][wc * 32 + nt * 8 + (lane >> 2)];
+        for (int nt = 0; nt < 4; ++nt) bf[nt] = sm.Bs[qi % 3][kk + (lane & 3)][wc * 32 + nt * 8 + (lane >> 2)];
 #pragma unroll
         for (int mt = 0; mt < S::MTW; ++mt)
 #pragma unroll
@@ -478,28 +491,37 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
   }
 }
 
-template <int NDERV>
+template <int NDERV, int BN>
 static cudaError_t fo_values_attr() {
-  return cudaFuncSetAttribute(k_fo_values<NDERV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(FoValSmem<NDERV>));
+  return cudaFuncSetAttribute(k_fo_values<NDERV, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(FoValSmem<NDERV, BN>));
 }
 
 cudaError_t init_contract() {
-  cudaError_t e = fo_values_attr<0>();
-  if (e == cudaSuccess) e = fo_values_attr<1>();
-  if (e == cudaSuccess) e = fo_values_attr<2>();
+  cudaError_t e = fo_values_attr<0, 64>();
+  if (e == cudaSuccess) e = fo_values_attr<1, 64>();
+  if (e == cudaSuccess) e = fo_values_attr<2, 64>();
+  if (e == cudaSuccess) e = fo_values_attr<0, 128>();
+  if (e == cudaSuccess) e = fo_values_attr<1, 128>();
+  if (e == cudaSuccess) e = fo_values_attr<2, 128>();
   return e;
 }
 
 void launch_fo_values(const BasisDev& B, int nderv, int npts, const double* px, const double* py, const double* pz,
-                      const double* coef, int ldc, int ncol, double* out, size_t ldo, cudaStream_t st) {
+                      const double* coef, int ldc, int ncol, double* out, size_t ldo, int bn, cudaStream_t st) {
   if (npts <= 0 || ncol <= 0) return;
-#define FV(D)                                                                                           \
-  k_fo_values<D><<<dim3((npts + FoValShape<D>::BP - 1) / FoValShape<D>::BP, (ncol + FV_BN - 1) / FV_BN), \
-                   FV_THREADS, sizeof(FoValSmem<D>), st>>>(B, npts, px, py, pz, coef, ldc, ncol, out, ldo)
-  if (nderv == 0) FV(0);
-  else if (nderv == 1) FV(1);
-  else FV(2);
+#define FV(D, W)                                                                                            \
+  k_fo_values<D, W><<<dim3((npts + FoValShape<D, W>::BP - 1) / FoValShape<D, W>::BP, (ncol + W - 1) / W), \
+                      FV_THREADS, sizeof(FoValSmem<D, W>), st>>>(B, npts, px, py, pz, coef, ldc, ncol, out, ldo)
+  if (bn == 128) {
+    if (nderv == 0) FV(0, 128);
+    else if (nderv == 1) FV(1, 128);
+    else FV(2, 128);
+  } else {
+    if (nderv == 0) FV(0, 64);
+    else if (nderv == 1) FV(1, 64);
+    else FV(2, 64);
+  }
 #undef FV
 }
 

@@ -700,33 +700,41 @@ k_coulomb_perfo(int ncalls, const int* __restrict__ lists, int accumulate, const
 // Many molecules in one launch
 // ---------------------------------------------------------------------------
 // Persistent CTAs (one per SM) walk a list of (job, tile, FO block) items
-// spanning every molecule and spin of a batch, CTA b taking items b, b + grid,
-// ...; a job is one (molecule, spin) with its own calls, coefficients, mesh
-// and output.  Each item is the same work as one CTA of the per-molecule
-// kernels, so every potential is the same bit for bit whichever CTA runs it.
+// spanning every molecule and spin of a batch, taking the next item from a
+// global counter (items of uneven cost balance themselves); a job is one
+// (molecule, spin) with its own calls, coefficients, mesh and output.  Each
+// item is the same work as one CTA of the per-molecule kernels and writes its
+// own outputs, so every potential is the same bit for bit whichever CTA runs it.
+__device__ __forceinline__ int next_item(int* counter, int* slot) {
+  __syncthreads();  // every thread is done with the previous item (and its shared memory)
+  if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+  __syncthreads();
+  return *slot;
+}
+
 template <int WM, bool MIXED>
 __global__ void __launch_bounds__(WS_THREADS, 1)
 k_coulomb_shared_batch(const CoulombJob* __restrict__ jobs, const int4* __restrict__ items, int nitems,
-                       const double* __restrict__ boys_tab) {
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+                       int* __restrict__ counter, const double* __restrict__ boys_tab) {
+  __shared__ int slot;
+  for (int it = next_item(counter, &slot); it < nitems; it = next_item(counter, &slot)) {
     const int4 w = items[it];
     const CoulombJob J = jobs[w.x];
     shared_tile<WM, MIXED>(w.y, w.z, J.ncalls, J.lists, J.share, J.calls, J.nfo, J.coef, J.pair_fmt, J.pairs,
                            J.momv, J.M, boys_tab, J.vh, J.ldv, J.cnt);
-    __syncthreads();  // shared memory is reused by the next item
   }
 }
 
 template <int WM, bool MIXED>
 __global__ void __launch_bounds__(WS_THREADS, 1)
 k_coulomb_perfo_batch(const CoulombJob* __restrict__ jobs, const int4* __restrict__ items, int nitems,
-                      const double* __restrict__ boys_tab) {
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+                      int* __restrict__ counter, const double* __restrict__ boys_tab) {
+  __shared__ int slot;
+  for (int it = next_item(counter, &slot); it < nitems; it = next_item(counter, &slot)) {
     const int4 w = items[it];
     const CoulombJob J = jobs[w.x];
     perfo_tile<WM, MIXED>(w.y, w.z, J.ncalls, J.lists, 1, J.calls, J.pairs, J.nfo, J.coef, J.pair_fmt, J.cfo,
                           J.momv, J.M, boys_tab, J.vh, J.ldv, J.cnt);
-    __syncthreads();
   }
 }
 
@@ -897,33 +905,38 @@ void launch_coulomb_classify(int ncalls, int npairs, int nfo, const int8_t* maxf
 }
 
 template <int WM>
-static void launch_batch_wm(const CoulombJob* jobs, const int4* items, int nitems, bool mixed,
+static void launch_batch_wm(const CoulombJob* jobs, const int4* items, int nitems, int* counters, bool mixed,
                             const double* boys_tab, int nctas, cudaStream_t st) {
   if (mixed) {
-    k_coulomb_shared_batch<WM, true><<<nctas, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(jobs, items, nitems, boys_tab);
-    k_coulomb_perfo_batch<WM, true><<<nctas, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(jobs, items, nitems, boys_tab);
+    k_coulomb_shared_batch<WM, true><<<nctas, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(jobs, items, nitems,
+                                                                                          counters, boys_tab);
+    k_coulomb_perfo_batch<WM, true><<<nctas, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(jobs, items, nitems,
+                                                                                        counters + 1, boys_tab);
   } else {
     k_coulomb_shared_batch<WM, false><<<nctas, WS_THREADS, sizeof(SharedSmem<WM>), st>>>(jobs, items, nitems,
-                                                                                           boys_tab);
+                                                                                           counters, boys_tab);
     k_coulomb_perfo_batch<WM, false><<<nctas, WS_THREADS, sizeof(PerFOSmem<WM>), st>>>(jobs, items, nitems,
-                                                                                         boys_tab);
+                                                                                         counters + 1, boys_tab);
   }
 }
 
-void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems, int wm, bool mixed,
+void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems, int* counters, int wm, bool mixed,
                           const double* boys_tab, int nctas, cudaStream_t st) {
   if (nitems <= 0) return;
   nctas = std::max(1, std::min(nctas, nitems));
-  if (wm == 4) launch_batch_wm<4>(jobs, items, nitems, mixed, boys_tab, nctas, st);
-  else if (wm == 2) launch_batch_wm<2>(jobs, items, nitems, mixed, boys_tab, nctas, st);
-  else launch_batch_wm<1>(jobs, items, nitems, mixed, boys_tab, nctas, st);
+  cudaMemsetAsync(counters, 0, 2 * sizeof(int), st);
+  if (wm == 4) launch_batch_wm<4>(jobs, items, nitems, counters, mixed, boys_tab, nctas, st);
+  else if (wm == 2) launch_batch_wm<2>(jobs, items, nitems, counters, mixed, boys_tab, nctas, st);
+  else launch_batch_wm<1>(jobs, items, nitems, counters, mixed, boys_tab, nctas, st);
 }
 
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
-                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st) {
+                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaEvent_t mid,
+                        cudaStream_t st) {
   const bool per_fo_only = cfg.per_fo_only;
+  unsigned long long* cnt_perfo = cnt + 3;  // the per-FO kernel counts apart from the shared-geometry one
   launch_coulomb_classify(ncalls, npairs, nfo, maxfmt, cfo, scr, per_fo_only, st);
   if (!per_fo_only && mixed && cfg.shared_tc) {
     const size_t nc = (size_t)npairs * nfo * COEF_LD, nm = (size_t)ncalls * nfo * MOM_LD;
@@ -942,17 +955,18 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
       launch_shared<1>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
                        ldv, cnt, mixed, st);
   }
+  if (mid) cudaEventRecord(mid, st);
   const int acc = per_fo_only ? 0 : 1;
   const int wm = cfg.perfo_wm > 0 ? cfg.perfo_wm : (nfo > 64 ? 4 : (nfo > 32 ? 2 : 1));
   if (wm == 4)
     launch_perfo<4>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                    cnt, mixed, st);
+                    cnt_perfo, mixed, st);
   else if (wm == 2)
     launch_perfo<2>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                    cnt, mixed, st);
+                    cnt_perfo, mixed, st);
   else
     launch_perfo<1>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
-                    cnt, mixed, st);
+                    cnt_perfo, mixed, st);
 }
 
 }  // namespace flosic

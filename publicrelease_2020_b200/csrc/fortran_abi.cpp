@@ -124,6 +124,10 @@ void flosic_sic_cycle_(const int64_t* ctx, const int32_t* ld, double* results, d
   *ierr = flosic_sic_cycle(handle(ctx), *ld, results, sic, debdax, cfrm, esic);
 }
 
+void flosic_sic_kernel_stats_(const int64_t* ctx, double* ms, int64_t* work, int32_t* ierr) {
+  *ierr = flosic_sic_kernel_stats(handle(ctx), ms, work);
+}
+
 // The handles of a batch as an INTEGER*8 array: the same bytes as the
 // C array of context pointers on a 64-bit host.
 static_assert(sizeof(flosic_ctx*) == sizeof(int64_t), "context handles are INTEGER*8");

@@ -93,6 +93,7 @@ struct CoulombConfig {
   bool shared_tc = true;
   int perfo_wm = 0;
   long long wait_limit = 0;  // polls of each tensor-core pipeline wait before it gives up (0: the default)
+  int fo_values_bn = 64;     // FOs per CTA of the fused FO-value kernel (64 or 128)
 };
 // One (molecule, spin) of a batched Coulomb launch: the arguments of the
 // per-molecule kernels (shared-geometry and per-FO calls of one spin).
@@ -117,8 +118,9 @@ void launch_coulomb_classify(int ncalls, int npairs, int nfo, const int8_t* maxf
                              const CoulombScratch& scr, bool per_fo_only, cudaStream_t st);
 // Every (job, tile, FO block) item of a batch in two persistent launches
 // (shared-geometry calls, then per-FO calls added): items[i] = {job, tile,
-// FO block of 32*wm FOs, 0}; nctas persistent CTAs.
-void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems, int wm, bool mixed,
+// FO block of 32*wm FOs, 0}, taken in list order from two device counters
+// (counters[0..1], zeroed here); nctas persistent CTAs.
+void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems, int* counters, int wm, bool mixed,
                           const double* boys_tab, int nctas, cudaStream_t st);
 void init_coulomb_tc();
 // TF32 hi/lo split of nrow x nfo rows of KSEG doubles into the chunk-major
@@ -130,10 +132,13 @@ void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* sha
                               const float* momv_hl, size_t mom_part, const MeshDev& M, const double* boys_tab,
                               double* vh, int ldv, unsigned long long* cnt, int* err, long long wait_limit,
                               cudaStream_t st);
+// cnt[0..2]: near/far/terms of the shared-geometry kernel, cnt[3..5]: of the per-FO kernel;
+// mid (may be null) is recorded between the two kernels.
 void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
                         const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
                         const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
-                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaStream_t st);
+                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaEvent_t mid,
+                        cudaStream_t st);
 
 // Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as
 // in apotnl_sic.F:419) from the FO values/derivatives phi[(ch*nfo+k)*ldp+p];
@@ -161,8 +166,9 @@ void dgemm(bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
 // out[(ch*ncol + k)*ldo + p] = sum_f B_ch(p, f) coef[k*ldc + f]: basis values
 // (nderv 0, 1, 2 -> 1, 4, 10 channels) at npts points times ncol coefficient columns.
 cudaError_t init_contract();
+// bn: FOs per CTA, 64 or 128 (the basis values of a point formed once per bn FOs).
 void launch_fo_values(const BasisDev& B, int nderv, int npts, const double* px, const double* py, const double* pz,
-                      const double* coef, int ldc, int ncol, double* out, size_t ldo, cudaStream_t st);
+                      const double* coef, int ldc, int ncol, double* out, size_t ldo, int bn, cudaStream_t st);
 // out[k*ldo + p] = w[p] a[k*lda + p]
 void launch_scale_rows(int P, int N, const double* a, int lda, const double* w, double* out, int ldo,
                        cudaStream_t st);

@@ -306,6 +306,7 @@ struct flosic_ctx {
   DevBuf<double> d_gemm_ws;  // split-K partial products of dgemm
   DevBuf<CoulombJob> d_jobs;  // batched Coulomb launch led by this context
   DevBuf<int4> d_items;
+  DevBuf<int> d_batch_counters;
   DevBuf<double> d_eig_a, d_eig_w, d_eig_v, d_eig_work;
   DevBuf<int> d_eig_info;
   bool have_geom = false, have_orb = false;
@@ -360,7 +361,9 @@ struct flosic_ctx {
   // stats
   long long launches = 0;
   double stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
-  cudaEvent_t ev[8] = {};
+  double kernel_ms[2] = {0, 0};  // Coulomb evaluation: shared-geometry kernel (with call set-up), per-FO kernel
+  unsigned long long kernel_work[6] = {0, 0, 0, 0, 0, 0};  // near/far/terms of each
+  cudaEvent_t ev[10] = {};
 
   BasisDev basis_dev() const {
     BasisDev B;
@@ -678,7 +681,7 @@ void fo_setup(flosic_ctx* c, int s) {
   const double* cthr = c->d_psi_thr.p + (size_t)s * c->nwfs[0] * nb;
   // PSIG_ch (nf x nw) = B_ch (FODs x nb) * C (nb x nw), basis values formed in the kernel
   launch_fo_values(c->basis_dev(), 1, nf, c->d_fodpts.p, c->d_fodpts.p + nf, c->d_fodpts.p + 2 * nf, cthr, nb, nw,
-                   c->d_psig.p, nf, st);
+                   c->d_psig.p, nf, c->coulomb_cfg.fo_values_bn, st);
   c->launches++;
   std::vector<double> psig((size_t)4 * nf * nw);
   CUDA_CHECK(cudaMemcpyAsync(psig.data(), c->d_psig.p, sizeof(double) * psig.size(), cudaMemcpyDeviceToHost, st));
@@ -738,7 +741,7 @@ void fo_values(flosic_ctx* c, int s) {
   // Phi_ch (P x nf) = B_ch (P x nb) C_FO, basis values formed in shared memory
   const size_t q0 = (size_t)c->eval_p0;
   launch_fo_values(c->basis_dev(), nderv, P, c->d_x.p + q0, c->d_y.p + q0, c->d_z.p + q0, S.cfo.p, nb, nf, S.phi.p,
-                   P, c->st);
+                   P, c->coulomb_cfg.fo_values_bn, c->st);
   c->launches++;
 }
 
@@ -746,6 +749,8 @@ void fo_values(flosic_ctx* c, int s) {
 // densities whose primitive projections are in d_u (dm == nullptr: FO k is
 // the rank-1 density of u_k), or for the one density given by its pair
 // blocks dm (nf = 1).  vh[k*P + p] over the evaluated mesh.
+float elapsed(cudaEvent_t a, cudaEvent_t b);
+
 void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
   const int P = c->eval_n;
   const int npairs = (int)c->pairs.size(), ncalls = (int)c->calls.size();
@@ -766,8 +771,8 @@ void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
   c->d_pairfmt.ensure((size_t)std::max(npairs, 1));
   c->d_share.ensure((size_t)std::max(ncalls, 1));
   c->d_lists.ensure((size_t)2 * ncalls + 2);
-  c->d_cnt.ensure(3);
-  CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 3 * sizeof(unsigned long long), st));
+  c->d_cnt.ensure(6);
+  CUDA_CHECK(cudaMemsetAsync(c->d_cnt.p, 0, 6 * sizeof(unsigned long long), st));
   const bool mixed = c->precision == FLOSIC_PRECISION_MIXED;
   if (mixed) {
     c->d_coef_hl.ensure((size_t)2 * std::max(npairs, 1) * nf * COEF_LD);
@@ -778,17 +783,21 @@ void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p, c->d_coef_hl.p, c->d_momv_hl.p, c->d_tc_err.p};
   launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
                      c->d_mom.p, c->eval_mesh(), c->d_boys.p, vh, P, c->coulomb_cfg, mixed, scr,
-                     c->d_cnt.p, st);
+                     c->d_cnt.p, c->ev[8], st);
+  CUDA_CHECK(cudaEventRecord(c->ev[9], st));
   c->launches += c->coulomb_cfg.per_fo_only ? 4 : 5;
-  unsigned long long cnt[3];
+  unsigned long long cnt[6];
   int tc_err = 0;
   CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
   if (mixed) CUDA_CHECK(cudaMemcpyAsync(&tc_err, c->d_tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
   if (tc_err) fail(FLOSIC_ERR_CUDA, "mixed-precision Coulomb kernel: a pipeline wait reached its limit");
-  c->work_near += cnt[0];
-  c->work_far += cnt[1];
-  c->work_terms += cnt[2];
+  c->work_near += cnt[0] + cnt[3];
+  c->work_far += cnt[1] + cnt[4];
+  c->work_terms += cnt[2] + cnt[5];
+  for (int j = 0; j < 6; ++j) c->kernel_work[j] += cnt[j];
+  c->kernel_ms[0] += elapsed(c->ev[3], c->ev[8]);
+  c->kernel_ms[1] += elapsed(c->ev[8], c->ev[9]);
   CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1212,6 +1221,7 @@ int flosic_sic_create(int device, flosic_ctx** out) {
     c->device = device;
     if (const char* e = std::getenv("FLOSIC_COULOMB")) c->coulomb_cfg.per_fo_only = (std::string(e) == "perfo");
     if (const char* e = std::getenv("FLOSIC_SHARED")) c->coulomb_cfg.shared_tc = (std::string(e) != "mma");
+    if (const char* e = std::getenv("FLOSIC_FOV_BN")) c->coulomb_cfg.fo_values_bn = std::atoi(e) == 128 ? 128 : 64;
     if (const char* e = std::getenv("FLOSIC_PERFO_WM")) {
       const int wm = std::atoi(e);
       c->coulomb_cfg.perfo_wm = (wm == 1 || wm == 2 || wm == 4) ? wm : 0;
@@ -1256,6 +1266,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_gemm_ws.release();
   c->d_jobs.release();
   c->d_items.release();
+  c->d_batch_counters.release();
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return FLOSIC_OK;
@@ -1816,6 +1827,8 @@ int flosic_sic_cycle(flosic_ctx* c, int ld, double* results, double* sic, double
     c->launches = 0;
     c->work_near = c->work_far = c->work_terms = 0;
     for (double& m : c->stage_ms) m = 0.0;
+    c->kernel_ms[0] = c->kernel_ms[1] = 0.0;
+    for (auto& w : c->kernel_work) w = 0;
     invalidate(c);
     double zsic = 0.0;
     for (int s = 0; s < c->nspn; ++s) {
@@ -1871,20 +1884,29 @@ int flosic_sic_batch_cycle(flosic_ctx** ctxs, int n, int wm, int ld, double* res
       c->launches = 0;
       c->work_near = c->work_far = c->work_terms = 0;
       for (double& x : c->stage_ms) x = 0.0;
+      c->kernel_ms[0] = c->kernel_ms[1] = 0.0;
+      for (auto& w : c->kernel_work) w = 0;
       invalidate(c);
       CUDA_CHECK(cudaEventRecord(c->ev[0], c->st));
       for (int s = 0; s < c->nspn; ++s) {
         if (c->nfrm[s] == 0) continue;
-        const CoulombJob J = batch_prepare(c, s);
-        const int job = (int)jobs.size();
-        jobs.push_back(J);
+        jobs.push_back(batch_prepare(c, s));
         owner.push_back({m, s});
-        const int nfb = (J.nfo + 32 * wm - 1) / (32 * wm);
-        for (int t = 0; t < J.M.ntiles; ++t)
-          for (int b = 0; b < nfb; ++b) items.push_back(make_int4(job, t, b, 0));
       }
       CUDA_CHECK(cudaEventRecord(c->ev[3], c->st));
       if (m > 0) CUDA_CHECK(cudaStreamWaitEvent(c0->st, c->ev[3], 0));
+    }
+    // work list, costliest jobs first (a tile walks every call of its job; the
+    // counter then hands the cheap items to whichever CTA frees up)
+    std::vector<int> order(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) order[j] = (int)j;
+    auto cost = [&](int j) { return (double)jobs[j].ncalls * std::min(jobs[j].nfo, 32 * wm); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    for (int job : order) {
+      const CoulombJob& J = jobs[job];
+      const int nfb = (J.nfo + 32 * wm - 1) / (32 * wm);
+      for (int t = 0; t < J.M.ntiles; ++t)
+        for (int b = 0; b < nfb; ++b) items.push_back(make_int4(job, t, b, 0));
     }
     // 2. all potentials of all molecules: two persistent launches on the first context's stream
     int nsm = 148;
@@ -1896,7 +1918,8 @@ int flosic_sic_batch_cycle(flosic_ctx** ctxs, int n, int wm, int ld, double* res
                                  c0->st));
       CUDA_CHECK(cudaMemcpyAsync(c0->d_items.p, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice,
                                  c0->st));
-      launch_coulomb_batch(c0->d_jobs.p, c0->d_items.p, (int)items.size(), wm,
+      c0->d_batch_counters.ensure(2);
+      launch_coulomb_batch(c0->d_jobs.p, c0->d_items.p, (int)items.size(), c0->d_batch_counters.p, wm,
                            c0->precision == FLOSIC_PRECISION_MIXED, c0->d_boys.p, nsm, c0->st);
       CUDA_CHECK(cudaGetLastError());
       c0->launches += 2;
@@ -2156,7 +2179,7 @@ int flosic_sic_densold(flosic_ctx* c, int ngrad, double* rhog, double* phig) {
       // PSIG (densold.F:160-185): coefficients at or below 1e-10 are skipped, as in d_psi_thr
       if (nwf > 0) {
         launch_fo_values(c->basis_dev(), nderv, np, c->d_x.p + p0, c->d_y.p + p0, c->d_z.p + p0, c->d_psi_thr.p, nb,
-                         nwf, dv.p, np, c->st);
+                         nwf, dv.p, np, c->coulomb_cfg.fo_values_bn, c->st);
         c->launches++;
       }
       launch_densold(np, nw0, nw1, ns, ngrad, dv.p, np, dr.p + p0, phig ? dph.p + p0 : nullptr, P, c->st);
@@ -2236,6 +2259,8 @@ int flosic_sic_cycle_partial(flosic_ctx* c, double* d_partial) {
     c->launches = 0;
     c->work_near = c->work_far = c->work_terms = 0;
     for (double& m : c->stage_ms) m = 0.0;
+    c->kernel_ms[0] = c->kernel_ms[1] = 0.0;
+    for (auto& w : c->kernel_work) w = 0;
     invalidate(c);
     std::vector<double> h(partial_doubles(c), 0.0);
     size_t o = 0;
@@ -2313,6 +2338,17 @@ int flosic_sic_stats(flosic_ctx* c, int64_t* launches, double* stage_ms, int64_t
     for (int i = 0; i < 7; ++i) stage_ms[i] = c->stage_ms[i];
   if (npairs) *npairs = (int64_t)c->pairs.size();
   if (ncalls) *ncalls = (int64_t)c->calls.size();
+  return FLOSIC_OK;
+}
+
+int flosic_sic_kernel_stats(flosic_ctx* c, double* ms, int64_t* work) {
+  if (!c) return FLOSIC_ERR_ARG;
+  if (ms) {
+    ms[0] = c->kernel_ms[0];
+    ms[1] = c->kernel_ms[1];
+  }
+  if (work)
+    for (int j = 0; j < 6; ++j) work[j] = (int64_t)c->kernel_work[j];
   return FLOSIC_OK;
 }
 

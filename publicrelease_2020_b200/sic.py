@@ -38,6 +38,7 @@ EXPORTS = [
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
     "flosic_sic_siclag_der", "flosic_sic_sicham", "flosic_sic_densold", "flosic_sic_coupot1",
     "flosic_sic_autotune", "flosic_sic_adjoint_fod", "flosic_sic_set_wait_limit", "flosic_sic_batch_cycle",
+    "flosic_sic_kernel_stats",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -72,6 +73,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_getvlxc_mgga.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
     L.flosic_sic_set_wait_limit.argtypes = [_vp, C.c_int64]
+    L.flosic_sic_kernel_stats.argtypes = [_vp, _dp, _i64]
     L.flosic_sic_batch_cycle.argtypes = [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_autotune.argtypes = [_vp, C.c_int, _ip, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")]
     L.flosic_sic_getvlxc_device.argtypes = [_vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]
@@ -339,6 +341,15 @@ class FlosicSIC:
         self._check(self.L.flosic_sic_stats(self.h, la, ms, npairs, ncalls, work))
         return dict(launches=int(la[0]), stage_ms=ms, npairs=int(npairs[0]), ncalls=int(ncalls[0]),
                     near_evals=int(work[0]), far_evals=int(work[1]), far_terms=int(work[2]))
+
+    def kernel_stats(self):
+        """The last cycle's Coulomb evaluation by kernel: {'shared': (ms, near,
+        far, terms), 'perfo': (ms, near, far, terms)} (flosic_sic_kernel_stats)."""
+        ms = np.zeros(2)
+        w = np.zeros(6, dtype=np.int64)
+        self._check(self.L.flosic_sic_kernel_stats(self.h, ms, w))
+        return {"shared": (float(ms[0]), int(w[0]), int(w[1]), int(w[2])),
+                "perfo": (float(ms[1]), int(w[3]), int(w[4]), int(w[5]))}
 
 
 def batch_cycle(ctxs, wm=0):

@@ -50,6 +50,9 @@ class _Ctx:
         return dict(launches=7, stage_ms=np.full(7, 1.0), npairs=3, ncalls=2, near_evals=1000, far_evals=50,
                     far_terms=200)
 
+    def kernel_stats(self):
+        return {"shared": (0.6, 600, 30, 120), "perfo": (0.4, 400, 20, 80)}
+
     def close(self):
         pass
 
@@ -142,6 +145,12 @@ def test_single_system_line(fakes, capsys):
     _check_line(line, 2)
     assert line["config"]["autotune"]["mixed"]["perfo_fo_slots"] == 32
     assert line["gpu_launches"] == 2 * 7
+    kern = line["roofline"]["kernels"]
+    assert set(kern) == {"k_coulomb_shared_tc", "k_coulomb_perfo"}   # mixed headline: TF32 shared kernel
+    per = kern["k_coulomb_perfo"]
+    # perfo: 2 steps x (400 near x 92 + 80 terms x 2) flops over 2 x 0.4 ms
+    assert per["achieved"] == pytest.approx((400 * 92 + 80 * 2) / 0.4e-3 / 1e12)
+    assert per["frac"] == pytest.approx(per["achieved"] / per["peak"])
 
 
 def test_batch_line(fakes, capsys):

@@ -1,0 +1,39 @@
+"""C2 at full size (40 atoms, 512 functions, 1,000,000 mesh points, 128 FOs,
+PBE, NSPN=1), FP64 path through the C ABI, against the FP64 oracle's
+RESULTS(1:13) and SIC-matrix columns of the first four FOs
+(tests/golden/c2_full_results.npz, made by make_c2_full_golden.py: the oracle
+needs tens of CPU-minutes for them).  Tolerances as in test_parity_gpu.py:
+RESULTS to 1e-8 Ha, SIC-matrix entries to 1e-8 of the largest (GGA)."""
+import os
+
+import numpy as np
+import pytest
+
+from publicrelease_2020_b200 import sic as S
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = np.load(os.path.join(HERE, "golden", "c2_full_results.npz"))
+
+
+def test_c2_full_size_matches_oracle():
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_c2_full_golden import system
+
+    sysm = system()
+    assert sysm.nmsh == int(GOLD["nmsh"]) and sysm.nbasis == int(GOLD["nbasis"])
+    ctx = S.open_system(sysm)
+    try:
+        r = ctx.cycle()
+    finally:
+        ctx.close()
+    gold, cols = GOLD["results"], GOLD["sic_cols"]
+    nfo = gold.shape[0]
+    g = r["results"][0][:nfo]
+    assert np.allclose(g[:, 0], gold[:, 0])
+    assert np.max(np.abs(g[:, 1:] - gold[:, 1:])) < 1e-8, np.abs(g[:, 1:] - gold[:, 1:]).max(axis=0)
+    n = int(GOLD["nfo"])
+    lam = r["sic"][0][:nfo, :n]            # [l][j] = SIC(j, l), columns l < nfo
+    assert np.max(np.abs(lam - cols)) < 1e-8 * np.abs(cols).max()

@@ -34,6 +34,8 @@ F_TOL_GGA = 1e-6   # Ha/bohr: GGA forces inherit the SIC-matrix differences abov
 def systems():
     return {
         "water_lda_nspn2": W.water(seed=0, nrad=18),
+        # C1 as configured: water on the reference's default NRLMOL basis (73 functions)
+        "water_default_basis_lda_nspn2": W.water(seed=0, nrad=18, basis="default"),
         "synthetic_pbe_nspn1": W.small_synthetic(seed=5, natoms=3, nbasis=24, nmsh=5000, nfo=4),
         "synthetic_pw91gga_nspn2": W.small_synthetic(seed=7, natoms=3, nbasis=30, nmsh=4000, nfo=3,
                                                      functional="GGA-PW91*GGA-PW91", nspn=2),

@@ -228,6 +228,7 @@ struct FoValShape {
   static constexpr int WR = BN == 64 ? 4 : 2;           // consumer warps along the rows
   static constexpr int MTW = ROWS / 8 / WR;             // m-tiles per consumer warp
   static constexpr int LDR = ROWS + 4;
+  static constexpr int GA = BP <= 32 ? 4 : 2;           // atoms per stage at most (their exponentials in smem)
 };
 
 template <int NDERV, int BN>
@@ -235,11 +236,11 @@ struct FoValSmem {
   using S = FoValShape<NDERV, BN>;
   double As[2][FV_KC][S::LDR];     // basis values: k = function, row = channel * BP + point
   double Bs[3][FV_KC][BN + 4];     // coefficients: k = function, column = FO (stage qi in Bs[qi % 3])
-  double g[S::BP][MAX_BARE];       // exp(-alpha r^2) of the atom's bare primitives
-  double rel[S::BP][3];            // point - atom centre
+  double g[S::GA][S::BP][MAX_BARE];  // exp(-alpha r^2) of each stage atom's bare primitives
+  double rel[S::GA][S::BP][3];       // point - atom centre
   double px[S::BP], py[S::BP], pz[S::BP];
   int kpad[2];                     // k rows of the stage in each buffer, -1 = end
-  int near[3];                     // per atom (mod 3): some point of the block in range
+  unsigned near[3];                // per window of atoms (mod 3): bit j set when atom j has a point in range
 };
 
 __device__ __forceinline__ void fv_bar_sync(int id, int n) {
@@ -346,101 +347,190 @@ k_fo_values(BasisDev B, int npts, const double* __restrict__ px, const double* _
       fv_bar_arrive(FV_BAR_FULL + b, FV_THREADS);
       ++qi;
     };
-    // coefficient rows of one stage into Bs[qi % 3] by cp.async (zero outside
-    // the matrix); issued early so their latency overlaps the stage's basis
-    // values.  Bs[qi % 3] was last read by stage qi - 3, which the consumers
-    // released before the producers passed begin() of stage qi - 1.
-    auto fetch_coef = [&](int q, int row0, int nfc, int kp) {
+    // The atoms go to the tensor cores in stages of up to 32 basis functions:
+    // consecutive atoms that some point of the block reaches (primitive
+    // screen of gorbdrv.f:186-195; the others' values are all zero) are
+    // packed into one stage while they fit, at most GA of them; an atom with
+    // more than 32 functions takes stages of its own, 32 functions each.
+    constexpr int GA = S::GA;
+    struct Member {
+      int atom, type, nbare, nc0, nc1, nc2, nfa, boff, off;
+      double ax, ay, az, amin;
+    };
+    auto member = [&](int at) {
+      Member m;
+      m.atom = at;
+      m.type = B.atom_type[at];
+      const int t = m.type, lmax = B.type_lmax[t];
+      m.nbare = B.type_nbare[t];
+      m.nc0 = B.type_ncon[t * 3];
+      m.nc1 = lmax >= 1 ? B.type_ncon[t * 3 + 1] : 0;
+      m.nc2 = lmax >= 2 ? B.type_ncon[t * 3 + 2] : 0;
+      m.nfa = m.nc0 + 3 * m.nc1 + 6 * m.nc2;
+      m.boff = B.atom_boff[at];
+      m.off = 0;
+      m.ax = B.atom_pos[3 * at];
+      m.ay = B.atom_pos[3 * at + 1];
+      m.az = B.atom_pos[3 * at + 2];
+      m.amin = B.type_amin[t];
+      return m;
+    };
+    // coefficient rows of the stage (function fi of the stage is row
+    // row_of(fi) of coef) into Bs[qi % 3] by cp.async (zero outside the
+    // matrix); issued early so their latency overlaps the basis values.
+    // Bs[qi % 3] was last read by stage qi - 3, which the consumers released
+    // before the producers passed begin() of stage qi - 1.
+    auto fetch_coef = [&](int q, int nfc, int kp, auto row_of) {
       for (int e = pt; e < kp * BN; e += FV_PROD) {
         const int n = e / kp, fi = e - n * kp;
         const bool v = fi < nfc && n0 + n < ncol;
-        cp_async8(&sm.Bs[q % 3][fi][n], v ? coef + (size_t)(n0 + n) * ldc + row0 + fi : coef, v);
+        cp_async8(&sm.Bs[q % 3][fi][n], v ? coef + (size_t)(n0 + n) * ldc + row_of(fi) : coef, v);
       }
       cp_commit();
     };
-    for (int a = 0; a < B.natoms; ++a) {
-      const int t = B.atom_type[a];
-      const double ax = B.atom_pos[3 * a], ay = B.atom_pos[3 * a + 1], az = B.atom_pos[3 * a + 2];
-      const double amin = B.type_amin[t];
-      const int lmax = B.type_lmax[t];
-      const int nc0 = B.type_ncon[t * 3], nc1 = lmax >= 1 ? B.type_ncon[t * 3 + 1] : 0;
-      const int nc2 = lmax >= 2 ? B.type_ncon[t * 3 + 2] : 0;
-      const int nfa = nc0 + 3 * nc1 + 6 * nc2;
-      const int b0 = B.atom_boff[a];
-      // primitive screen of the whole atom (gorbdrv.f:186-195): skipped when no
-      // point of the block is in range (all its values are then zero)
-      bool near = false;
-      for (int i = pt; i < np; i += FV_PROD) {
-        const double x = sm.px[i] - ax, y = sm.py[i] - ay, z = sm.pz[i] - az;
-        if ((x * x + y * y + z * z) * amin < CUTEXP) near = true;
-      }
-      if (near) atomicOr(&sm.near[a % 3], 1);
-      if (pt == 0) sm.near[(a + 1) % 3] = 0;
-      fv_bar_sync(FV_BAR_PROD, FV_PROD);  // also: every producer is done with g of the previous atom
-      if (!sm.near[a % 3]) continue;
-      {
-        const int nfc = min(FV_KC, nfa);
-        fetch_coef(qi, b0, nfc, (nfc + 3) & ~3);  // lands while the basis values are formed
-      }
-      const int nbare = B.type_nbare[t];
-      for (int e = pt; e < S::BP * nbare; e += FV_PROD) {
-        const int i = e / nbare, ib = e - i * nbare;
-        const double x = sm.px[i] - ax, y = sm.py[i] - ay, z = sm.pz[i] - az;
+    // exp(-alpha r^2) of member slot ms at the block's points
+    auto exps = [&](int ms, const Member& m) {
+      for (int e = pt; e < S::BP * m.nbare; e += FV_PROD) {
+        const int i = e / m.nbare, ib = e - i * m.nbare;
+        const double x = sm.px[i] - m.ax, y = sm.py[i] - m.ay, z = sm.pz[i] - m.az;
         const double r2 = x * x + y * y + z * z;
         double v = 0.0;
-        if (i < np && r2 * amin < CUTEXP) {
-          const double rex = B.type_alpha[t * MAX_BARE + ib] * r2;
+        if (i < np && r2 * m.amin < CUTEXP) {
+          const double rex = B.type_alpha[m.type * MAX_BARE + ib] * r2;
           v = (rex < CUTEXP) ? exp(-rex) : 0.0;
         }
-        sm.g[i][ib] = v;
+        sm.g[ms][i][ib] = v;
         if (ib == 0) {
-          sm.rel[i][0] = x;
-          sm.rel[i][1] = y;
-          sm.rel[i][2] = z;
+          sm.rel[ms][i][0] = x;
+          sm.rel[ms][i][1] = y;
+          sm.rel[ms][i][2] = z;
         }
       }
-      fv_bar_sync(FV_BAR_PROD, FV_PROD);
-      // the atom's functions: l-major, then Cartesian component, then contraction
-      const int nlc = nc0 + nc1 + nc2;
-      const double* alp = B.type_alpha + t * MAX_BARE;
-      for (int f0 = 0; f0 < nfa; f0 += FV_KC) {
-        const int nfc = min(FV_KC, nfa - f0), kp = (nfc + 3) & ~3;
-        const int b = qi & 1;
-        if (f0 > 0) fetch_coef(qi, b0 + f0, nfc, kp);  // later chunks of a large atom
-        begin(b);
-        // one item per (point, contraction): its radial sums, then the
-        // components that fall in this stage
-        for (int e = pt; e < S::BP * nlc; e += FV_PROD) {
-          const int lc = e / S::BP, i = e - lc * S::BP;
-          const int l = lc < nc0 ? 0 : (lc < nc0 + nc1 ? 1 : 2);
-          const int c = lc - (l == 0 ? 0 : (l == 1 ? nc0 : nc0 + nc1));
-          const double* con = B.type_bfcon + ((size_t)(t * 3 + l) * MAX_CON + c) * MAX_BARE;
-          double R0 = 0.0, R1 = 0.0, R2 = 0.0;
-          for (int ib = 0; ib < nbare; ++ib) {
-            const double cg = con[ib] * sm.g[i][ib];
-            R0 += cg;
-            if (NDERV > 0) {
-              const double a2 = 2.0 * alp[ib];
-              R1 += cg * a2;
-              if (NDERV > 1) R2 += cg * a2 * a2;
-            }
-          }
-          double* As_b = &sm.As[b][0][0];
-          if (l == 0) fv_contraction<NDERV, 0>(R0, R1, R2, sm.rel[i], As_b, S::LDR, S::BP, i, c - f0, nc0, nfc);
-          else if (l == 1)
-            fv_contraction<NDERV, 1>(R0, R1, R2, sm.rel[i], As_b, S::LDR, S::BP, i, nc0 + c - f0, nc1, nfc);
-          else
-            fv_contraction<NDERV, 2>(R0, R1, R2, sm.rel[i], As_b, S::LDR, S::BP, i, nc0 + 3 * nc1 + c - f0, nc2,
-                                     nfc);
+    };
+    // one item per (point, contraction of member slot ms): its radial sums,
+    // then the components whose stage column fbase + mu * ncon lies in [0, nfc)
+    auto item = [&](int ms, const Member& m, int lc, int i, int f0, double* As_b, int nfc) {
+      const int l = lc < m.nc0 ? 0 : (lc < m.nc0 + m.nc1 ? 1 : 2);
+      const int c = lc - (l == 0 ? 0 : (l == 1 ? m.nc0 : m.nc0 + m.nc1));
+      const double* con = B.type_bfcon + ((size_t)(m.type * 3 + l) * MAX_CON + c) * MAX_BARE;
+      const double* alp = B.type_alpha + m.type * MAX_BARE;
+      double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+      for (int ib = 0; ib < m.nbare; ++ib) {
+        const double cg = con[ib] * sm.g[ms][i][ib];
+        R0 += cg;
+        if (NDERV > 0) {
+          const double a2 = 2.0 * alp[ib];
+          R1 += cg * a2;
+          if (NDERV > 1) R2 += cg * a2 * a2;
         }
-        for (int e = pt; e < S::BP * (kp - nfc); e += FV_PROD) {  // zero rows up to the k-step of 4
-          const int fi = nfc + e / S::BP, i = e % S::BP;
+      }
+      const int base = m.off - f0;
+      if (l == 0) fv_contraction<NDERV, 0>(R0, R1, R2, sm.rel[ms][i], As_b, S::LDR, S::BP, i, base + c, m.nc0, nfc);
+      else if (l == 1)
+        fv_contraction<NDERV, 1>(R0, R1, R2, sm.rel[ms][i], As_b, S::LDR, S::BP, i, base + m.nc0 + c, m.nc1, nfc);
+      else
+        fv_contraction<NDERV, 2>(R0, R1, R2, sm.rel[ms][i], As_b, S::LDR, S::BP, i, base + m.nc0 + 3 * m.nc1 + c,
+                                 m.nc2, nfc);
+    };
+    auto pad_rows = [&](int b, int nfc, int kp) {  // zero rows up to the k-step of 4
+      for (int e = pt; e < S::BP * (kp - nfc); e += FV_PROD) {
+        const int fi = nfc + e / S::BP, i = e % S::BP;
 #pragma unroll
-          for (int ch = 0; ch < S::NCH; ++ch) sm.As[b][fi][ch * S::BP + i] = 0.0;
-        }
-        cp_wait<0>();  // this thread's coefficient copies have landed
-        finish(b, kp);
+        for (int ch = 0; ch < S::NCH; ++ch) sm.As[b][fi][ch * S::BP + i] = 0.0;
       }
+    };
+    int win = 0;
+    for (int a = 0; a < B.natoms;) {
+      // screen the window a .. a + GA - 1; every producer passed the previous
+      // stage's items, so g and rel may be rewritten after this barrier
+      const int wn = min(GA, B.natoms - a);
+      unsigned bits = 0;
+      for (int j = 0; j < wn; ++j) {
+        const int at = a + j;
+        const int t = B.atom_type[at];
+        const double ax = B.atom_pos[3 * at], ay = B.atom_pos[3 * at + 1], az = B.atom_pos[3 * at + 2];
+        const double amin = B.type_amin[t];
+        for (int i = pt; i < np; i += FV_PROD) {
+          const double x = sm.px[i] - ax, y = sm.py[i] - ay, z = sm.pz[i] - az;
+          if ((x * x + y * y + z * z) * amin < CUTEXP) bits |= 1u << j;
+        }
+      }
+      if (bits) atomicOr(&sm.near[win % 3], bits);
+      if (pt == 0) sm.near[(win + 1) % 3] = 0u;
+      fv_bar_sync(FV_BAR_PROD, FV_PROD);
+      const unsigned mask = sm.near[win % 3];
+      ++win;
+      // the stage's atoms (the same on every producer)
+      Member mem[GA];
+      int ng = 0, tot = 0, next = a + wn;
+      bool big = false;
+      for (int j = 0; j < wn; ++j) {
+        if (!((mask >> j) & 1u)) continue;
+        Member m = member(a + j);
+        if (m.nfa > FV_KC) {
+          if (ng == 0) {
+            mem[0] = m;
+            ng = 1;
+            big = true;
+            next = a + j + 1;
+          } else {
+            next = a + j;
+          }
+          break;
+        }
+        if (tot + m.nfa > FV_KC) {
+          next = a + j;
+          break;
+        }
+        m.off = tot;
+        tot += m.nfa;
+        mem[ng++] = m;
+      }
+      a = next;
+      if (ng == 0) continue;
+      if (big) {
+        const Member& m = mem[0];
+        const int nlc = m.nc0 + m.nc1 + m.nc2;
+        fetch_coef(qi, min(FV_KC, m.nfa), (min(FV_KC, m.nfa) + 3) & ~3, [&](int fi) { return m.boff + fi; });
+        exps(0, m);
+        fv_bar_sync(FV_BAR_PROD, FV_PROD);
+        for (int f0 = 0; f0 < m.nfa; f0 += FV_KC) {
+          const int nfc = min(FV_KC, m.nfa - f0), kp = (nfc + 3) & ~3;
+          const int b = qi & 1;
+          if (f0 > 0) fetch_coef(qi, nfc, kp, [&](int fi) { return m.boff + f0 + fi; });
+          begin(b);
+          double* As_b = &sm.As[b][0][0];
+          for (int e = pt; e < S::BP * nlc; e += FV_PROD) item(0, m, e / S::BP, e % S::BP, f0, As_b, nfc);
+          pad_rows(b, nfc, kp);
+          cp_wait<0>();  // this thread's coefficient copies have landed
+          finish(b, kp);
+        }
+        continue;
+      }
+      const int kp = (tot + 3) & ~3;
+      fetch_coef(qi, tot, kp, [&](int fi) {
+        int k = 0;
+        while (k + 1 < ng && fi >= mem[k + 1].off) ++k;
+        return mem[k].boff + fi - mem[k].off;
+      });
+      for (int k = 0; k < ng; ++k) exps(k, mem[k]);
+      fv_bar_sync(FV_BAR_PROD, FV_PROD);
+      const int b = qi & 1;
+      begin(b);
+      double* As_b = &sm.As[b][0][0];
+      // all members' items in one range, so that every producer has work
+      int start[GA + 1];
+      start[0] = 0;
+      for (int k = 0; k < ng; ++k) start[k + 1] = start[k] + S::BP * (mem[k].nc0 + mem[k].nc1 + mem[k].nc2);
+      for (int e = pt; e < start[ng]; e += FV_PROD) {
+        int k = 0;
+        while (e >= start[k + 1]) ++k;
+        const int r = e - start[k];
+        item(k, mem[k], r / S::BP, r % S::BP, 0, As_b, tot);
+      }
+      pad_rows(b, tot, kp);
+      cp_wait<0>();
+      finish(b, kp);
     }
     // end marker, then release of the last two stages
     {

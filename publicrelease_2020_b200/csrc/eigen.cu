@@ -24,7 +24,6 @@ constexpr int EIG_THREADS = 1024;
 constexpr int EIG_MAX_N = 1024;          // pairs held in shared memory: EIG_MAX_N / 2
 constexpr int EIG_SMEM_MAX_N = 160;      // matrix in shared memory up to 160 x 161 doubles (206 KB)
 constexpr int EIG_MAX_SWEEPS = 60;
-constexpr int EIG_ILP = 4;                // element pairs of Vt in flight per thread
 
 // A(i, j) at A[i * (n + 1) + j]: the odd pitch spreads a column over the
 // shared-memory banks.  The rotations are accumulated transposed, Vt(m, k) =
@@ -74,37 +73,20 @@ k_sym_eigen(int n, const double* __restrict__ ain, double* __restrict__ aglob, d
         rs[k] = s;
       }
       __syncthreads();
-      // rows p, q of A (A <- J^T A) and of Vt (V <- V J); the Vt rows live in
-      // L2, so each thread loads EIG_ILP element pairs before it stores any
-      for (int e0 = tid; e0 < half * n; e0 += nt * EIG_ILP) {
-        double vx[EIG_ILP], vy[EIG_ILP];
-#pragma unroll
-        for (int u = 0; u < EIG_ILP; ++u) {
-          const int e = e0 + u * nt;
-          vx[u] = vy[u] = 0.0;
-          if (e < half * n) {
-            const int k = e / n, j = e - k * n;
-            if (rs[k] != 0.0) {
-              vx[u] = vt[rp[k] * n + j];
-              vy[u] = vt[rq[k] * n + j];
-            }
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < EIG_ILP; ++u) {
-          const int e = e0 + u * nt;
-          if (e >= half * n) continue;
-          const int k = e / n, j = e - k * n;
-          const double s = rs[k];
-          if (s == 0.0) continue;
-          const double c = rc[k];
-          const int p = rp[k], q = rq[k];
-          const double x = A[p * ld + j], y = A[q * ld + j];
-          A[p * ld + j] = c * x - s * y;
-          A[q * ld + j] = s * x + c * y;
-          vt[p * n + j] = c * vx[u] - s * vy[u];
-          vt[q * n + j] = s * vx[u] + c * vy[u];
-        }
+      // rows p, q of A (A <- J^T A) and of Vt (V <- V J)
+      for (int e = tid; e < half * n; e += nt) {
+        const int k = e / n, j = e - k * n;
+        const double s = rs[k];
+        if (s == 0.0) continue;
+        const double c = rc[k];
+        const int p = rp[k], q = rq[k];
+        double x = A[p * ld + j], y = A[q * ld + j];
+        A[p * ld + j] = c * x - s * y;
+        A[q * ld + j] = s * x + c * y;
+        x = vt[p * n + j];
+        y = vt[q * n + j];
+        vt[p * n + j] = c * x - s * y;
+        vt[q * n + j] = s * x + c * y;
       }
       __syncthreads();
       // columns p, q of A (A <- A J); lanes run over rows i

@@ -124,6 +124,24 @@ int flosic_sic_mgga_mixin(flosic_ctx* ctx, int lspx, int iorbx, double* mixin);
 enum { FLOSIC_PRECISION_FP64 = 0, FLOSIC_PRECISION_MIXED = 1 };
 int flosic_sic_set_precision(flosic_ctx* ctx, int mode);
 
+/* Route of the FO density that enters the SIC exchange-correlation.
+   FLOSIC_DENSITY_PHI2 (default): rho = phi^2 with its derivatives, formed from
+   the FO values on the mesh.
+   FLOSIC_DENSITY_PAIRS: the reference's own route (poisson1.f:849-948, with
+   the pair polynomials of gtdncf.F:5-1113), which replaces the density the
+   reference's POISSON1 accumulates into RHOG for APOTNL_SIC
+   (apotnl_sic.F:232-430): each Poisson call adds its Gaussian pairs' density
+   polynomials at the mesh points inside its RCUT sphere only, dropping
+   polynomial coefficients of magnitude <= 1e-14.  It differs from phi^2 by
+   that truncation (the density tails far from every call centre) and by the
+   pairs the plan screens out (coupot_sic.F:228-315); gradient-corrected and
+   especially meta-GGA energies amplify the difference at low density.  Costs
+   one more pass over the near (pair, point) work of the Coulomb evaluation,
+   in FP64 whatever the precision mode.  Changing the route invalidates the
+   cached potentials. */
+enum { FLOSIC_DENSITY_PHI2 = 0, FLOSIC_DENSITY_PAIRS = 1 };
+int flosic_sic_set_density_mode(flosic_ctx* ctx, int mode);
+
 /* Poll limit of every wait between the roles of the mixed-precision
    tensor-core Coulomb kernel (no counterpart in the reference).  Each wait on
    a pipeline barrier gives up after `polls` polls (polls <= 0: the default,

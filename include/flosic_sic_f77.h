@@ -57,6 +57,7 @@ void flosic_sic_mgga_mixin_(const int64_t* ctx, const int32_t* lspx, const int32
                             int32_t* ierr);
 void flosic_sic_set_precision_(const int64_t* ctx, const int32_t* mode, int32_t* ierr);
 void flosic_sic_set_wait_limit_(const int64_t* ctx, const int64_t* polls, int32_t* ierr);
+void flosic_sic_set_density_mode_(const int64_t* ctx, const int32_t* mode, int32_t* ierr);
 void flosic_sic_autotune_(const int64_t* ctx, const int32_t* reps, int32_t* perfo_fos, float* ms,
                           int32_t* ierr);
 void flosic_sic_getvlxc_device_(const int64_t* ctx, const int32_t* npts, const int64_t* d_rhog,

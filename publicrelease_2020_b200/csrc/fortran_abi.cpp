@@ -95,6 +95,10 @@ void flosic_sic_set_wait_limit_(const int64_t* ctx, const int64_t* polls, int32_
   *ierr = flosic_sic_set_wait_limit(handle(ctx), *polls);
 }
 
+void flosic_sic_set_density_mode_(const int64_t* ctx, const int32_t* mode, int32_t* ierr) {
+  *ierr = flosic_sic_set_density_mode(handle(ctx), *mode);
+}
+
 void flosic_sic_autotune_(const int64_t* ctx, const int32_t* reps, int32_t* perfo_fos, float* ms, int32_t* ierr) {
   *ierr = flosic_sic_autotune(handle(ctx), *reps, perfo_fos, ms);
 }

@@ -815,7 +815,8 @@ __device__ __forceinline__ void block_reduce_parts(double v[NPART], double* out)
 }
 
 // Per (point, FO k): the FO density channels from phi (1, 4 or 10 channels:
-// value, gradient, second derivatives), the XC potential, the SIC potential
+// value, gradient, second derivatives) or, when rhog is given, the
+// reference-route channels read from it, the XC potential, the SIC potential
 // V = V_xc + V_H, Y = w V phi for the SIC matrix and the energy partials.  For
 // SCAN (mgga) also tau = |grad phi|^2/2 and the Hamiltonian ingredients Z of
 // call_mgga.f90, which enter the SIC matrix through four Y channels
@@ -826,6 +827,7 @@ __device__ __forceinline__ void block_reduce_parts(double v[NPART], double* out)
 template <bool MGGA>
 __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, int nspn, XCParams xp,
                                                    const double* __restrict__ phi, int ldp,
+                                                   const double* __restrict__ rhog,
                                                    double* __restrict__ vh, double* __restrict__ vpot,
                                                    double* __restrict__ y, double* __restrict__ part, int nblk) {
   const int k = blockIdx.y;
@@ -846,6 +848,10 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, 
       for (int ch = 1; ch < 4; ++ch) f[ch] = phi[((size_t)ch * nfo + k) * ldp + p];
 #pragma unroll
       for (int d = 1; d <= 3; ++d) r[d] = 2 * f[0] * f[d];
+      if (rhog) {
+#pragma unroll
+        for (int d = 0; d < 4; ++d) r[d] = rhog[((size_t)d * nfo + k) * ldp + p];
+      }
       const double tau = 0.5 * (f[1] * f[1] + f[2] * f[2] + f[3] * f[3]);
       const size_t kp = (size_t)k * M.n + p;
       const size_t cs = (size_t)nfo * M.n;  // Y channel stride
@@ -885,6 +891,9 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, 
     } else {
       for (int d = 1; d < 10; ++d) r[d] = 0.0;
     }
+    if (rhog) {
+      for (int d = 0; d < (gga ? 10 : 1); ++d) r[d] = rhog[((size_t)d * nfo + k) * ldp + p];
+    }
     const size_t kp = (size_t)k * M.n + p;
     const double coul = vh[kp] * fnspn / 2.0;
     vh[kp] = coul;
@@ -910,15 +919,15 @@ __global__ void __launch_bounds__(XC_THREADS) k_xc(MeshDev M, int nfo, int gga, 
 }
 
 void launch_xc(const MeshDev& M, int nfo, int gga, int mgga, int nspn, const int* xc, const double* phi, int ldp,
-               double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st) {
+               const double* rhog, double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st) {
   XCParams xp;
   xp.igga[0] = xc[0];
   xp.idftyp[0] = xc[1];
   xp.igga[1] = xc[2];
   xp.idftyp[1] = xc[3];
   dim3 grid(nblk, nfo);
-  if (mgga) k_xc<true><<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
-  else k_xc<false><<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, vh, vpot, y, part, nblk);
+  if (mgga) k_xc<true><<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, rhog, vh, vpot, y, part, nblk);
+  else k_xc<false><<<grid, XC_THREADS, 0, st>>>(M, nfo, gga, nspn, xp, phi, ldp, rhog, vh, vpot, y, part, nblk);
 }
 
 // Compensated (Neumaier) sums of the block partials, in block order.

@@ -145,8 +145,10 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
 // writes the SIC potential V = Vxc + VH*nspn/2 and Y = w V phi, and per-block
 // energy partial sums part[(k*nblk + blk)*NPART + j].
 constexpr int NPART = 11;
+// rhog (may be null): density channels rhog[(ch*nfo + k)*ldp + p] to use in
+// place of those formed from phi (the reference's pair-route density).
 void launch_xc(const MeshDev& M, int nfo, int gga, int mgga, int nspn, const int* xc, const double* phi, int ldp,
-               double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st);
+               const double* rhog, double* vh, double* vpot, double* y, double* part, int nblk, cudaStream_t st);
 void launch_reduce_parts(int nfo, int nblk, const double* part, double* sums, cudaStream_t st);
 
 // FO density channels of one FO: rhog[ch*ldr + p] (10 channels for GGA).
@@ -181,6 +183,16 @@ bool launch_sym_eigen(int n, const double* a, double* work, double* w, double* v
 cudaError_t preload_xc_rhog();
 void launch_xc_rhog(const MeshDev& M, int gga, const int* xc, const double* rhog, int ldr, double* vxc,
                     double* part, int nblk, cudaStream_t st);
+
+// FO densities by the reference's route (csrc/density.cu): nch channels (1,
+// 4 or 10) of each of nfo FOs, rhog[(ch*nfo + k)*ldr + p] over the mesh M,
+// from the pairs of every call at the points inside the call's RCUT sphere
+// (poisson1.f:849-948).  u: the FOs' primitive projections; cfo: the calls'
+// per-FO geometry; dc: npairs*nfo*pair_density_ld(nch) doubles of scratch.
+int pair_density_ld(int nch);
+void launch_pair_density(int npairs, const PairGeo* pairs, int ncalls, const CallInfo* calls, const CallFO* cfo,
+                         int nfo, int nprim, const double* u, int nch, const MeshDev& M, double* dc, double* rhog,
+                         size_t ldr, cudaStream_t st);
 
 void upload_constants(const double* leb_ang, const double* leb_w);
 

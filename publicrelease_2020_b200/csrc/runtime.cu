@@ -287,9 +287,11 @@ struct SpinCache {
   DevBuf<double> vh;           // raw Coulomb [k][P]
   DevBuf<double> vpot;         // SIC potential [k][P]
   DevBuf<double> y;            // w V phi [k][P]
+  DevBuf<double> rhog;         // pair-route density channels [ch][k][P] (FLOSIC_DENSITY_PAIRS)
   CoulBufs bc;                 // batched Coulomb launch only
   void release() {
     bc.release();
+    rhog.release();
     cfo.release();
     phi.release();
     vh.release();
@@ -355,6 +357,8 @@ struct flosic_ctx {
   DevBuf<float> d_coef_hl, d_momv_hl;
   CoulombConfig coulomb_cfg;     // FLOSIC_COULOMB=perfo, FLOSIC_SHARED=mma, FLOSIC_PERFO_WM=1|2|4 (A/B checks)
   int precision = FLOSIC_PRECISION_FP64;
+  int density = FLOSIC_DENSITY_PHI2;
+  DevBuf<double> d_dens_coef;    // pair-route density polynomials of one spin (FLOSIC_DENSITY_PAIRS)
   DevBuf<unsigned long long> d_cnt;
   unsigned long long work_near = 0, work_far = 0, work_terms = 0;
   DevBuf<CallFO> d_callfo;
@@ -801,6 +805,23 @@ void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
   CUDA_CHECK(cudaGetLastError());
 }
 
+// FLOSIC_DENSITY_PAIRS: the FO densities of spin s by the reference's route,
+// from the Gaussian pairs of every POISSON1 call at the points inside its RCUT
+// sphere (poisson1.f:849-948), into S.rhog; the primitive projections in d_u
+// and the calls' per-FO geometry cfo must be those of spin s.
+void pair_density(flosic_ctx* c, int s, const CallFO* cfo) {
+  if (c->density != FLOSIC_DENSITY_PAIRS) return;
+  SpinCache& S = c->spin[s];
+  const int nf = S.nf, P = c->eval_n, nch = c->nch();
+  const int npairs = (int)c->pairs.size(), ncalls = (int)c->calls.size();
+  c->d_dens_coef.ensure((size_t)std::max(npairs, 1) * nf * pair_density_ld(nch));
+  S.rhog.ensure((size_t)nch * nf * P);
+  launch_pair_density(npairs, c->d_pairs.p, ncalls, c->d_calls.p, cfo, nf, c->nprim, c->d_u.p, nch, c->eval_mesh(),
+                      c->d_dens_coef.p, S.rhog.p, (size_t)P, c->st);
+  CUDA_CHECK(cudaGetLastError());
+  c->launches += 2;
+}
+
 // COUPOT_SIC's Coulomb part for the FOs of spin s.
 void coulomb(flosic_ctx* c, int s) {
   SpinCache& S = c->spin[s];
@@ -835,6 +856,7 @@ void spin_potentials(flosic_ctx* c, int s) {
   CUDA_CHECK(cudaEventRecord(c->ev[7], st));
   coulomb(c, s);
   CUDA_CHECK(cudaEventRecord(c->ev[4], st));
+  pair_density(c, s, c->d_callfo.p);  // FLOSIC_DENSITY_PAIRS only; timed with XC
   spin_xc(c, s);
   c->stage_ms[0] += elapsed(c->ev[0], c->ev[1]);
   c->stage_ms[1] += elapsed(c->ev[1], c->ev[7]);
@@ -858,7 +880,8 @@ void spin_xc(flosic_ctx* c, int s) {
   // XC reads the raw Coulomb potential; keep a scaled copy out of place
   c->d_tmp.ensure((size_t)nf * P);
   CUDA_CHECK(cudaMemcpyAsync(c->d_tmp.p, S.vh.p, sizeof(double) * nf * P, cudaMemcpyDeviceToDevice, st));
-  launch_xc(c->eval_mesh(), nf, c->gga, c->mgga, c->nspn, c->xc, S.phi.p, P, c->d_tmp.p, S.vpot.p, S.y.p,
+  const double* rhog = c->density == FLOSIC_DENSITY_PAIRS ? S.rhog.p : nullptr;
+  launch_xc(c->eval_mesh(), nf, c->gga, c->mgga, c->nspn, c->xc, S.phi.p, P, rhog, c->d_tmp.p, S.vpot.p, S.y.p,
             c->d_part.p, nblk, st);
   launch_reduce_parts(nf, nblk, c->d_part.p, c->d_sums.p, st);
   c->launches += 2;
@@ -1137,6 +1160,7 @@ CoulombJob batch_prepare(flosic_ctx* c, int s) {
   CoulombScratch scr{B.pairfmt.p, B.share.p, B.lists.p, nullptr, nullptr, nullptr};
   launch_coulomb_classify(ncalls, npairs, nf, B.maxfmt.p, B.callfo.p, scr, false, st);
   c->launches += 6;
+  pair_density(c, s, B.callfo.p);
   S.vh.ensure((size_t)nf * P);
   CoulombJob J{};
   J.ncalls = ncalls;
@@ -1262,7 +1286,7 @@ int flosic_sic_destroy(flosic_ctx* c) {
   c->d_sic.release(); c->d_tmp.release(); c->d_maxfmt.release(); c->d_callfo.release(); c->d_cnt.release(); c->d_pairfmt.release();
   c->d_share.release(); c->d_lists.release(); c->d_setup_list.release();
   c->d_eig_a.release(); c->d_eig_w.release(); c->d_eig_v.release(); c->d_eig_work.release(); c->d_eig_info.release();
-  c->d_coef_hl.release(); c->d_momv_hl.release(); c->d_tc_err.release();
+  c->d_coef_hl.release(); c->d_momv_hl.release(); c->d_tc_err.release(); c->d_dens_coef.release();
   c->d_gemm_ws.release();
   c->d_jobs.release();
   c->d_items.release();
@@ -1560,10 +1584,17 @@ int flosic_sic_coupot_sic(flosic_ctx* c, int kxxs, int kxxo, double* coulomb, do
     const int P = c->nmsh, k = kxxo - 1;
     std::vector<double> v(P), r((size_t)10 * P, 0.0);
     CUDA_CHECK(cudaMemcpyAsync(v.data(), S.vh.p + (size_t)k * P, sizeof(double) * P, cudaMemcpyDeviceToHost, c->st));
-    c->d_tmp.ensure((size_t)10 * P);
-    launch_density(P, S.nf, k, c->nch(), S.phi.p, P, c->d_tmp.p, P, c->st);
-    const int nch = c->gga ? 10 : 1;  // the meta-GGA layout has 10 channels, 4..9 zero
-    CUDA_CHECK(cudaMemcpyAsync(r.data(), c->d_tmp.p, sizeof(double) * nch * P, cudaMemcpyDeviceToHost, c->st));
+    if (c->density == FLOSIC_DENSITY_PAIRS) {
+      // the channels POISSON1 accumulated (meta-GGA: 4, the rest of the 10-channel layout zero)
+      CUDA_CHECK(cudaMemcpy2DAsync(r.data(), sizeof(double) * P, S.rhog.p + (size_t)k * P,
+                                   sizeof(double) * P * S.nf, sizeof(double) * P, c->nch(), cudaMemcpyDeviceToHost,
+                                   c->st));
+    } else {
+      c->d_tmp.ensure((size_t)10 * P);
+      launch_density(P, S.nf, k, c->nch(), S.phi.p, P, c->d_tmp.p, P, c->st);
+      const int nch = c->gga ? 10 : 1;  // the meta-GGA layout has 10 channels, 4..9 zero
+      CUDA_CHECK(cudaMemcpyAsync(r.data(), c->d_tmp.p, sizeof(double) * nch * P, cudaMemcpyDeviceToHost, c->st));
+    }
     CUDA_CHECK(cudaStreamSynchronize(c->st));
     for (int i = 0; i < P; ++i) {
       const int o = c->perm[i];
@@ -1653,6 +1684,22 @@ int flosic_sic_set_wait_limit(flosic_ctx* c, int64_t polls) {
   return guarded([&] {
     if (!c) fail(FLOSIC_ERR_ARG, "null context");
     c->coulomb_cfg.wait_limit = polls > 0 ? (long long)polls : 0;
+  });
+}
+
+int flosic_sic_set_density_mode(flosic_ctx* c, int mode) {
+  return guarded([&] {
+    if (!c) fail(FLOSIC_ERR_ARG, "null context");
+    if (mode != FLOSIC_DENSITY_PHI2 && mode != FLOSIC_DENSITY_PAIRS) fail(FLOSIC_ERR_ARG, "unknown density mode");
+    if (mode != c->density) {
+      c->density = mode;
+      for (auto& s : c->spin) {
+        s.pot_valid = false;
+        s.sic_valid = false;
+        if (mode == FLOSIC_DENSITY_PHI2) s.rhog.release();
+      }
+      if (mode == FLOSIC_DENSITY_PHI2) c->d_dens_coef.release();
+    }
   });
 }
 

@@ -38,9 +38,10 @@ EXPORTS = [
     "flosic_sic_cycle_partial", "flosic_sic_cycle_combine", "flosic_sic_adjoint", "flosic_sic_mgga_mixin",
     "flosic_sic_siclag_der", "flosic_sic_sicham", "flosic_sic_densold", "flosic_sic_coupot1",
     "flosic_sic_autotune", "flosic_sic_adjoint_fod", "flosic_sic_set_wait_limit", "flosic_sic_batch_cycle",
-    "flosic_sic_kernel_stats",
+    "flosic_sic_kernel_stats", "flosic_sic_set_density_mode",
 ]
 PRECISION = {"fp64": 0, "mixed": 1}
+DENSITY = {"phi2": 0, "pairs": 1}
 
 _lib = None
 
@@ -73,6 +74,7 @@ def load_library(path=LIB_PATH):
     L.flosic_sic_getvlxc_mgga.argtypes = [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_set_precision.argtypes = [_vp, C.c_int]
     L.flosic_sic_set_wait_limit.argtypes = [_vp, C.c_int64]
+    L.flosic_sic_set_density_mode.argtypes = [_vp, C.c_int]
     L.flosic_sic_kernel_stats.argtypes = [_vp, _dp, _i64]
     L.flosic_sic_batch_cycle.argtypes = [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
     L.flosic_sic_autotune.argtypes = [_vp, C.c_int, _ip, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")]
@@ -198,6 +200,13 @@ class FlosicSIC:
     def set_precision(self, mode):
         """"fp64" (the drop-in, default) or "mixed"."""
         self._check(self.L.flosic_sic_set_precision(self.h, PRECISION[mode]))
+
+    def set_density_mode(self, mode):
+        """FO density route of the SIC exchange-correlation: "phi2" (default,
+        rho = phi^2 from the FO values) or "pairs" (the reference's POISSON1
+        route: Gaussian-pair polynomials at the points inside each call's RCUT
+        sphere, coefficients below 1e-14 dropped)."""
+        self._check(self.L.flosic_sic_set_density_mode(self.h, DENSITY[mode]))
 
     def set_wait_limit(self, polls):
         """Poll limit of the mixed-precision tensor-core kernel's pipeline waits

@@ -443,6 +443,8 @@ void build_pair_plan(flosic_ctx* c) {
   const int nspn = c->nspn;
   auto flush = [&](std::vector<PairGeo>& b, bool weird) {
     auto emit = [&](const PairGeo* first, int n) {
+      // the per-FO Coulomb kernel stages a call's pairs in MXPR shared slots
+      if (n > MXPR) fail(FLOSIC_ERR_CAPACITY, "Poisson call with more than MXPR pairs");
       CallInfo ci;
       ci.p0 = (int)pairs.size();
       ci.np = n;

@@ -268,6 +268,8 @@ def run_ours(args, rank, world, local_rank):
         ctx.set_shard(rank, world)
     ctx.set_geometry(sysm)
     ctx.set_orbitals(sysm.psi, sysm.nwfs, sysm.fods)
+    ctx.set_density_mode(args.density)
+    cfg["fo_density"] = args.density
     ld = ctx.ld
     if world > 1:
         from publicrelease_2020_b200.shard import sharded_cycle
@@ -598,6 +600,9 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2half", "c2tiny", "c2prof", "c3", "c4", "c5", "c5prof", "water",
                                                       "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--density", default="phi2", choices=["phi2", "pairs"],
+                    help="FO density route of the SIC XC: phi^2 from the FO values (default) or the "
+                         "reference's Gaussian-pair route at each Poisson call's near points")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the per-FO Coulomb kernel's default tile width instead of timing the candidates")
     args = ap.parse_args()

@@ -38,6 +38,9 @@ class _Ctx:
     def set_precision(self, mode):
         self.mode = mode
 
+    def set_density_mode(self, mode):
+        self.density = mode
+
     def autotune(self, reps=1):
         return 32, {32: 1.0}
 
@@ -139,11 +142,12 @@ def _check_line(line, steps):
 
 def test_single_system_line(fakes, capsys):
     args = types.SimpleNamespace(workload="water", steps=2, warmup=3, precision="both", no_autotune=False,
-                                 no_cpu_baseline=True)
+                                 no_cpu_baseline=True, density="phi2")
     bench.run_ours(args, 0, 1, 0)
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     _check_line(line, 2)
     assert line["config"]["autotune"]["mixed"]["perfo_fo_slots"] == 32
+    assert line["config"]["fo_density"] == "phi2"
     assert line["gpu_launches"] == 2 * 7
     kern = line["roofline"]["kernels"]
     assert set(kern) == {"k_coulomb_shared_tc", "k_coulomb_perfo"}   # mixed headline: TF32 shared kernel

@@ -243,6 +243,7 @@ def run_reference(args, rank, world):
             vals.append(v)
     value = float(np.mean(vals))
     cfg["parallelism"] = "host threads"
+    cfg["fo_density"] = "pairs"  # the reference's own route (poisson1.f), which the CPU port follows
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "strong",

@@ -3,7 +3,9 @@ PBE, NSPN=1), FP64 path through the C ABI, against the FP64 oracle's
 RESULTS(1:13) and SIC-matrix columns of the first four FOs
 (tests/golden/c2_full_results.npz, made by make_c2_full_golden.py: the oracle
 needs tens of CPU-minutes for them).  Tolerances as in test_parity_gpu.py:
-RESULTS to 1e-8 Ha, SIC-matrix entries to 1e-8 of the largest (GGA)."""
+RESULTS to 1e-8 Ha, SIC-matrix entries to 1e-8 of the largest (GGA).  With the
+reference's own FO density route selected (FLOSIC_DENSITY_PAIRS) the SIC-matrix
+columns are held to 1e-9 of the largest, as for the small systems."""
 import os
 
 import numpy as np
@@ -17,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = np.load(os.path.join(HERE, "golden", "c2_full_results.npz"))
 
 
-def test_c2_full_size_matches_oracle():
+@pytest.mark.parametrize("density,sic_rtol", [("phi2", 1e-8), ("pairs", 1e-9)])
+def test_c2_full_size_matches_oracle(density, sic_rtol):
     import sys
     sys.path.insert(0, os.path.join(HERE, "golden"))
     from make_c2_full_golden import system
@@ -26,6 +29,7 @@ def test_c2_full_size_matches_oracle():
     assert sysm.nmsh == int(GOLD["nmsh"]) and sysm.nbasis == int(GOLD["nbasis"])
     ctx = S.open_system(sysm)
     try:
+        ctx.set_density_mode(density)
         r = ctx.cycle()
     finally:
         ctx.close()
@@ -36,4 +40,5 @@ def test_c2_full_size_matches_oracle():
     assert np.max(np.abs(g[:, 1:] - gold[:, 1:])) < 1e-8, np.abs(g[:, 1:] - gold[:, 1:]).max(axis=0)
     n = int(GOLD["nfo"])
     lam = r["sic"][0][:nfo, :n]            # [l][j] = SIC(j, l), columns l < nfo
-    assert np.max(np.abs(lam - cols)) < 1e-8 * np.abs(cols).max()
+    err = np.max(np.abs(lam - cols)) / np.abs(cols).max()
+    assert err < sic_rtol, (density, err, np.abs(g[:, 1:] - gold[:, 1:]).max(axis=0))

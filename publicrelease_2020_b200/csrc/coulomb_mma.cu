@@ -930,11 +930,11 @@ void launch_coulomb_batch(const CoulombJob* jobs, const int4* items, int nitems,
   else launch_batch_wm<1>(jobs, items, nitems, counters, mixed, boys_tab, nctas, st);
 }
 
-void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
-                        const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
-                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
-                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaEvent_t mid,
-                        cudaStream_t st) {
+cudaError_t launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
+                               const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
+                               const MeshDev& M, const double* boys_tab, double* vh, int ldv,
+                               const CoulombConfig& cfg, bool mixed, const CoulombScratch& scr,
+                               unsigned long long* cnt, cudaEvent_t mid, cudaStream_t st) {
   const bool per_fo_only = cfg.per_fo_only;
   unsigned long long* cnt_perfo = cnt + 3;  // the per-FO kernel counts apart from the shared-geometry one
   launch_coulomb_classify(ncalls, npairs, nfo, maxfmt, cfo, scr, per_fo_only, st);
@@ -942,8 +942,10 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
     const size_t nc = (size_t)npairs * nfo * COEF_LD, nm = (size_t)ncalls * nfo * MOM_LD;
     launch_split_tf32((size_t)npairs, nfo, coef, scr.coef_hl, st);
     launch_split_tf32((size_t)ncalls, nfo, momv, scr.momv_hl, st);
-    launch_coulomb_shared_tc(ncalls, scr.lists, scr.share, calls, nfo, scr.coef_hl, nc, scr.pair_fmt, pairs,
-                             scr.momv_hl, nm, M, boys_tab, vh, ldv, cnt, scr.err, cfg.wait_limit, st);
+    const cudaError_t e = launch_coulomb_shared_tc(ncalls, scr.lists, scr.share, calls, nfo, scr.coef_hl, nc,
+                                                   scr.pair_fmt, pairs, scr.momv_hl, nm, M, boys_tab, vh, ldv, cnt,
+                                                   scr.err, cfg.wait_limit, st);
+    if (e != cudaSuccess) return e;
   } else if (!per_fo_only) {
     if (nfo > 64)
       launch_shared<4>(ncalls, scr.lists, scr.share, calls, nfo, coef, scr.pair_fmt, pairs, momv, M, boys_tab, vh,
@@ -967,6 +969,7 @@ void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs,
   else
     launch_perfo<1>(ncalls, scr.lists, acc, calls, pairs, nfo, coef, scr.pair_fmt, cfo, momv, M, boys_tab, vh, ldv,
                     cnt_perfo, mixed, st);
+  return cudaGetLastError();
 }
 
 }  // namespace flosic

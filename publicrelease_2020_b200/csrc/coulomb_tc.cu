@@ -19,22 +19,29 @@
 //                shared memory (one coalesced load each, tile class computed
 //                once), then walk them; both producers of a point follow the
 //                operand windows, the owner of each segment (alternating)
-//                writes its B rows (its point) and copies its A rows (FO pt)
+//                writes its B rows (its point); eight producer threads, one per
+//                4-row position of a window, load the A rows of all 128 FOs of
+//                every chunk with one TMA tiled copy each (cp.async.bulk.tensor:
+//                the hi and lo parts, 2 KB each, side by side)
 // Operand windows (32 K rows; hi and lo parts of A and B; 64 KB) are triple
-// buffered in shared memory in the no-swizzle K-major core-matrix layout (8 rows
-// x 16 bytes per core matrix).  Hand-over: mbarriers full/empty per window
-// buffer (the A-row copies complete on it by cp.async.mbarrier.arrive, so no
-// producer waits for its own copies), accfull/accempty per accumulator, done at
-// the end of the tile; every
+// buffered in shared memory in a no-swizzle K-major core-matrix layout (8 rows
+// x 16 bytes per core matrix) whose 4-column chunks are 2 KB blocks of all 128
+// rows, so that one TMA box lands as one chunk.  Hand-over: mbarriers full (the
+// producers' stores) and tma (the copies' transaction bytes) per window buffer,
+// empty per window buffer, accfull/accempty per accumulator, done at the end of
+// the tile; every
 // wait has an iteration limit after which the CTA sets an abort flag, drains its
 // copies and MMAs, frees tensor memory and returns with an error flag set.
+#include <algorithm>
+
+#include <cuda.h>
+
 #include "coulomb_common.cuh"
 
 namespace flosic {
 
 constexpr int TC_THREADS = 512;
 constexpr int TC_KW = 32;                // K rows per operand window
-constexpr int TC_KG = TC_KW / 4;         // core matrices along K
 constexpr int TC_NB = 3;                 // window buffers
 constexpr int TC_FLUSH = 2;              // windows per FP32 accumulation group
 constexpr int TC_EPI0 = 4;               // first epilogue warp
@@ -53,20 +60,23 @@ struct TcCall {
 };
 
 struct TcSmem {
-  float A[TC_NB][2][TILE * TC_KW];  // [buffer][hi, lo] FO rows x K
+  float A[TC_NB][TC_KW / 4][2][TILE * 4];  // [buffer][4-column chunk][hi, lo] FO rows x 4 columns
   float B[TC_NB][2][TILE * TC_KW];  // [buffer][hi, lo] point rows x K
   double px[TILE], py[TILE], pz[TILE];
   TcCall calls[TC_NSTAGE];
-  uint64_t full[TC_NB], empty[TC_NB], accfull[2], accempty[2], done, drain;
+  uint64_t full[TC_NB], tma[TC_NB], empty[TC_NB], accfull[2], accempty[2], done, drain;
   int win_rows[TC_NB], win_last[TC_NB];
   int ngroups;
   uint32_t tmem;
   int abort;
 };
 
-// Float offset of (row, k) in the no-swizzle K-major core-matrix layout.
+// Float offset of (row, k) in the no-swizzle K-major core-matrix layout: core
+// matrices (8 rows x 4 columns, 128 bytes) of one 4-column chunk follow each
+// other over the 128 rows (SBO 128 bytes), chunks follow each other (LBO 2 KB).
+constexpr int TC_CHUNK = TILE * 4;  // floats of one 4-column chunk of all rows
 __device__ __forceinline__ int cm_off(int row, int k) {
-  return ((row >> 3) * TC_KG + (k >> 2)) * 32 + (row & 7) * 4 + (k & 3);
+  return (k >> 2) * TC_CHUNK + (row >> 3) * 32 + (row & 7) * 4 + (k & 3);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -108,10 +118,18 @@ __device__ __forceinline__ bool mbar_wait_drain(uint64_t* b, uint32_t parity) {
   return false;
 }
 
-// Arrive on b once every cp.async this thread has issued so far has landed
-// (the barrier's expected count includes this arrival).
-__device__ __forceinline__ void cp_async_arrive(uint64_t* b) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(b)) : "memory");
+// Expect `bytes` more transaction bytes on b in its current phase.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+// TMA tiled load of the box at (0, y, z, w) of a 4-D tensor map into shared
+// memory; its bytes complete on b.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int y, int z, int w, uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(z), "r"(w), "r"(smem_u32(b))
+      : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -278,9 +296,9 @@ __device__ __forceinline__ void h_values_kf(float (&v)[KSEG], int kf, float dx, 
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* __restrict__ share,
-                    const CallInfo* __restrict__ calls, int nfo, const float* __restrict__ coef_hl,
+                    const CallInfo* __restrict__ calls, int nfo, const __grid_constant__ CUtensorMap tm_coef,
                     const int8_t* __restrict__ pair_fmt, const PairGeo* __restrict__ pairs,
-                    const float* __restrict__ momv_hl, size_t coef_part, size_t mom_part, MeshDev M,
+                    const __grid_constant__ CUtensorMap tm_mom, MeshDev M,
                     const double* __restrict__ boys_tab, double* __restrict__ vh, int ldv,
                     unsigned long long* __restrict__ cnt, int* __restrict__ err, long wait_limit) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -300,7 +318,8 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
   }
   if (tid == 0) {
     for (int b = 0; b < TC_NB; ++b) {
-      mbar_init(&S.full[b], 2 * TC_NPROD);  // per producer: its stores, and its cp.async copies
+      mbar_init(&S.full[b], TC_NPROD);  // per producer: its stores
+      mbar_init(&S.tma[b], TC_KW / 4);  // the 8 loading threads, plus the copies' transaction bytes
       mbar_init(&S.empty[b], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -338,37 +357,47 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
       hi[d] = M.tile_hi[3 * tile + d];
     }
     const double x = S.px[p], y = S.py[p], z = S.pz[p];
+    // eight threads (two per warp of the second producer half) load the A
+    // chunks: the one of window position tma_pos loads every chunk that lands
+    // there, and arrives once per window on the window's tma barrier
+    const int tma_pos = (half == 1 && (pt & 15) == 0) ? (pt >> 4) : -1;
     int w = 0, fill = 0, buf = 0;
-    bool open = false, ok = true;
+    bool open = false, ok = true, open_ok = false;  // open_ok: this thread's wait for the open window succeeded
     auto win_open = [&]() {
       buf = w % TC_NB;
-      if (w >= TC_NB && !mbar_wait(&S.empty[buf], (uint32_t)((w / TC_NB - 1) & 1), abort, wait_limit)) ok = false;
+      open_ok = w < TC_NB || mbar_wait(&S.empty[buf], (uint32_t)((w / TC_NB - 1) & 1), abort, wait_limit);
+      if (!open_ok) ok = false;
       fill = 0;
       open = true;
     };
     auto win_close = [&](int rows, int last) {
       // the thread's own st.shared become visible to the tensor core (async
-      // proxy); its cp.async copies arrive on the barrier when they land
+      // proxy); the A chunks' TMA copies complete on the window's tma barrier
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       if (pt == 0 && half == 0) {
         S.win_rows[buf] = rows;
         S.win_last[buf] = last;
       }
-      cp_async_arrive(&S.full[buf]);
+      if (tma_pos >= 0) mbar_arrive(&S.tma[buf]);
       mbar_arrive(&S.full[buf]);
       ++w;
       open = false;
     };
-    // one segment: B rows of this point (v, rows; zeros when !live) and A rows
-    // of FO pt from src
-    const size_t cstride = (size_t)nfo * 4;  // floats between the 4-row chunks of one A row
-    auto emit = [&](const float (&v)[KSEG], bool mine, bool live, int rows, const float* src, size_t part) {
+    // one segment: B rows of this point (v, rows; zeros when !live), and, by the
+    // loading thread of each chunk's window position, the A rows of the block's
+    // 128 FOs from chunk z0 of map tm
+    auto emit = [&](const float (&v)[KSEG], bool mine, bool live, int rows, const CUtensorMap* tm, int z0) {
 #pragma unroll
       for (int j4 = 0; j4 < KSEG / 4; ++j4) {
         if (4 * j4 >= rows || !ok) break;
         if (!open) {
           win_open();
           if (!ok) break;
+        }
+        if (tma_pos == (fill >> 2)) {
+          // one box = the chunk's hi and lo parts, which lie next to each other
+          mbar_expect_tx(&S.tma[buf], 2u * TC_CHUNK * (uint32_t)sizeof(float));
+          tma_load_4d(S.A[buf][fill >> 2][0], tm, k0, z0 + j4, 0, &S.tma[buf]);
         }
         const int o = cm_off(p, fill);
         if (!mine) {
@@ -382,11 +411,6 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
         } else {
           *reinterpret_cast<float4*>(&S.B[buf][0][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
           *reinterpret_cast<float4*>(&S.B[buf][1][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        if (mine && src) {
-          const int oa = cm_off(pt, fill);
-          cp_async16(&S.A[buf][0][oa], src + j4 * cstride);
-          cp_async16(&S.A[buf][1][oa], src + part + j4 * cstride);
         }
         fill += 4;
         if (fill == TC_KW) win_close(TC_KW, 0);
@@ -441,8 +465,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
                 g_values(v, pg.C[0], pg.C[1], pg.C[2], pg.delta, x, y, z, kn, boys_tab);
               }
             }
-            const float* src = pt < nk ? coef_hl + ((size_t)q * (KSEG / 4) * nfo + k0 + pt) * 4 : nullptr;
-            emit(v, mine, nr, kn, src, coef_part);
+            emit(v, mine, nr, kn, &tm_coef, q * (KSEG / 4));
           }
         }
         if (e.cls != 0) {  // far segment (NPOT=2)
@@ -460,8 +483,7 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
               const float dx = (float)(x - e.cx), dy = (float)(y - e.cy), dz = (float)(z - e.cz);
               h_values_kf(v, e.kf, dx, dy, dz, dx * dx + dy * dy + dz * dz);
             }
-            const float* src = pt < nk ? momv_hl + ((size_t)e.c * (KSEG / 4) * nfo + k0 + pt) * 4 : nullptr;
-            emit(v, mine, fr, e.kf, src, mom_part);
+            emit(v, mine, fr, e.kf, &tm_mom, e.c * (KSEG / 4));
           }
         }
       }
@@ -476,26 +498,41 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
           const int o = cm_off(p, fill);
           *reinterpret_cast<float4*>(&S.B[buf][0][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
           *reinterpret_cast<float4*>(&S.B[buf][1][o]) = make_float4(0.f, 0.f, 0.f, 0.f);
-          const int oa = cm_off(pt, fill);
-          *reinterpret_cast<float4*>(&S.A[buf][0][oa]) = make_float4(0.f, 0.f, 0.f, 0.f);
-          *reinterpret_cast<float4*>(&S.A[buf][1][oa]) = make_float4(0.f, 0.f, 0.f, 0.f);
+          *reinterpret_cast<float4*>(&S.A[buf][fill >> 2][0][4 * pt]) = make_float4(0.f, 0.f, 0.f, 0.f);
+          *reinterpret_cast<float4*>(&S.A[buf][fill >> 2][1][4 * pt]) = make_float4(0.f, 0.f, 0.f, 0.f);
           }
           fill += 4;
         }
         win_close(fill, 1);
       }
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy of this thread is left in flight
+    if (tma_pos >= 0) {
+      // every copy lands before the tile ends: a loading thread whose wait for
+      // a window left open by an abort succeeded takes its part of that
+      // window's phase (the buffer's previous phase has completed), then waits
+      // for the last phase of each buffer (the earlier ones completed before
+      // their buffer was reused); a phase that a failed wait left incomplete
+      // ends this wait at its limit
+      int wl = w;
+      if (open && open_ok) {
+        mbar_arrive(&S.tma[buf]);
+        wl = w + 1;
+      }
+      for (int j = max(0, wl - TC_NB); j < wl; ++j)
+        if (!mbar_wait_drain(&S.tma[j % TC_NB], (uint32_t)((j / TC_NB) & 1))) *abort = 1;
+    }
   } else if (warp == 0) {
     // ---------------- MMA issue
     if (lane == 0) {
       constexpr uint32_t idesc = tf32_idesc(TILE, TILE);
-      constexpr uint32_t LBO = 128, SBO = TC_KG * 128;
+      // B: chunks of one part follow each other (2 KB); A: a chunk's hi and lo
+      // parts lie together, so its chunks are 4 KB apart
+      constexpr uint32_t LBO = TC_CHUNK * sizeof(float), LBO_A = 2 * LBO, SBO = 128;
       int a = 0, nin = 0, g = 0;
       for (int w = 0;; ++w) {
         const int b = w % TC_NB;
         if (!mbar_wait(&S.full[b], (uint32_t)((w / TC_NB) & 1), abort, wait_limit)) break;
-        // the window's cp.async data (generic proxy) is read by the tensor core
+        if (!mbar_wait(&S.tma[b], (uint32_t)((w / TC_NB) & 1), abort, wait_limit)) break;
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         tc_fence_after();
         const int r = S.win_rows[b], last = S.win_last[b];
@@ -505,12 +542,12 @@ k_coulomb_shared_tc(int ncalls, const int* __restrict__ lists, const CallShare* 
             tc_fence_after();
           }
           const uint32_t d = tmem + (uint32_t)(a * TILE);
-          const uint32_t ah = smem_u32(S.A[b][0]), al = smem_u32(S.A[b][1]);
+          const uint32_t ah = smem_u32(S.A[b][0][0]), al = smem_u32(S.A[b][0][1]);
           const uint32_t bh = smem_u32(S.B[b][0]), bl = smem_u32(S.B[b][1]);
           for (int ks = 0; ks < r / 8; ++ks) {
-            const uint32_t off = (uint32_t)ks * 256u;
-            const uint64_t dah = smem_desc(ah + off, LBO, SBO), dal = smem_desc(al + off, LBO, SBO);
-            const uint64_t dbh = smem_desc(bh + off, LBO, SBO), dbl = smem_desc(bl + off, LBO, SBO);
+            const uint32_t offa = (uint32_t)ks * 2u * LBO_A, offb = (uint32_t)ks * 2u * LBO;  // 8 K columns
+            const uint64_t dah = smem_desc(ah + offa, LBO_A, SBO), dal = smem_desc(al + offa, LBO_A, SBO);
+            const uint64_t dbh = smem_desc(bh + offb, LBO, SBO), dbl = smem_desc(bl + offb, LBO, SBO);
             tc_mma_tf32(d, dah, dbh, idesc, (nin > 0 || ks > 0) ? 1u : 0u);
             tc_mma_tf32(d, dah, dbl, idesc, 1u);
             tc_mma_tf32(d, dal, dbh, idesc, 1u);
@@ -643,16 +680,62 @@ void launch_split_tf32(size_t nrow, int nfo, const double* src, float* out, cuda
   k_split_tf32<<<blocks, 256, 0, st>>>(nrow, nfo, src, out, n);
 }
 
-void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
-                              const float* coef_hl, size_t coef_part, const int8_t* pair_fmt, const PairGeo* pairs,
-                              const float* momv_hl, size_t mom_part, const MeshDev& M, const double* boys_tab,
-                              double* vh, int ldv, unsigned long long* cnt, int* err, long long wait_limit,
-                              cudaStream_t st) {
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, looked up once through the runtime (the
+// library links no driver library).
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<EncodeTiledFn>(nullptr);
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of TF32 hi/lo rows in the split layout [nrow][KSEG/4][nfo][4]
+// floats, lo part at + part floats: dimensions (4 columns, nfo FOs, nrow*KSEG/4
+// chunks, 2 parts), box (4, 128, 1, 2) = one 2 KB chunk of a 128-FO block in
+// both parts (hi, then lo); FOs past nfo read as zero.  Every stride is a multiple of 16 bytes (nfo*16;
+// part is a multiple of 4 floats since KSEG is).
+bool rows_map(CUtensorMap* m, const float* base, int nfo, size_t nrow, size_t part) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc || !base || nfo <= 0) return false;
+  const size_t nchunk = std::max<size_t>(nrow, 1) * (KSEG / 4);
+  const size_t pstride = std::max(part, nchunk * (size_t)nfo * 4) * sizeof(float);
+  const cuuint64_t dims[4] = {4, (cuuint64_t)nfo, (cuuint64_t)nchunk, 2};
+  const cuuint64_t strides[3] = {16, (cuuint64_t)nfo * 16, (cuuint64_t)pstride};
+  const cuuint32_t box[4] = {4, TILE, 1, 2};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+cudaError_t launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls,
+                                     int nfo, const float* coef_hl, size_t coef_part, const int8_t* pair_fmt,
+                                     const PairGeo* pairs, const float* momv_hl, size_t mom_part, const MeshDev& M,
+                                     const double* boys_tab, double* vh, int ldv, unsigned long long* cnt, int* err,
+                                     long long wait_limit, cudaStream_t st) {
+  static_assert(KSEG % 4 == 0, "the split layout's parts start on 16-byte boundaries");
+  CUtensorMap tm_coef, tm_mom;
+  const size_t npairs = coef_part / ((size_t)nfo * KSEG), nmom = mom_part / ((size_t)nfo * KSEG);
+  if (!rows_map(&tm_coef, coef_hl, nfo, npairs, coef_part) || !rows_map(&tm_mom, momv_hl, nfo, nmom, mom_part))
+    return cudaErrorInvalidValue;
   dim3 grid(M.ntiles, (nfo + TILE - 1) / TILE);
   const long lim = wait_limit > 0 ? (long)wait_limit : TC_SPIN_LIMIT;
-  k_coulomb_shared_tc<<<grid, TC_THREADS, sizeof(TcSmem), st>>>(ncalls, lists, share, calls, nfo, coef_hl,
-                                                                   pair_fmt, pairs, momv_hl, coef_part, mom_part, M,
-                                                                   boys_tab, vh, ldv, cnt, err, lim);
+  k_coulomb_shared_tc<<<grid, TC_THREADS, sizeof(TcSmem), st>>>(ncalls, lists, share, calls, nfo, tm_coef, pair_fmt,
+                                                                   pairs, tm_mom, M, boys_tab, vh, ldv, cnt, err, lim);
+  return cudaGetLastError();
 }
 
 }  // namespace flosic

@@ -126,19 +126,20 @@ void init_coulomb_tc();
 // TF32 hi/lo split of nrow x nfo rows of KSEG doubles into the chunk-major
 // [nrow][KSEG/4][nfo][4] layout (hi, then lo at + nrow*nfo*KSEG floats).
 void launch_split_tf32(size_t nrow, int nfo, const double* src, float* out, cudaStream_t st);
-// Mixed-precision shared-geometry Coulomb GEMM on tcgen05 (csrc/coulomb_tc.cu).
-void launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls, int nfo,
-                              const float* coef_hl, size_t coef_part, const int8_t* pair_fmt, const PairGeo* pairs,
-                              const float* momv_hl, size_t mom_part, const MeshDev& M, const double* boys_tab,
-                              double* vh, int ldv, unsigned long long* cnt, int* err, long long wait_limit,
-                              cudaStream_t st);
+// Mixed-precision shared-geometry Coulomb GEMM on tcgen05 (csrc/coulomb_tc.cu);
+// the A rows reach shared memory by TMA through tensor maps built here.
+cudaError_t launch_coulomb_shared_tc(int ncalls, const int* lists, const CallShare* share, const CallInfo* calls,
+                                     int nfo, const float* coef_hl, size_t coef_part, const int8_t* pair_fmt,
+                                     const PairGeo* pairs, const float* momv_hl, size_t mom_part, const MeshDev& M,
+                                     const double* boys_tab, double* vh, int ldv, unsigned long long* cnt, int* err,
+                                     long long wait_limit, cudaStream_t st);
 // cnt[0..2]: near/far/terms of the shared-geometry kernel, cnt[3..5]: of the per-FO kernel;
 // mid (may be null) is recorded between the two kernels.
-void launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
-                        const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
-                        const MeshDev& M, const double* boys_tab, double* vh, int ldv, const CoulombConfig& cfg,
-                        bool mixed, const CoulombScratch& scr, unsigned long long* cnt, cudaEvent_t mid,
-                        cudaStream_t st);
+cudaError_t launch_coulomb_mma(int ncalls, const CallInfo* calls, const PairGeo* pairs, int npairs, int nfo,
+                               const double* coef, const int8_t* maxfmt, const CallFO* cfo, const double* momv,
+                               const MeshDev& M, const double* boys_tab, double* vh, int ldv,
+                               const CoulombConfig& cfg, bool mixed, const CoulombScratch& scr,
+                               unsigned long long* cnt, cudaEvent_t mid, cudaStream_t st);
 
 // Exchange-correlation of the FO densities (fully polarised, NSPN forced to 2 as
 // in apotnl_sic.F:419) from the FO values/derivatives phi[(ch*nfo+k)*ldp+p];

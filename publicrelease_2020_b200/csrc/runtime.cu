@@ -787,9 +787,9 @@ void coulomb_eval(flosic_ctx* c, int nf, const double* dm, double* vh) {
     CUDA_CHECK(cudaMemsetAsync(c->d_tc_err.p, 0, sizeof(int), st));
   }
   CoulombScratch scr{c->d_pairfmt.p, c->d_share.p, c->d_lists.p, c->d_coef_hl.p, c->d_momv_hl.p, c->d_tc_err.p};
-  launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p, c->d_callfo.p,
-                     c->d_mom.p, c->eval_mesh(), c->d_boys.p, vh, P, c->coulomb_cfg, mixed, scr,
-                     c->d_cnt.p, c->ev[8], st);
+  CUDA_CHECK(launch_coulomb_mma(ncalls, c->d_calls.p, c->d_pairs.p, npairs, nf, c->d_coef.p, c->d_maxfmt.p,
+                                c->d_callfo.p, c->d_mom.p, c->eval_mesh(), c->d_boys.p, vh, P, c->coulomb_cfg, mixed,
+                                scr, c->d_cnt.p, c->ev[8], st));
   CUDA_CHECK(cudaEventRecord(c->ev[9], st));
   c->launches += c->coulomb_cfg.per_fo_only ? 4 : 5;
   unsigned long long cnt[6];

@@ -3,8 +3,10 @@ context re-sharded between passes (flosic_sic_set_shard after the geometry and
 orbitals are set), its packed partial sums added on the device and combined.
 It must equal the one-pass cycle to rounding (1e-10 relative, the bar of the
 multi-context shard tests), again when repeated, and the context must run
-the whole mesh again after set_shard(0, 1).  The file sorts after the other GPU
-tests, before the allocation-free entry point's."""
+the whole mesh again after set_shard(0, 1); in both FO density routes (the
+reference's pair route forms each point's density from the calls whose sphere
+holds it, whichever pass the point falls in).  The file sorts after the other
+GPU tests, before the allocation-free entry point's."""
 import numpy as np
 import pytest
 
@@ -31,11 +33,13 @@ def _close(a, b, sysm):
         assert np.allclose(a["cfrm"][s][:n], b["cfrm"][s][:n], rtol=1e-10, atol=1e-12)
 
 
+@pytest.mark.parametrize("density", ["phi2", "pairs"])
 @pytest.mark.parametrize("name", list(SYSTEMS))
-def test_chunked_cycle_equals_one_pass(name):
+def test_chunked_cycle_equals_one_pass(name, density):
     sysm = SYSTEMS[name]()
     ctx = S.open_system(sysm)
     try:
+        ctx.set_density_mode(density)
         ref = ctx.cycle()
         st = ctx.stats()
         got = chunked_cycle(ctx, 3, device="cuda:0")

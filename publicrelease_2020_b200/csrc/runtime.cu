@@ -2023,12 +2023,17 @@ int flosic_sic_mgga_mixin(flosic_ctx* c, int lspx, int iorbx, double* mixin) {
     spin_potentials(c, s);
     SpinCache& S = c->spin[s];
     const int P = c->nmsh;
-    // the FO's density channels and tau (as k_xc forms them), then SUBVLXC's SCAN branch
+    // the FO's density channels (those k_xc used: phi^2, or the pair route's)
+    // and tau, then SUBVLXC's SCAN branch
     DevBuf<double> dr, dv, dm;
     dr.ensure((size_t)11 * P);
     dv.ensure(2 * (size_t)P);
     dm.ensure(4 * (size_t)P);
-    launch_density(P, S.nf, k, 4, S.phi.p, P, dr.p, P, c->st);
+    if (c->density == FLOSIC_DENSITY_PAIRS)
+      CUDA_CHECK(cudaMemcpy2DAsync(dr.p, sizeof(double) * P, S.rhog.p + (size_t)k * P, sizeof(double) * P * S.nf,
+                                   sizeof(double) * P, 4, cudaMemcpyDeviceToDevice, c->st));
+    else
+      launch_density(P, S.nf, k, 4, S.phi.p, P, dr.p, P, c->st);
     launch_fo_tau(P, S.nf, k, S.phi.p, P, dr.p + (size_t)10 * P, c->st);
     const int nblk = std::min(1024, (P + 255) / 256);
     c->d_part.ensure((size_t)nblk * NPART);

@@ -119,6 +119,29 @@ def test_cycle_pairs_matches_oracle(pair):
     assert abs(g["esic"] - r["esic"]) < ESIC_TOL, (name, g["esic"], r["esic"])
 
 
+def test_scan_mixin_pairs_matches_oracle(pair):
+    """MGGA#### records (flosic_sic_mgga_mixin) from the pair-route density:
+    the oracle's MIXIN of APOTNL_SIC (its own pair-route density and tau), with
+    the masks of the file-writer test (SCAN amplifies rounding where rho is
+    far below its maximum)."""
+    name, sysm, ctx, orc = pair
+    if "scan" not in name:
+        pytest.skip("MIXIN belongs to meta-GGA functionals")
+    n = sysm.nmsh
+    for s in range(1, sysm.nspn + 1):
+        for k in range(1, sysm.nfrm[s - 1] + 1):
+            m = ctx.mgga_mixin(s, k)
+            o = orc.apotnl_sic(s, k)
+            _, rho, _ = orc.coupot_sic(s, k)
+            r0 = rho[0]
+            keep = r0 > 1e-3 * r0.max()
+            assert np.all(m[n:] == 0.0)
+            for d in range(4):
+                scale = np.abs(o["mixin"][keep, d]).max()
+                assert np.max(np.abs(m[:n][keep, d] - o["mixin"][keep, d])) <= 1e-8 * scale, (name, s, k, d)
+                assert np.sum(np.abs(m[:n, d] - o["mixin"][:, d]) * r0 * sysm.wmsh) <= 1e-8 * scale, (name, s, k, d)
+
+
 def test_mode_switch_restores_phi2(pair):
     """Switching back to phi^2 invalidates the cached potentials: the cycle
     then equals a fresh context's default cycle bit for bit."""
